@@ -1,0 +1,1413 @@
+// C ABI of libdtb (include/dtb.h): host-side construction of the network
+// (parameter classes, pull / push CSR), memory plan, step scheduling (push or
+// pull per chunk of steps, CUDA graphs), state access and BOLD.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "dtb.h"
+#include "dtb_io.h"
+#include "dtb_kernels.cuh"
+
+using namespace dtb;
+
+// ------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return fail(DTB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                                    \
+    } while (0)
+
+#define RET(expr)                      \
+    do {                               \
+        int r_ = (expr);               \
+        if (r_ != DTB_OK) return r_;   \
+    } while (0)
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+using Row26 = std::array<uint32_t, 26>;
+struct RowHash {
+    size_t operator()(const Row26& r) const
+    {
+        uint64_t h = 1469598103934665603ull;
+        for (uint32_t v : r) { h ^= v; h *= 1099511628211ull; }
+        return (size_t)h;
+    }
+};
+
+inline uint32_t fbits(float f)
+{
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+// Property row (+ decay) -> class parameters (models/block.py:156-169 split).
+ParamClass make_class(const float* prop, const float* decay, float dt)
+{
+    ParamClass p;
+    std::memset(&p, 0, sizeof(p));
+    p.g = make_float4(prop[10], prop[11], prop[12], prop[13]);
+    p.Vu = make_float4(prop[14], prop[15], prop[16], prop[17]);
+    p.decay = make_float4(decay[0], decay[1], decay[2], decay[3]);
+    p.gL = prop[6];
+    p.VL = prop[7];
+    volatile float rc = 1.0f / prop[4];  // torch: C.reciprocal() * dt
+    p.rCdt = rc * dt;
+    p.Vth = prop[8];
+    p.Vreset = prop[9];
+    p.Tref = prop[5];
+    p.Iext = prop[2];
+    p.noise = prop[0];
+    const float s = prop[3];
+    p.sub = (s >= 0.0f && s < 2147483647.0f && std::floor(s) == s) ? (int32_t)s : -1;
+    p.C = prop[4];
+    return p;
+}
+
+// exp(-dt/tau) evaluated as tau.reciprocal() * (-dt) then exp (block.py:71).
+void default_decay(const float* prop, float dt, float* out)
+{
+    for (int c = 0; c < 4; ++c) {
+        volatile float r = 1.0f / prop[18 + c];
+        volatile float x = r * (-dt);
+        out[c] = std::exp(x);
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ handle
+struct dtb_block {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int64_t N = 0, S = 0;
+    int n_sub = 0, n_classes = 0;
+    int pc_cap = 0, sub_cap = 0;
+    ParamClass* d_pc = nullptr;
+    uint32_t* d_sub_count = nullptr;
+    float dt = 0.1f;
+    uint64_t seed = 0;
+    uint32_t stream_id = 0;
+    DevState ds{};
+    std::vector<void*> allocs;
+    int64_t dev_bytes = 0;
+    // host mirrors
+    std::vector<ParamClass> classes;
+    std::vector<std::array<float, 22>> class_prop_base;  // creation-time rows (scale_property base)
+    std::vector<std::array<float, 22>> class_prop;       // current rows
+    std::vector<std::array<float, 4>> class_decay;
+    std::vector<uint32_t> sub_count;
+    uint64_t steps = 0;          // host mirror of ctl->steps_done
+    uint32_t stats_cap = 0;
+    bool has_pull = false, has_push = false;
+    int64_t max_out = 0, max_in = 0;
+    // scratch
+    uint32_t* d_forced[2] = {nullptr, nullptr};
+    uint8_t* d_u8 = nullptr;      // [N] upload staging for forced sets
+    float* d_export = nullptr;    // [4N]
+    float* d_iui_override = nullptr;
+    bool override_pending = false;
+    unsigned* d_err = nullptr;
+    // pinned host staging
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    RunParams* h_run = nullptr;   // pinned
+    // auto mode
+    double last_frac = -1.0;
+    double pull_threshold = 0.05;
+    int chunk = 32;
+    // graphs: [mode][isolated-agnostic] chunk graphs
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+    int graph_len[3] = {0, 0, 0};
+    bool use_graphs = true;
+    // attached BOLD
+    int bold_R = 0;
+};
+
+struct dtb_bold {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t R = 0;
+    int dtype = 0;
+    double eps, ts, tf, t0, alpha, E0, V0, dt;
+    void* s = nullptr; void* q = nullptr; void* v = nullptr; void* f = nullptr;
+    void* tmp_u = nullptr; void* tmp_o = nullptr;  // device staging for host pointers
+    void* tmp_w = nullptr; size_t tmp_w_bytes = 0;
+};
+
+template <typename T>
+static int dalloc(dtb_block* b, T** p, size_t count)
+{
+    void* q = nullptr;
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DTB_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s (held %lld bytes)", bytes,
+                    cudaGetErrorString(e), (long long)b->dev_bytes);
+    }
+    b->allocs.push_back(q);
+    b->dev_bytes += (int64_t)bytes;
+    *p = reinterpret_cast<T*>(q);
+    return DTB_OK;
+}
+
+static int ensure_pinned(dtb_block* b, size_t bytes)
+{
+    if (b->pinned_bytes >= bytes) return DTB_OK;
+    if (b->pinned) cudaFreeHost(b->pinned);
+    b->pinned = nullptr;
+    b->pinned_bytes = 0;
+    CK(cudaMallocHost(&b->pinned, bytes));
+    b->pinned_bytes = bytes;
+    return DTB_OK;
+}
+
+static inline unsigned grid_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+static int copy_out(dtb_block* b, void* dst, const void* dsrc, size_t bytes, int where)
+{
+    if (bytes == 0) return DTB_OK;
+    if (where == DTB_DEVICE) {
+        CK(cudaMemcpyAsync(dst, dsrc, bytes, cudaMemcpyDeviceToDevice, b->stream));
+    } else {
+        CK(cudaMemcpyAsync(dst, dsrc, bytes, cudaMemcpyDeviceToHost, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
+    }
+    return DTB_OK;
+}
+
+// ------------------------------------------------------------ classes
+// Deduplicates property rows (+ decay) into the class table.
+static int build_classes(dtb_block* b, int64_t N, const float* property, const float* decay,
+                         std::vector<uint32_t>& cls)
+{
+    std::unordered_map<Row26, uint32_t, RowHash> map;
+    map.reserve(1024);
+    b->classes.clear();
+    b->class_prop.clear();
+    b->class_decay.clear();
+    cls.resize((size_t)N);
+    int max_sub = -1;
+    for (int64_t i = 0; i < N; ++i) {
+        const float* pr = property + i * DTB_NPROP;
+        float dc[4];
+        if (decay) std::memcpy(dc, decay + i * 4, sizeof(dc));
+        else default_decay(pr, b->dt, dc);
+        Row26 key;
+        for (int c = 0; c < 22; ++c) key[c] = fbits(pr[c]);
+        for (int c = 0; c < 4; ++c) key[22 + c] = fbits(dc[c]);
+        auto it = map.find(key);
+        uint32_t id;
+        if (it == map.end()) {
+            id = (uint32_t)b->classes.size();
+            map.emplace(key, id);
+            b->classes.push_back(make_class(pr, dc, b->dt));
+            std::array<float, 22> row;
+            std::memcpy(row.data(), pr, sizeof(float) * 22);
+            b->class_prop.push_back(row);
+            std::array<float, 4> d4 = {dc[0], dc[1], dc[2], dc[3]};
+            b->class_decay.push_back(d4);
+            max_sub = std::max(max_sub, b->classes.back().sub);
+        } else {
+            id = it->second;
+        }
+        cls[(size_t)i] = id;
+    }
+    // models/block.py:146 iterates range(sub_idx.max().int() + 1)
+    float mx = -INFINITY;
+    for (auto& r : b->class_prop) mx = std::max(mx, r[3]);
+    b->n_sub = (N > 0 && mx >= 0.0f) ? (int)mx + 1 : 0;
+    b->n_classes = (int)b->classes.size();
+    b->sub_count.assign((size_t)b->n_sub, 0u);
+    for (int64_t i = 0; i < N; ++i) {
+        const int s = b->classes[cls[(size_t)i]].sub;
+        if (s >= 0 && s < b->n_sub) b->sub_count[(size_t)s]++;
+    }
+    (void)max_sub;
+    return DTB_OK;
+}
+
+// ------------------------------------------------------------ state setup
+static int alloc_state(dtb_block* b)
+{
+    const int64_t N = b->N;
+    DevState& s = b->ds;
+    s.N = N;
+    s.n_words = ((N + 127) / 128) * 4;
+    RET(dalloc(b, &s.V, (size_t)N));
+    RET(dalloc(b, &s.J, (size_t)N));
+    RET(dalloc(b, &s.tlast, (size_t)N));
+    RET(dalloc(b, &s.isyn_override, (size_t)N));
+    for (int p = 0; p < 2; ++p) RET(dalloc(b, &s.bits[p], (size_t)s.n_words));
+    RET(dalloc(b, &s.abits, (size_t)s.n_words));
+    RET(dalloc(b, &s.ctl, 1));
+    RET(dalloc(b, &s.unmapped_nact, 1));
+    RET(dalloc(b, &b->d_err, 4));
+    CK(cudaMemsetAsync(s.J, 0, sizeof(float4) * (size_t)N, b->stream));
+    CK(cudaMemsetAsync(s.tlast, 0, sizeof(float) * (size_t)N, b->stream));
+    for (int p = 0; p < 2; ++p) CK(cudaMemsetAsync(s.bits[p], 0, sizeof(uint32_t) * (size_t)s.n_words, b->stream));
+    CK(cudaMemsetAsync(s.abits, 0, sizeof(uint32_t) * (size_t)s.n_words, b->stream));
+    CK(cudaMemsetAsync(s.ctl, 0, sizeof(Ctl), b->stream));
+    CK(cudaMemsetAsync(s.unmapped_nact, 0, sizeof(uint32_t), b->stream));
+    s.seed = b->seed;
+    s.stream_id = b->stream_id;
+    s.dt = b->dt;
+    s.forced_active = nullptr;
+    s.forced_new = nullptr;
+    return DTB_OK;
+}
+
+// Class table, per-neuron class ids, subblock tables and initial V.
+static int upload_class_tables(dtb_block* b)
+{
+    DevState& s = b->ds;
+    if (b->n_classes > b->pc_cap || !b->d_pc) {
+        const int cap = std::max(64, b->n_classes);
+        RET(dalloc(b, &b->d_pc, (size_t)cap));
+        b->pc_cap = cap;
+    }
+    CK(cudaMemcpyAsync(b->d_pc, b->classes.data(), sizeof(ParamClass) * b->classes.size(), cudaMemcpyHostToDevice,
+                       b->stream));
+    s.pc = b->d_pc;
+    if (b->n_sub > b->sub_cap || !b->d_sub_count) {
+        const int cap = std::max(16, b->n_sub);
+        RET(dalloc(b, &b->d_sub_count, (size_t)cap));
+        RET(dalloc(b, &s.sub_spk, (size_t)cap));
+        RET(dalloc(b, &s.sub_nact, (size_t)cap));
+        RET(dalloc(b, &s.sub_vsum, (size_t)cap));
+        CK(cudaMemsetAsync(s.sub_spk, 0, sizeof(uint32_t) * cap, b->stream));
+        CK(cudaMemsetAsync(s.sub_nact, 0, sizeof(uint32_t) * cap, b->stream));
+        CK(cudaMemsetAsync(s.sub_vsum, 0, sizeof(double) * cap, b->stream));
+        b->sub_cap = cap;
+        s.st_spk = nullptr;       // stats rows are n_sub wide: reallocate
+        b->stats_cap = 0;
+    }
+    if (b->n_sub)
+        CK(cudaMemcpyAsync(b->d_sub_count, b->sub_count.data(), sizeof(uint32_t) * b->n_sub, cudaMemcpyHostToDevice,
+                           b->stream));
+    s.sub_count = b->d_sub_count;
+    s.n_sub = b->n_sub;
+    CK(cudaStreamSynchronize(b->stream));
+    return DTB_OK;
+}
+
+// Class table, per-neuron class ids, subblock tables and initial V.
+static int upload_classes(dtb_block* b, const std::vector<uint32_t>& cls, bool init_v)
+{
+    DevState& s = b->ds;
+    RET(upload_class_tables(b));
+    uint32_t* dcls = nullptr;
+    RET(dalloc(b, &dcls, (size_t)b->N));
+    CK(cudaMemcpy(dcls, cls.data(), sizeof(uint32_t) * (size_t)b->N, cudaMemcpyHostToDevice));
+    s.cls = dcls;
+    if (init_v) {
+        // models/block.py:56: V = ones * (V_th + V_reset) / 2
+        std::vector<float> v0((size_t)b->N);
+        for (int64_t i = 0; i < b->N; ++i) {
+            const ParamClass& p = b->classes[cls[(size_t)i]];
+            volatile float sum = p.Vth + p.Vreset;
+            v0[(size_t)i] = sum / 2.0f;
+        }
+        CK(cudaMemcpy(s.V, v0.data(), sizeof(float) * (size_t)b->N, cudaMemcpyHostToDevice));
+    }
+    return DTB_OK;
+}
+
+static int ensure_stats(dtb_block* b, uint32_t rows)
+{
+    if (b->stats_cap >= rows && b->ds.st_spk) return DTB_OK;
+    const uint32_t cap = std::max<uint32_t>(rows, 64);
+    DevState& s = b->ds;
+    RET(dalloc(b, &s.st_spk, (size_t)cap * std::max(1, b->n_sub)));
+    RET(dalloc(b, &s.st_mean, (size_t)cap * std::max(1, b->n_sub)));
+    RET(dalloc(b, &s.st_nact, (size_t)cap));
+    b->stats_cap = cap;
+    CK(cudaMemcpyAsync(&s.ctl->stats_cap, &cap, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    for (auto& g : b->graph) if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    return DTB_OK;
+}
+
+// Host CSR builders: stable counting sorts keep the given entry order
+// inside every row (pull: by post, torch.sparse.mm order; push: by pre,
+// cuda/src/configuration.cpp:228 stable_sort_by_key).
+static int build_csr_host(int64_t N, int64_t S, const uint32_t* key, const uint32_t* other, const uint8_t* kind,
+                          const float* w, std::vector<int64_t>& rowptr, std::vector<uint32_t>& col,
+                          std::vector<float2>& val, int64_t& max_row)
+{
+    rowptr.assign((size_t)N + 1, 0);
+    for (int64_t e = 0; e < S; ++e) rowptr[(size_t)key[e] + 1]++;
+    max_row = 0;
+    for (int64_t i = 0; i < N; ++i) {
+        max_row = std::max<int64_t>(max_row, rowptr[(size_t)i + 1]);
+        rowptr[(size_t)i + 1] += rowptr[(size_t)i];
+    }
+    col.resize((size_t)S);
+    val.resize((size_t)S);
+    std::vector<int64_t> cur(rowptr.begin(), rowptr.end() - 1);
+    for (int64_t e = 0; e < S; ++e) {
+        const int64_t d = cur[(size_t)key[e]]++;
+        col[(size_t)d] = other[e] | (kind[e] ? kKindBit : 0u);
+        val[(size_t)d] = make_float2(w[2 * e], w[2 * e + 1]);
+    }
+    return DTB_OK;
+}
+
+static int upload_csr(dtb_block* b, const std::vector<int64_t>& rowptr, const std::vector<uint32_t>& col,
+                      const std::vector<float2>& val, const int64_t** drow, const uint32_t** dcol, const float2** dval)
+{
+    int64_t* r = nullptr; uint32_t* c = nullptr; float2* v = nullptr;
+    RET(dalloc(b, &r, rowptr.size()));
+    RET(dalloc(b, &c, col.size()));
+    RET(dalloc(b, &v, val.size()));
+    CK(cudaMemcpy(r, rowptr.data(), sizeof(int64_t) * rowptr.size(), cudaMemcpyHostToDevice));
+    if (!col.empty()) {
+        CK(cudaMemcpy(c, col.data(), sizeof(uint32_t) * col.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(v, val.data(), sizeof(float2) * val.size(), cudaMemcpyHostToDevice));
+    }
+    *drow = r; *dcol = c; *dval = v;
+    return DTB_OK;
+}
+
+static void destroy_block(dtb_block* b)
+{
+    if (!b) return;
+    DeviceGuard g(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto& gr : b->graph) if (gr) cudaGraphExecDestroy(gr);
+    for (void* p : b->allocs) cudaFree(p);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
+    if (b->pinned) cudaFreeHost(b->pinned);
+    if (b->h_run) cudaFreeHost(b->h_run);
+    delete b;
+}
+
+static int finish_create(dtb_block* b)
+{
+    CK(cudaMallocHost((void**)&b->h_run, sizeof(RunParams)));
+    RET(ensure_stats(b, 256));
+    CK(cudaStreamSynchronize(b->stream));
+    return DTB_OK;
+}
+
+// ------------------------------------------------------------ launches
+static int launch_update(dtb_block* b, const DevState& s, bool gather, bool forced)
+{
+    const unsigned grid = grid_for(s.N, kWarpNeurons * (kStepThreads / 32));
+    if (grid == 0) return DTB_OK;
+    if (forced) {
+        if (gather) k_step<true, true, true><<<grid, kStepThreads, 0, b->stream>>>(s);
+        else k_step<false, true, true><<<grid, kStepThreads, 0, b->stream>>>(s);
+    } else {
+        if (gather) k_step<true, true, false><<<grid, kStepThreads, 0, b->stream>>>(s);
+        else k_step<false, true, false><<<grid, kStepThreads, 0, b->stream>>>(s);
+    }
+    CK(cudaGetLastError());
+    return DTB_OK;
+}
+
+static int launch_gather_only(dtb_block* b, const DevState& s)
+{
+    const unsigned grid = grid_for(s.N, kWarpNeurons * (kStepThreads / 32));
+    if (grid == 0) return DTB_OK;
+    k_step<true, false, false><<<grid, kStepThreads, 0, b->stream>>>(s);
+    CK(cudaGetLastError());
+    return DTB_OK;
+}
+
+static int launch_scatter(dtb_block* b, const DevState& s)
+{
+    const int64_t warps = (s.n_words + 31) / 32;
+    const unsigned grid = grid_for(warps * 32, 256);
+    if (grid == 0) return DTB_OK;
+    k_scatter<<<grid, 256, 0, b->stream>>>(s);
+    CK(cudaGetLastError());
+    return DTB_OK;
+}
+
+// n steps with one propagation method (no host synchronisation).
+static int enqueue_steps(dtb_block* b, int n, int mode)
+{
+    if (n <= 0) return DTB_OK;
+    const DevState& s = b->ds;
+    if (mode == DTB_MODE_PUSH) {
+        for (int k = 0; k < n; ++k) {
+            RET(launch_update(b, s, false, false));
+            RET(launch_scatter(b, s));
+        }
+    } else {
+        RET(launch_update(b, s, false, false));
+        for (int k = 1; k < n; ++k) RET(launch_update(b, s, true, false));
+        RET(launch_gather_only(b, s));
+    }
+    return DTB_OK;
+}
+
+static int enqueue_chunk(dtb_block* b, int n, int mode)
+{
+    if (!b->use_graphs || n != b->chunk || b->stream == nullptr) return enqueue_steps(b, n, mode);
+    cudaGraphExec_t& ge = b->graph[mode];
+    if (!ge) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_steps(b, n, mode);
+        cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+        if (rc != DTB_OK) { if (g) cudaGraphDestroy(g); return rc; }
+        if (ce != cudaSuccess) return fail(DTB_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { ge = nullptr; return fail(DTB_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce)); }
+    }
+    CK(cudaGraphLaunch(ge, b->stream));
+    return DTB_OK;
+}
+
+static int choose_mode(dtb_block* b, int mode)
+{
+    if (mode == DTB_MODE_PUSH && !b->has_push) return DTB_MODE_PULL;
+    if (mode == DTB_MODE_PULL && !b->has_pull) return DTB_MODE_PUSH;
+    if (mode != DTB_MODE_AUTO) return mode;
+    if (!b->has_push) return DTB_MODE_PULL;
+    if (!b->has_pull) return DTB_MODE_PUSH;
+    const double f = b->last_frac < 0.0 ? 0.0 : b->last_frac;
+    return f > b->pull_threshold ? DTB_MODE_PULL : DTB_MODE_PUSH;
+}
+
+static int set_run_params(dtb_block* b, float noise_rate, int isolated)
+{
+    b->h_run->run_base = b->steps;
+    b->h_run->noise_rate = noise_rate;
+    b->h_run->isolated = isolated ? 1 : 0;
+    CK(cudaMemcpyAsync(&b->ds.ctl->run_base, b->h_run, sizeof(RunParams), cudaMemcpyHostToDevice, b->stream));
+    return DTB_OK;
+}
+
+// Copies `rows` stats rows to the caller (row offset `row0` of the outputs).
+static int emit_stats(dtb_block* b, int rows, int64_t row0, float* sum_out, float* mean_out, uint32_t* nact_out,
+                      int where, std::vector<uint32_t>* nact_host)
+{
+    const size_t ns = (size_t)b->n_sub;
+    const size_t bs = rows * ns * sizeof(float);
+    const size_t bn = rows * sizeof(uint32_t);
+    if (where == DTB_DEVICE) {
+        if (sum_out && bs) CK(cudaMemcpyAsync(sum_out + row0 * ns, b->ds.st_spk, bs, cudaMemcpyDeviceToDevice, b->stream));
+        if (mean_out && bs) CK(cudaMemcpyAsync(mean_out + row0 * ns, b->ds.st_mean, bs, cudaMemcpyDeviceToDevice, b->stream));
+        if (nact_out) CK(cudaMemcpyAsync(nact_out + row0, b->ds.st_nact, bn, cudaMemcpyDeviceToDevice, b->stream));
+    }
+    const bool need_host = where == DTB_HOST || nact_host;
+    if (need_host) {
+        RET(ensure_pinned(b, 2 * bs + bn + 64));
+        char* p = reinterpret_cast<char*>(b->pinned);
+        if (where == DTB_HOST && bs) {
+            if (sum_out) CK(cudaMemcpyAsync(p, b->ds.st_spk, bs, cudaMemcpyDeviceToHost, b->stream));
+            if (mean_out) CK(cudaMemcpyAsync(p + bs, b->ds.st_mean, bs, cudaMemcpyDeviceToHost, b->stream));
+        }
+        CK(cudaMemcpyAsync(p + 2 * bs, b->ds.st_nact, bn, cudaMemcpyDeviceToHost, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
+        if (where == DTB_HOST) {
+            if (sum_out && bs) std::memcpy(sum_out + row0 * ns, p, bs);
+            if (mean_out && bs) std::memcpy(mean_out + row0 * ns, p + bs, bs);
+            if (nact_out) std::memcpy(nact_out + row0, p + 2 * bs, bn);
+        }
+        if (nact_host) {
+            nact_host->resize(rows);
+            std::memcpy(nact_host->data(), p + 2 * bs, bn);
+        }
+    }
+    return DTB_OK;
+}
+
+template <typename T>
+static BoldScalars<T> bold_scalars(const dtb_bold* m)
+{
+    BoldScalars<T> c;
+    const double div_alpha = 1.0 / m->alpha;
+    c.eps = (T)m->eps; c.ts = (T)m->ts; c.tf = (T)m->tf; c.t0 = (T)m->t0; c.E0 = (T)m->E0; c.V0 = (T)m->V0;
+    c.dt = (T)m->dt; c.base = (T)(1.0 - m->E0); c.exq = (T)(div_alpha - 1.0); c.exv = (T)div_alpha;
+    c.k7 = (T)(7.0 * m->E0); c.k2 = (T)(2.0 * m->E0 - 0.2); c.one_em5 = (T)1e-05;
+    return c;
+}
+
+// ------------------------------------------------------------ C ABI
+extern "C" {
+
+int dtb_abi_version(void) { return DTB_ABI_VERSION; }
+
+int dtb_last_error(char* buf, size_t len)
+{
+    if (!buf || len == 0) return DTB_ERR_ARG;
+    std::snprintf(buf, len, "%s", g_err.c_str());
+    return DTB_OK;
+}
+
+static int create_common(dtb_block* b, int device, float dt, uint64_t seed, uint32_t stream_id)
+{
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(DTB_ERR_ARG, "device %d out of range (%d devices)", device, ndev);
+    if (!(dt > 0.0f)) return fail(DTB_ERR_ARG, "dt must be positive");
+    b->device = device;
+    b->dt = dt;
+    b->seed = seed;
+    b->stream_id = stream_id;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking));
+    b->stream = b->own_stream;
+    return DTB_OK;
+}
+
+int dtb_block_create(const dtb_block_desc* d, dtb_block** out)
+{
+    if (!d || !out) return fail(DTB_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (d->n_neurons <= 0 || d->n_neurons > (int64_t)kIndexMask) return fail(DTB_ERR_LIMIT, "n_neurons must be in [1, 2^31-1]");
+    if (!d->property) return fail(DTB_ERR_ARG, "property is null");
+    if (d->n_synapses < 0) return fail(DTB_ERR_ARG, "n_synapses < 0");
+    if (d->n_synapses > 0 && (!d->post || !d->pre || !d->kind || !d->weight)) return fail(DTB_ERR_ARG, "synapse arrays are null");
+    const int64_t N = d->n_neurons, S = d->n_synapses;
+    for (int64_t e = 0; e < S; ++e) {
+        if (d->post[e] >= (uint64_t)N || d->pre[e] >= (uint64_t)N)
+            return fail(DTB_ERR_ARG, "synapse %lld references neuron out of range (post %u, pre %u, N %lld)", (long long)e,
+                        d->post[e], d->pre[e], (long long)N);
+        if (d->kind[e] != 0 && d->kind[e] != 2) return fail(DTB_ERR_ARG, "synapse %lld: kind must be 0 or 2", (long long)e);
+    }
+    dtb_block* b = new dtb_block();
+    DeviceGuard guard(d->device < 0 ? 0 : d->device);
+    int rc = create_common(b, d->device, d->dt, d->seed, d->stream_id);
+    if (rc == DTB_OK) {
+        b->N = N;
+        b->S = S;
+        std::vector<uint32_t> cls;
+        rc = build_classes(b, N, d->property, d->decay, cls);
+        if (rc == DTB_OK) rc = alloc_state(b);
+        if (rc == DTB_OK) rc = upload_classes(b, cls, true);
+        if (rc == DTB_OK) {
+            std::vector<int64_t> rp; std::vector<uint32_t> col; std::vector<float2> val;
+            rc = build_csr_host(N, S, d->post, d->pre, d->kind, d->weight, rp, col, val, b->max_in);
+            if (rc == DTB_OK) rc = upload_csr(b, rp, col, val, &b->ds.prow, &b->ds.pcol, &b->ds.pw);
+            b->has_pull = (rc == DTB_OK);
+            if (rc == DTB_OK && d->build_push) {
+                rc = build_csr_host(N, S, d->pre, d->post, d->kind, d->weight, rp, col, val, b->max_out);
+                if (rc == DTB_OK) rc = upload_csr(b, rp, col, val, &b->ds.qrow, &b->ds.qcol, &b->ds.qw);
+                b->has_push = (rc == DTB_OK);
+            }
+        }
+        if (rc == DTB_OK) rc = finish_create(b);
+    }
+    if (rc != DTB_OK) { destroy_block(b); return rc; }
+    *out = b;
+    return DTB_OK;
+}
+
+int dtb_block_create_synthetic(const dtb_synth_desc* d, dtb_block** out)
+{
+    if (!d || !out) return fail(DTB_ERR_ARG, "null argument");
+    *out = nullptr;
+    const int R = d->n_regions;
+    if (R <= 0 || !d->region_start || !d->region_n_exc || !d->cum || !d->class_property)
+        return fail(DTB_ERR_ARG, "bad synthetic description");
+    if (d->K < 1 || d->K > 1024) return fail(DTB_ERR_LIMIT, "K must be in [1, 1024]");
+    const int64_t N = d->region_start[R];
+    if (d->region_start[0] != 0 || N <= 0 || N > (int64_t)kIndexMask) return fail(DTB_ERR_LIMIT, "bad neuron count");
+    for (int r = 0; r < R; ++r) {
+        if (d->region_start[r + 1] < d->region_start[r]) return fail(DTB_ERR_ARG, "region_start must be non-decreasing");
+        if (d->region_n_exc[r] < 0 || d->region_n_exc[r] > d->region_start[r + 1] - d->region_start[r])
+            return fail(DTB_ERR_ARG, "region_n_exc out of range");
+    }
+    const int64_t S = N * (int64_t)d->K;
+    dtb_block* b = new dtb_block();
+    DeviceGuard guard(d->device < 0 ? 0 : d->device);
+    int rc = create_common(b, d->device, d->dt, d->seed, d->stream_id);
+    std::vector<uint32_t> cls;
+    if (rc == DTB_OK) {
+        b->N = N;
+        b->S = S;
+        // classes = subblocks 2r (excitatory) / 2r+1 (inhibitory)
+        const int nc = 2 * R;
+        b->classes.clear(); b->class_prop.clear(); b->class_decay.clear();
+        for (int c = 0; c < nc; ++c) {
+            const float* pr = d->class_property + (size_t)c * DTB_NPROP;
+            float dc[4];
+            if (d->class_decay) std::memcpy(dc, d->class_decay + (size_t)c * 4, sizeof(dc));
+            else default_decay(pr, b->dt, dc);
+            ParamClass p = make_class(pr, dc, b->dt);
+            p.sub = c;
+            b->classes.push_back(p);
+            std::array<float, 22> row; std::memcpy(row.data(), pr, sizeof(float) * 22); row[3] = (float)c;
+            b->class_prop.push_back(row);
+            b->class_decay.push_back({dc[0], dc[1], dc[2], dc[3]});
+        }
+        b->n_classes = nc;
+        b->n_sub = nc;
+        b->sub_count.assign((size_t)nc, 0u);
+        cls.resize((size_t)N);
+        for (int r = 0; r < R; ++r) {
+            const int64_t s0 = d->region_start[r], s1 = d->region_start[r + 1], ne = d->region_n_exc[r];
+            for (int64_t i = s0; i < s1; ++i) cls[(size_t)i] = (uint32_t)(2 * r + ((i - s0) >= ne ? 1 : 0));
+            b->sub_count[(size_t)(2 * r)] = (uint32_t)ne;
+            b->sub_count[(size_t)(2 * r + 1)] = (uint32_t)(s1 - s0 - ne);
+        }
+        rc = alloc_state(b);
+        if (rc == DTB_OK) rc = upload_classes(b, cls, true);
+    }
+    // generate the pull CSR on the device
+    if (rc == DTB_OK) {
+        int64_t* prow = nullptr; uint32_t* pcol = nullptr; float2* pw = nullptr;
+        int64_t* rs = nullptr; int64_t* ne = nullptr; float* cum = nullptr; uint32_t* outdeg = nullptr;
+        rc = dalloc(b, &prow, (size_t)N + 1);
+        if (rc == DTB_OK) rc = dalloc(b, &pcol, (size_t)S);
+        if (rc == DTB_OK) rc = dalloc(b, &pw, (size_t)S);
+        // temporaries (freed at the end of creation)
+        void *t_rs = nullptr, *t_ne = nullptr, *t_cum = nullptr, *t_out = nullptr;
+        if (rc == DTB_OK) {
+            cudaError_t e = cudaMalloc(&t_rs, sizeof(int64_t) * (R + 1));
+            if (e == cudaSuccess) e = cudaMalloc(&t_ne, sizeof(int64_t) * R);
+            if (e == cudaSuccess) e = cudaMalloc(&t_cum, sizeof(float) * (size_t)R * R);
+            if (e == cudaSuccess) e = cudaMalloc(&t_out, sizeof(uint32_t) * (size_t)(N + 1));
+            if (e != cudaSuccess) { cudaGetLastError(); rc = fail(DTB_ERR_NOMEM, "generator temporaries: %s", cudaGetErrorString(e)); }
+            rs = (int64_t*)t_rs; ne = (int64_t*)t_ne; cum = (float*)t_cum; outdeg = (uint32_t*)t_out;
+        }
+        if (rc == DTB_OK) {
+            cudaMemcpy(rs, d->region_start, sizeof(int64_t) * (R + 1), cudaMemcpyHostToDevice);
+            cudaMemcpy(ne, d->region_n_exc, sizeof(int64_t) * R, cudaMemcpyHostToDevice);
+            cudaMemcpy(cum, d->cum, sizeof(float) * (size_t)R * R, cudaMemcpyHostToDevice);
+            cudaMemset(outdeg, 0, sizeof(uint32_t) * (size_t)(N + 1));
+            cudaMemset(b->d_err, 0, 16);
+            // rowptr = i*K
+            std::vector<int64_t> hrow((size_t)N + 1);
+            for (int64_t i = 0; i <= N; ++i) hrow[(size_t)i] = i * d->K;
+            cudaMemcpy(prow, hrow.data(), sizeof(int64_t) * hrow.size(), cudaMemcpyHostToDevice);
+            GenArgs g;
+            g.N = N; g.R = R; g.region_start = rs; g.region_n_exc = ne; g.cum = cum; g.K = d->K;
+            int Kp = 1; while (Kp < d->K) Kp <<= 1;
+            g.Kp = Kp; g.w_scale = d->w_scale; g.seed = d->gen_seed; g.pcol = pcol; g.pw = pw;
+            g.outdeg = d->build_push ? outdeg : nullptr; g.err = b->d_err;
+            const size_t smem = sizeof(unsigned long long) * (size_t)Kp * kGenWarps;
+            cudaFuncSetAttribute(k_gen_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k_gen_rows<<<grid_for(N, kGenWarps), kGenWarps * 32, smem, b->stream>>>(g);
+            cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+            unsigned herr[4] = {0, 0, 0, 0};
+            if (e == cudaSuccess) e = cudaMemcpy(herr, b->d_err, 16, cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) rc = fail(DTB_ERR_CUDA, "generator: %s", cudaGetErrorString(e));
+            else if (herr[0]) rc = fail(DTB_ERR_ARG, "generator: %u rows could not draw K distinct sources", herr[0]);
+            b->ds.prow = prow; b->ds.pcol = pcol; b->ds.pw = pw;
+            b->has_pull = (rc == DTB_OK);
+            b->max_in = d->K;
+        }
+        // push CSR by transposition on the device
+        if (rc == DTB_OK && d->build_push) {
+            int64_t* qrow = nullptr; uint32_t* qcol = nullptr; float2* qw = nullptr;
+            rc = dalloc(b, &qrow, (size_t)N + 1);
+            if (rc == DTB_OK) rc = dalloc(b, &qcol, (size_t)S);
+            if (rc == DTB_OK) rc = dalloc(b, &qw, (size_t)S);
+            long long* tiles = nullptr;
+            const int64_t ntiles = (N + kScanTile - 1) / kScanTile;
+            if (rc == DTB_OK) {
+                cudaError_t e = cudaMalloc(&tiles, sizeof(long long) * (size_t)(ntiles + 1));
+                if (e != cudaSuccess) { cudaGetLastError(); rc = fail(DTB_ERR_NOMEM, "scan temporaries"); }
+            }
+            if (rc == DTB_OK) {
+                k_scan_tiles<<<(unsigned)ntiles, kScanThreads, 0, b->stream>>>(outdeg, N, qrow, tiles);
+                k_scan_tile_sums<<<1, kScanThreads, 0, b->stream>>>(tiles, ntiles);
+                k_scan_add<<<grid_for(N, 256), 256, 0, b->stream>>>(qrow, N, tiles, ntiles);
+                cudaMemsetAsync(outdeg, 0, sizeof(uint32_t) * (size_t)(N + 1), b->stream);
+                k_fill_push<<<grid_for(N * 32, 256), 256, 0, b->stream>>>(N, prow, pcol, pw, qrow, outdeg, qcol, qw);
+                cudaMemsetAsync(b->d_err, 0, 16, b->stream);
+                const size_t smem = (sizeof(unsigned long long) + sizeof(float2)) * (size_t)kSortCap * kSortWarps;
+                cudaFuncSetAttribute(k_sort_push_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                k_sort_push_rows<<<grid_for(N, kSortWarps), kSortWarps * 32, smem, b->stream>>>(N, qrow, qcol, qw, b->d_err);
+                cudaError_t e = cudaGetLastError();
+                if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+                unsigned herr[4] = {0, 0, 0, 0};
+                if (e == cudaSuccess) e = cudaMemcpy(herr, b->d_err, 16, cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess) rc = fail(DTB_ERR_CUDA, "push CSR build: %s", cudaGetErrorString(e));
+                else if (herr[0]) rc = fail(DTB_ERR_LIMIT, "push CSR build: %u rows longer than %d", herr[0], kSortCap);
+                // max out-degree
+                if (rc == DTB_OK) {
+                    std::vector<int64_t> hq((size_t)N + 1);
+                    cudaMemcpy(hq.data(), qrow, sizeof(int64_t) * hq.size(), cudaMemcpyDeviceToHost);
+                    int64_t mx = 0;
+                    for (int64_t i = 0; i < N; ++i) mx = std::max(mx, hq[(size_t)i + 1] - hq[(size_t)i]);
+                    b->max_out = mx;
+                }
+            }
+            if (tiles) cudaFree(tiles);
+            b->ds.qrow = qrow; b->ds.qcol = qcol; b->ds.qw = qw;
+            b->has_push = (rc == DTB_OK);
+        }
+        cudaFree(t_rs); cudaFree(t_ne); cudaFree(t_cum); cudaFree(t_out);
+    }
+    if (rc == DTB_OK) rc = finish_create(b);
+    if (rc != DTB_OK) { destroy_block(b); return rc; }
+    *out = b;
+    return DTB_OK;
+}
+
+int dtb_block_create_from_npz(const char* dir, float dt, uint64_t seed, uint32_t stream_id, int device, int build_push,
+                              dtb_block** out)
+{
+    if (!dir || !out) return fail(DTB_ERR_ARG, "null argument");
+    *out = nullptr;
+    // generation/read_block.py:31-40: block_0.npz, block_1.npz, ... and their bases
+    std::vector<std::map<std::string, NpyArray>> files;
+    for (int i = 0;; ++i) {
+        std::string path = std::string(dir) + "/block_" + std::to_string(i) + ".npz";
+        FILE* f = std::fopen(path.c_str(), "rb");
+        if (!f) break;
+        std::fclose(f);
+        std::map<std::string, NpyArray> m;
+        std::string err;
+        if (!npz_read(path, m, err)) return fail(DTB_ERR_FORMAT, "%s", err.c_str());
+        files.push_back(std::move(m));
+    }
+    if (files.empty()) return fail(DTB_ERR_IO, "no block_0.npz in %s", dir);
+    std::vector<int64_t> bases(files.size() + 1, 0);
+    for (size_t i = 0; i < files.size(); ++i) {
+        auto it = files[i].find("property");
+        if (it == files[i].end() || it->second.shape.size() != 2 || it->second.shape[1] != DTB_NPROP ||
+            it->second.descr != "<f4")
+            return fail(DTB_ERR_FORMAT, "block_%zu.npz: property must be float32 [N,22]", i);
+        if (files[i].count("src_timestamp") || files[i].count("src_neuron_idx"))
+            return fail(DTB_ERR_FORMAT, "block_%zu.npz: input (src) blocks are not supported", i);
+        bases[i + 1] = bases[i] + it->second.shape[0];
+    }
+    const int64_t N = bases.back();
+    std::vector<float> prop((size_t)N * DTB_NPROP);
+    std::vector<uint32_t> post, pre;
+    std::vector<uint8_t> kind;
+    std::vector<float> w;
+    for (size_t i = 0; i < files.size(); ++i) {
+        auto& m = files[i];
+        const NpyArray& p = m["property"];
+        std::memcpy(prop.data() + bases[i] * DTB_NPROP, p.data.data(), p.data.size());
+        const char* names[5] = {"output_neuron_idx", "input_block_idx", "input_neuron_idx", "input_channel_offset", "weight"};
+        for (auto nm : names)
+            if (!m.count(nm)) return fail(DTB_ERR_FORMAT, "block_%zu.npz: missing %s", i, nm);
+        const NpyArray &on = m["output_neuron_idx"], &ib = m["input_block_idx"], &in = m["input_neuron_idx"],
+                       &ic = m["input_channel_offset"], &wt = m["weight"];
+        const int64_t E = on.count();
+        if (ib.count() != E || in.count() != E || ic.count() != E || wt.count() != 2 * E)
+            return fail(DTB_ERR_FORMAT, "block_%zu.npz: inconsistent synapse array lengths", i);
+        if (on.descr != "<u4" || in.descr != "<u4" || ib.descr != "<i2" || ic.descr != "|u1" || wt.descr != "<f4")
+            return fail(DTB_ERR_FORMAT, "block_%zu.npz: unexpected synapse dtypes", i);
+        const uint32_t* onp = reinterpret_cast<const uint32_t*>(on.data.data());
+        const int16_t* ibp = reinterpret_cast<const int16_t*>(ib.data.data());
+        const uint32_t* inp = reinterpret_cast<const uint32_t*>(in.data.data());
+        const uint8_t* icp = reinterpret_cast<const uint8_t*>(ic.data.data());
+        const float* wtp = reinterpret_cast<const float*>(wt.data.data());
+        for (int64_t e = 0; e < E; ++e) {
+            const int64_t sb = (int64_t)i + ibp[e];
+            if (sb < 0 || sb >= (int64_t)files.size()) return fail(DTB_ERR_FORMAT, "block_%zu.npz: input_block_idx out of range", i);
+            const int64_t po = bases[i] + onp[e], pr = bases[(size_t)sb] + inp[e];
+            if (po >= bases[i + 1] || pr >= bases[(size_t)sb + 1]) return fail(DTB_ERR_FORMAT, "block_%zu.npz: neuron index out of range", i);
+            post.push_back((uint32_t)po);
+            pre.push_back((uint32_t)pr);
+            kind.push_back(icp[e]);
+            w.push_back(wtp[2 * e]);
+            w.push_back(wtp[2 * e + 1]);
+        }
+    }
+    dtb_block_desc d;
+    std::memset(&d, 0, sizeof(d));
+    d.n_neurons = N; d.property = prop.data(); d.decay = nullptr;
+    d.n_synapses = (int64_t)post.size(); d.post = post.data(); d.pre = pre.data(); d.kind = kind.data(); d.weight = w.data();
+    d.dt = dt; d.seed = seed; d.stream_id = stream_id; d.device = device; d.build_push = build_push;
+    return dtb_block_create(&d, out);
+}
+
+int dtb_block_destroy(dtb_block* b)
+{
+    destroy_block(b);
+    return DTB_OK;
+}
+
+int dtb_block_set_stream(dtb_block* b, void* stream)
+{
+    if (!b) return fail(DTB_ERR_ARG, "null handle");
+    DeviceGuard g(b->device);
+    if (b->stream != (cudaStream_t)stream) {
+        for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+    }
+    b->stream = (cudaStream_t)stream;
+    return DTB_OK;
+}
+
+int dtb_block_synchronize(dtb_block* b)
+{
+    if (!b) return fail(DTB_ERR_ARG, "null handle");
+    DeviceGuard g(b->device);
+    CK(cudaStreamSynchronize(b->stream));
+    return DTB_OK;
+}
+
+int dtb_block_get_info(const dtb_block* b, dtb_block_info* info)
+{
+    if (!b || !info) return fail(DTB_ERR_ARG, "null argument");
+    info->n_neurons = b->N;
+    info->n_synapses = b->S;
+    info->n_subblocks = b->n_sub;
+    info->n_classes = b->n_classes;
+    info->has_pull = b->has_pull;
+    info->has_push = b->has_push;
+    info->device_bytes = b->dev_bytes;
+    info->max_outdegree = b->max_out;
+    info->max_indegree = b->max_in;
+    return DTB_OK;
+}
+
+int dtb_block_run(dtb_block* b, int n_steps, float noise_rate, int isolated, int mode, float* sum_out,
+                  float* mean_out, uint32_t* nact_out, int where)
+{
+    if (!b) return fail(DTB_ERR_ARG, "null handle");
+    if (n_steps < 0) return fail(DTB_ERR_ARG, "n_steps < 0");
+    if (mode < DTB_MODE_AUTO || mode > DTB_MODE_PULL) return fail(DTB_ERR_ARG, "bad mode %d", mode);
+    if (where != DTB_HOST && where != DTB_DEVICE) return fail(DTB_ERR_ARG, "bad where");
+    if (!b->has_pull && !b->has_push) return fail(DTB_ERR_STATE, "network has no synapse tables");
+    DeviceGuard g(b->device);
+    b->override_pending = false;
+    int64_t done = 0;
+    while (done < n_steps) {
+        const int m = choose_mode(b, mode);
+        const uint32_t cap = b->stats_cap;
+        int n = (int)std::min<int64_t>(n_steps - done, (int64_t)std::min<uint32_t>(cap, (uint32_t)b->chunk));
+        RET(set_run_params(b, noise_rate, isolated));
+        RET(enqueue_chunk(b, n, m));
+        b->steps += (uint64_t)n;
+        std::vector<uint32_t> nact;
+        const bool want_nact = (mode == DTB_MODE_AUTO);
+        RET(emit_stats(b, n, done, sum_out, mean_out, nact_out, where, want_nact ? &nact : nullptr));
+        if (want_nact && n > 0) {
+            double tot = 0.0;
+            for (uint32_t v : nact) tot += v;
+            b->last_frac = tot / ((double)n * (double)std::max<int64_t>(1, b->N));
+        }
+        done += n;
+    }
+    return DTB_OK;
+}
+
+int dtb_block_step_forced(dtb_block* b, float noise_rate, int isolated, int mode, const uint8_t* forced_active,
+                          const uint8_t* forced_new_active, float* sum_out, float* mean_out, int where)
+{
+    if (!b) return fail(DTB_ERR_ARG, "null handle");
+    DeviceGuard g(b->device);
+    b->override_pending = false;
+    DevState s = b->ds;
+    const uint8_t* src[2] = {forced_active, forced_new_active};
+    for (int k = 0; k < 2; ++k) {
+        if (!src[k]) continue;
+        if (!b->d_forced[k]) RET(dalloc(b, &b->d_forced[k], (size_t)s.n_words));
+        if (!b->d_u8) RET(dalloc(b, &b->d_u8, (size_t)b->N));
+        if (where == DTB_HOST) CK(cudaMemcpyAsync(b->d_u8, src[k], (size_t)b->N, cudaMemcpyHostToDevice, b->stream));
+        else CK(cudaMemcpyAsync(b->d_u8, src[k], (size_t)b->N, cudaMemcpyDeviceToDevice, b->stream));
+        k_u8_to_bits<<<grid_for(s.n_words, 256), 256, 0, b->stream>>>(b->d_u8, b->N, b->d_forced[k], s.n_words);
+        CK(cudaGetLastError());
+    }
+    s.forced_active = forced_active ? b->d_forced[0] : nullptr;
+    s.forced_new = forced_new_active ? b->d_forced[1] : nullptr;
+    RET(set_run_params(b, noise_rate, isolated));
+    const int m = choose_mode(b, mode);
+    RET(launch_update(b, s, false, true));
+    if (m == DTB_MODE_PUSH) RET(launch_scatter(b, s));
+    else RET(launch_gather_only(b, s));
+    b->steps += 1;
+    RET(emit_stats(b, 1, 0, sum_out, mean_out, nullptr, where, nullptr));
+    CK(cudaStreamSynchronize(b->stream));
+    return DTB_OK;
+}
+
+int dtb_block_get(dtb_block* b, int field, void* dst, int where)
+{
+    if (!b || !dst) return fail(DTB_ERR_ARG, "null argument");
+    if (where != DTB_HOST && where != DTB_DEVICE) return fail(DTB_ERR_ARG, "bad where");
+    DeviceGuard g(b->device);
+    const DevState& s = b->ds;
+    const int64_t N = b->N;
+    auto export_buf = [&](void** p) -> int {
+        if (where == DTB_DEVICE) { *p = dst; return DTB_OK; }
+        if (!b->d_export) RET(dalloc(b, &b->d_export, (size_t)N * 4));
+        *p = b->d_export;
+        return DTB_OK;
+    };
+    switch (field) {
+    case DTB_FIELD_V: return copy_out(b, dst, s.V, sizeof(float) * N, where);
+    case DTB_FIELD_T_LAST: return copy_out(b, dst, s.tlast, sizeof(float) * N, where);
+    case DTB_FIELD_J: {
+        void* p; RET(export_buf(&p));
+        k_export_J<<<grid_for(N, 256), 256, 0, b->stream>>>(s, (float*)p);
+        CK(cudaGetLastError());
+        if (where == DTB_HOST) return copy_out(b, dst, p, sizeof(float) * 4 * N, where);
+        return DTB_OK;
+    }
+    case DTB_FIELD_I_UI:
+    case DTB_FIELD_I_SYN: {
+        if (b->override_pending) {
+            if (field == DTB_FIELD_I_SYN) return copy_out(b, dst, s.isyn_override, sizeof(float) * N, where);
+            return copy_out(b, dst, b->d_iui_override, sizeof(float) * 4 * N, where);
+        }
+        void* p; RET(export_buf(&p));
+        if (field == DTB_FIELD_I_UI) k_export_current<<<grid_for(N, 256), 256, 0, b->stream>>>(s, (float*)p, nullptr);
+        else k_export_current<<<grid_for(N, 256), 256, 0, b->stream>>>(s, nullptr, (float*)p);
+        CK(cudaGetLastError());
+        if (where == DTB_HOST) return copy_out(b, dst, p, sizeof(float) * (field == DTB_FIELD_I_UI ? 4 : 1) * N, where);
+        return DTB_OK;
+    }
+    case DTB_FIELD_ACTIVE:
+    case DTB_FIELD_NEW_ACTIVE: {
+        const uint32_t* bits = field == DTB_FIELD_ACTIVE ? s.abits : s.bits[(b->steps + 1) & 1];
+        void* p; RET(export_buf(&p));
+        k_bits_to_u8<<<grid_for(N, 256), 256, 0, b->stream>>>(bits, N, (uint8_t*)p);
+        CK(cudaGetLastError());
+        if (where == DTB_HOST) return copy_out(b, dst, p, (size_t)N, where);
+        return DTB_OK;
+    }
+    case DTB_FIELD_T: return copy_out(b, dst, &s.ctl->t, sizeof(float), where);
+    case DTB_FIELD_STEP: {
+        if (where == DTB_HOST) { std::memcpy(dst, &b->steps, sizeof(uint64_t)); return DTB_OK; }
+        return copy_out(b, dst, &s.ctl->steps_done, sizeof(uint64_t), where);
+    }
+    case DTB_FIELD_SUB_COUNT:
+        if (where == DTB_HOST) { if (b->n_sub) std::memcpy(dst, b->sub_count.data(), sizeof(uint32_t) * b->n_sub); return DTB_OK; }
+        return copy_out(b, dst, s.sub_count, sizeof(uint32_t) * b->n_sub, where);
+    default: return fail(DTB_ERR_ARG, "unknown field %d", field);
+    }
+}
+
+int dtb_block_get_csr(dtb_block* b, int which, int64_t* rowptr, uint32_t* index, float* weight, int where)
+{
+    if (!b || (which != 0 && which != 1)) return fail(DTB_ERR_ARG, "bad argument");
+    if ((which == 0 && !b->has_pull) || (which == 1 && !b->has_push)) return fail(DTB_ERR_STATE, "CSR not built");
+    DeviceGuard g(b->device);
+    const int64_t* r = which ? b->ds.qrow : b->ds.prow;
+    const uint32_t* c = which ? b->ds.qcol : b->ds.pcol;
+    const float2* w = which ? b->ds.qw : b->ds.pw;
+    if (rowptr) RET(copy_out(b, rowptr, r, sizeof(int64_t) * (size_t)(b->N + 1), where));
+    if (index) RET(copy_out(b, index, c, sizeof(uint32_t) * (size_t)b->S, where));
+    if (weight) RET(copy_out(b, weight, w, sizeof(float2) * (size_t)b->S, where));
+    return DTB_OK;
+}
+
+int dtb_block_set(dtb_block* b, int field, const void* src, int where)
+{
+    if (!b || !src) return fail(DTB_ERR_ARG, "null argument");
+    DeviceGuard g(b->device);
+    const DevState& s = b->ds;
+    const int64_t N = b->N;
+    const cudaMemcpyKind k = where == DTB_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    switch (field) {
+    case DTB_FIELD_V: CK(cudaMemcpyAsync(s.V, src, sizeof(float) * N, k, b->stream)); break;
+    case DTB_FIELD_T_LAST: CK(cudaMemcpyAsync(s.tlast, src, sizeof(float) * N, k, b->stream)); break;
+    case DTB_FIELD_J: {
+        if (!b->d_export) RET(dalloc(b, &b->d_export, (size_t)N * 4));
+        CK(cudaMemcpyAsync(b->d_export, src, sizeof(float) * 4 * N, k, b->stream));
+        k_J_from_planar<<<grid_for(N, 256), 256, 0, b->stream>>>(s, b->d_export);
+        CK(cudaGetLastError());
+        break;
+    }
+    case DTB_FIELD_T: CK(cudaMemcpyAsync(&s.ctl->t, src, sizeof(float), k, b->stream)); break;
+    case DTB_FIELD_STEP: {
+        uint64_t v;
+        if (where == DTB_HOST) std::memcpy(&v, src, 8);
+        else CK(cudaMemcpy(&v, src, 8, cudaMemcpyDeviceToHost));
+        b->steps = v;
+        CK(cudaMemcpyAsync(&s.ctl->steps_done, &b->steps, sizeof(uint64_t), cudaMemcpyHostToDevice, b->stream));
+        break;
+    }
+    default: return fail(DTB_ERR_ARG, "field %d cannot be set", field);
+    }
+    CK(cudaStreamSynchronize(b->stream));
+    return DTB_OK;
+}
+
+int dtb_block_update_property(dtb_block* b, const float* property, const float* decay)
+{
+    if (!b || !property) return fail(DTB_ERR_ARG, "null argument");
+    DeviceGuard g(b->device);
+    DevState& s = b->ds;
+    // keep the current synaptic current (computed with the old parameters)
+    if (!b->override_pending) {
+        if (!b->d_iui_override) RET(dalloc(b, &b->d_iui_override, (size_t)b->N * 4));
+        k_export_current<<<grid_for(b->N, 256), 256, 0, b->stream>>>(s, b->d_iui_override, s.isyn_override);
+        CK(cudaGetLastError());
+        const uint32_t one = 1u;
+        CK(cudaMemcpyAsync(&s.ctl->use_isyn_override, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
+    }
+    std::vector<uint32_t> cls;
+    RET(build_classes(b, b->N, property, decay, cls));
+    RET(upload_class_tables(b));
+    CK(cudaMemcpy(const_cast<uint32_t*>(s.cls), cls.data(), sizeof(uint32_t) * (size_t)b->N, cudaMemcpyHostToDevice));
+    if (!s.st_spk) RET(ensure_stats(b, 256));
+    b->class_prop_base.clear();
+    for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+    b->override_pending = true;
+    return DTB_OK;
+}
+
+int dtb_block_scale_property_by_subblock(dtb_block* b, int n, const int32_t* sub, const int32_t* col, const float* value)
+{
+    if (!b || n < 0 || (n > 0 && (!sub || !col || !value))) return fail(DTB_ERR_ARG, "bad argument");
+    DeviceGuard g(b->device);
+    if (b->class_prop_base.empty()) b->class_prop_base = b->class_prop;
+    for (int i = 0; i < n; ++i) {
+        if (col[i] < 0 || col[i] >= DTB_NPROP || col[i] == 3) return fail(DTB_ERR_ARG, "column %d cannot be scaled", col[i]);
+    }
+    for (int i = 0; i < n; ++i) {
+        for (int c = 0; c < b->n_classes; ++c) {
+            if (b->classes[(size_t)c].sub != sub[i]) continue;
+            auto& row = b->class_prop[(size_t)c];
+            volatile float v = b->class_prop_base[(size_t)c][(size_t)col[i]] * value[i];
+            row[(size_t)col[i]] = v;
+            float dc[4] = {b->class_decay[(size_t)c][0], b->class_decay[(size_t)c][1], b->class_decay[(size_t)c][2],
+                           b->class_decay[(size_t)c][3]};
+            if (col[i] >= 18) { default_decay(row.data(), b->dt, dc); b->class_decay[(size_t)c] = {dc[0], dc[1], dc[2], dc[3]}; }
+            ParamClass p = make_class(row.data(), dc, b->dt);
+            p.sub = b->classes[(size_t)c].sub;
+            b->classes[(size_t)c] = p;
+        }
+    }
+    CK(cudaMemcpyAsync(const_cast<ParamClass*>(b->ds.pc), b->classes.data(), sizeof(ParamClass) * b->classes.size(),
+                       cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    return DTB_OK;
+}
+
+int dtb_block_update_conn_weight(dtb_block* b, int64_t n, const uint8_t* channel, const uint32_t* post,
+                                 const uint32_t* pre, const float* value)
+{
+    if (!b || n < 0 || (n > 0 && (!channel || !post || !pre || !value))) return fail(DTB_ERR_ARG, "bad argument");
+    if (n == 0) return DTB_OK;
+    for (int64_t i = 0; i < n; ++i)
+        if (channel[i] > 3) return fail(DTB_ERR_ARG, "channel must be 0..3");
+    DeviceGuard g(b->device);
+    uint8_t* dch = nullptr; uint32_t* dpo = nullptr; uint32_t* dpr = nullptr; float* dv = nullptr; unsigned* miss = nullptr;
+    cudaError_t e = cudaMalloc(&dch, (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&dpo, 4 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&dpr, 4 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&dv, 4 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&miss, 4);
+    unsigned hmiss = 0;
+    if (e == cudaSuccess) {
+        cudaMemcpy(dch, channel, (size_t)n, cudaMemcpyHostToDevice);
+        cudaMemcpy(dpo, post, 4 * (size_t)n, cudaMemcpyHostToDevice);
+        cudaMemcpy(dpr, pre, 4 * (size_t)n, cudaMemcpyHostToDevice);
+        cudaMemcpy(dv, value, 4 * (size_t)n, cudaMemcpyHostToDevice);
+        cudaMemset(miss, 0, 4);
+        k_update_weight<<<grid_for(n, 128), 128, 0, b->stream>>>(b->ds, n, dch, dpo, dpr, dv,
+                                                                const_cast<float2*>(b->ds.pw),
+                                                                const_cast<float2*>(b->ds.qw), miss);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        if (e == cudaSuccess) e = cudaMemcpy(&hmiss, miss, 4, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(dch); cudaFree(dpo); cudaFree(dpr); cudaFree(dv); cudaFree(miss);
+    if (e != cudaSuccess) return fail(DTB_ERR_CUDA, "update_conn_weight: %s", cudaGetErrorString(e));
+    if (hmiss) return fail(DTB_ERR_ARG, "update_conn_weight: %u synapses not found", hmiss);
+    return DTB_OK;
+}
+
+// Checkpoint format: "DTBCKPT1", N (i64), steps (u64), t (f32), override flag (u32),
+// then V[N], J[N] float4, t_last[N], and I_syn override[N] if the flag is set.
+int dtb_block_save(dtb_block* b, const char* path)
+{
+    if (!b || !path) return fail(DTB_ERR_ARG, "null argument");
+    DeviceGuard g(b->device);
+    const int64_t N = b->N;
+    std::vector<float> V((size_t)N), T((size_t)N), I((size_t)N);
+    std::vector<float4> J((size_t)N);
+    float t = 0.0f;
+    CK(cudaStreamSynchronize(b->stream));
+    CK(cudaMemcpy(V.data(), b->ds.V, 4 * N, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(J.data(), b->ds.J, 16 * N, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(T.data(), b->ds.tlast, 4 * N, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&t, &b->ds.ctl->t, 4, cudaMemcpyDeviceToHost));
+    const uint32_t ov = b->override_pending ? 1u : 0u;
+    if (ov) CK(cudaMemcpy(I.data(), b->ds.isyn_override, 4 * N, cudaMemcpyDeviceToHost));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(DTB_ERR_IO, "cannot write %s", path);
+    bool ok = std::fwrite("DTBCKPT1", 1, 8, f) == 8;
+    ok = ok && std::fwrite(&N, 8, 1, f) == 1 && std::fwrite(&b->steps, 8, 1, f) == 1 && std::fwrite(&t, 4, 1, f) == 1 &&
+         std::fwrite(&ov, 4, 1, f) == 1;
+    ok = ok && std::fwrite(V.data(), 4, (size_t)N, f) == (size_t)N;
+    ok = ok && std::fwrite(J.data(), 16, (size_t)N, f) == (size_t)N;
+    ok = ok && std::fwrite(T.data(), 4, (size_t)N, f) == (size_t)N;
+    if (ov) ok = ok && std::fwrite(I.data(), 4, (size_t)N, f) == (size_t)N;
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(DTB_ERR_IO, "write failed: %s", path);
+    return DTB_OK;
+}
+
+int dtb_block_load(dtb_block* b, const char* path)
+{
+    if (!b || !path) return fail(DTB_ERR_ARG, "null argument");
+    DeviceGuard g(b->device);
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(DTB_ERR_IO, "cannot read %s", path);
+    char magic[8];
+    int64_t N = 0;
+    uint64_t steps = 0;
+    float t = 0.0f;
+    uint32_t ov = 0;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "DTBCKPT1", 8) == 0;
+    ok = ok && std::fread(&N, 8, 1, f) == 1 && std::fread(&steps, 8, 1, f) == 1 && std::fread(&t, 4, 1, f) == 1 &&
+         std::fread(&ov, 4, 1, f) == 1;
+    if (!ok || N != b->N || ov > 1) { std::fclose(f); return fail(DTB_ERR_FORMAT, "%s is not a checkpoint of this network", path); }
+    std::vector<float> V((size_t)N), T((size_t)N), I((size_t)N);
+    std::vector<float4> J((size_t)N);
+    ok = std::fread(V.data(), 4, (size_t)N, f) == (size_t)N && std::fread(J.data(), 16, (size_t)N, f) == (size_t)N &&
+         std::fread(T.data(), 4, (size_t)N, f) == (size_t)N;
+    if (ok && ov) ok = std::fread(I.data(), 4, (size_t)N, f) == (size_t)N;
+    std::fclose(f);
+    if (!ok) return fail(DTB_ERR_FORMAT, "truncated checkpoint %s", path);
+    CK(cudaStreamSynchronize(b->stream));
+    CK(cudaMemcpy(b->ds.V, V.data(), 4 * N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->ds.J, J.data(), 16 * N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->ds.tlast, T.data(), 4 * N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(&b->ds.ctl->t, &t, 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(&b->ds.ctl->steps_done, &steps, 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(&b->ds.ctl->use_isyn_override, &ov, 4, cudaMemcpyHostToDevice));
+    if (ov) CK(cudaMemcpy(b->ds.isyn_override, I.data(), 4 * N, cudaMemcpyHostToDevice));
+    b->steps = steps;
+    b->override_pending = false;
+    return DTB_OK;
+}
+
+// ------------------------------------------------------------ BOLD (standalone)
+static int bold_init_state(dtb_bold* m)
+{
+    const int64_t R = m->R;
+    const unsigned gr = grid_for(R, 256);
+    if (m->dtype == 0) {
+        k_fill<float><<<gr, 256, 0, m->stream>>>((float*)m->s, R, 0.0f);
+        k_fill<float><<<gr, 256, 0, m->stream>>>((float*)m->q, R, 0.0f);
+        k_fill<float><<<gr, 256, 0, m->stream>>>((float*)m->v, R, 1.0f);
+        k_fill<float><<<gr, 256, 0, m->stream>>>((float*)m->f, R, 1.0f);
+    } else {
+        k_fill<double><<<gr, 256, 0, m->stream>>>((double*)m->s, R, 0.0);
+        k_fill<double><<<gr, 256, 0, m->stream>>>((double*)m->q, R, 0.0);
+        k_fill<double><<<gr, 256, 0, m->stream>>>((double*)m->v, R, 1.0);
+        k_fill<double><<<gr, 256, 0, m->stream>>>((double*)m->f, R, 1.0);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(m->stream));
+    return DTB_OK;
+}
+
+static void bold_free(dtb_bold* m)
+{
+    if (!m) return;
+    DeviceGuard g(m->device);
+    void* ps[] = {m->s, m->q, m->v, m->f, m->tmp_u, m->tmp_o, m->tmp_w};
+    for (void* p : ps) if (p) cudaFree(p);
+    delete m;
+}
+
+int dtb_bold_create(int64_t n_regions, int dtype, double epsilon, double tao_s, double tao_f, double tao_0, double alpha,
+                    double E_0, double V_0, double delta_t, int device, dtb_bold** out)
+{
+    if (!out || n_regions <= 0 || (dtype != 0 && dtype != 1)) return fail(DTB_ERR_ARG, "bad argument");
+    *out = nullptr;
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(DTB_ERR_ARG, "device out of range");
+    DeviceGuard g(device);
+    dtb_bold* m = new dtb_bold();
+    m->device = device; m->R = n_regions; m->dtype = dtype;
+    m->eps = epsilon; m->ts = tao_s; m->tf = tao_f; m->t0 = tao_0; m->alpha = alpha; m->E0 = E_0; m->V0 = V_0; m->dt = delta_t;
+    const size_t el = dtype ? 8 : 4;
+    void** ps[] = {&m->s, &m->q, &m->v, &m->f, &m->tmp_u, &m->tmp_o};
+    for (void** p : ps) {
+        if (cudaMalloc(p, el * (size_t)n_regions) != cudaSuccess) {
+            cudaGetLastError();
+            bold_free(m);
+            return fail(DTB_ERR_NOMEM, "BOLD state allocation failed");
+        }
+    }
+    int rc = bold_init_state(m);
+    if (rc != DTB_OK) { bold_free(m); return rc; }
+    *out = m;
+    return DTB_OK;
+}
+
+int dtb_bold_destroy(dtb_bold* m)
+{
+    bold_free(m);
+    return DTB_OK;
+}
+
+int dtb_bold_set_stream(dtb_bold* m, void* stream)
+{
+    if (!m) return fail(DTB_ERR_ARG, "null handle");
+    m->stream = (cudaStream_t)stream;
+    return DTB_OK;
+}
+
+int dtb_bold_run(dtb_bold* m, const void* u, void* out, int where)
+{
+    if (!m || !u || !out) return fail(DTB_ERR_ARG, "null argument");
+    DeviceGuard g(m->device);
+    const size_t bytes = (m->dtype ? 8 : 4) * (size_t)m->R;
+    const void* du = u;
+    void* dout = out;
+    if (where == DTB_HOST) {
+        CK(cudaMemcpyAsync(m->tmp_u, u, bytes, cudaMemcpyHostToDevice, m->stream));
+        du = m->tmp_u;
+        dout = m->tmp_o;
+    }
+    const unsigned gr = grid_for(m->R, 128);
+    if (m->dtype == 0)
+        k_bold_run<float><<<gr, 128, 0, m->stream>>>(m->R, (const float*)du, (float*)m->s, (float*)m->q, (float*)m->v,
+                                                     (float*)m->f, (float*)dout, bold_scalars<float>(m));
+    else
+        k_bold_run<double><<<gr, 128, 0, m->stream>>>(m->R, (const double*)du, (double*)m->s, (double*)m->q,
+                                                      (double*)m->v, (double*)m->f, (double*)dout,
+                                                      bold_scalars<double>(m));
+    CK(cudaGetLastError());
+    if (where == DTB_HOST) {
+        CK(cudaMemcpyAsync(out, m->tmp_o, bytes, cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+    }
+    return DTB_OK;
+}
+
+int dtb_bold_state_update(dtb_bold* m, const void* w, int64_t E, int64_t Rp, int64_t S, int where)
+{
+    if (!m || !w) return fail(DTB_ERR_ARG, "null argument");
+    if (E * Rp != m->R || S < 4) return fail(DTB_ERR_ARG, "state_update: w must be [E][R/E][>=4] with E*Rp == R");
+    DeviceGuard g(m->device);
+    const size_t el = m->dtype ? 8 : 4;
+    const size_t bytes = el * (size_t)m->R * (size_t)S;
+    const void* dw = w;
+    if (where == DTB_HOST) {
+        if (m->tmp_w_bytes < bytes) {
+            if (m->tmp_w) cudaFree(m->tmp_w);
+            m->tmp_w = nullptr;
+            m->tmp_w_bytes = 0;
+            CK(cudaMalloc(&m->tmp_w, bytes));
+            m->tmp_w_bytes = bytes;
+        }
+        CK(cudaMemcpyAsync(m->tmp_w, w, bytes, cudaMemcpyHostToDevice, m->stream));
+        dw = m->tmp_w;
+    }
+    const unsigned gr = grid_for(m->R, 128);
+    if (m->dtype == 0)
+        k_bold_state_update<float><<<gr, 128, 0, m->stream>>>(m->R, S, (const float*)dw, (float*)m->s, (float*)m->q,
+                                                              (float*)m->v, (float*)m->f, 1e-05f);
+    else
+        k_bold_state_update<double><<<gr, 128, 0, m->stream>>>(m->R, S, (const double*)dw, (double*)m->s,
+                                                               (double*)m->q, (double*)m->v, (double*)m->f, 1e-05);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(m->stream));
+    return DTB_OK;
+}
+
+int dtb_bold_get(dtb_bold* m, int field, void* dst, int where)
+{
+    if (!m || !dst || field < 0 || field > 3) return fail(DTB_ERR_ARG, "bad argument");
+    DeviceGuard g(m->device);
+    void* src[4] = {m->s, m->q, m->v, m->f};
+    const size_t bytes = (m->dtype ? 8 : 4) * (size_t)m->R;
+    CK(cudaMemcpyAsync(dst, src[field], bytes, where == DTB_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                       m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return DTB_OK;
+}
+
+int dtb_bold_set(dtb_bold* m, int field, const void* srcp, int where)
+{
+    if (!m || !srcp || field < 0 || field > 3) return fail(DTB_ERR_ARG, "bad argument");
+    DeviceGuard g(m->device);
+    void* dst[4] = {m->s, m->q, m->v, m->f};
+    const size_t bytes = (m->dtype ? 8 : 4) * (size_t)m->R;
+    CK(cudaMemcpyAsync(dst[field], srcp, bytes, where == DTB_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                       m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return DTB_OK;
+}
+
+// ------------------------------------------------------------ block-attached BOLD
+int dtb_block_attach_bold(dtb_block* b, int n_regions, const int32_t* sub_to_region, double epsilon, double tao_s,
+                          double tao_f, double tao_0, double alpha, double E_0, double V_0)
+{
+    if (!b || n_regions <= 0 || !sub_to_region) return fail(DTB_ERR_ARG, "bad argument");
+    DeviceGuard g(b->device);
+    std::vector<double> rn((size_t)n_regions, 0.0);
+    for (int i = 0; i < b->n_sub; ++i) {
+        const int r = sub_to_region[i];
+        if (r >= n_regions) return fail(DTB_ERR_ARG, "sub_to_region[%d] = %d out of range", i, r);
+        if (r >= 0) rn[(size_t)r] += (double)b->sub_count[(size_t)i];
+    }
+    BoldDev& bd = b->ds.bold;
+    int32_t* sr = nullptr; double* drn = nullptr; double* st = nullptr;
+    RET(dalloc(b, &sr, (size_t)std::max(1, b->n_sub)));
+    RET(dalloc(b, &drn, (size_t)n_regions));
+    RET(dalloc(b, &st, (size_t)n_regions * 6));
+    if (b->n_sub) CK(cudaMemcpy(sr, sub_to_region, sizeof(int32_t) * b->n_sub, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(drn, rn.data(), sizeof(double) * n_regions, cudaMemcpyHostToDevice));
+    std::vector<double> init((size_t)n_regions * 6, 0.0);
+    for (int r = 0; r < n_regions; ++r) { init[(size_t)(2 * n_regions + r)] = 1.0; init[(size_t)(3 * n_regions + r)] = 1.0; }
+    CK(cudaMemcpy(st, init.data(), sizeof(double) * init.size(), cudaMemcpyHostToDevice));
+    bd.n_regions = n_regions;
+    bd.sub_region = sr;
+    bd.region_n = drn;
+    bd.s = st; bd.q = st + n_regions; bd.v = st + 2 * n_regions; bd.f = st + 3 * n_regions;
+    bd.act = st + 4 * n_regions; bd.out = st + 5 * n_regions;
+    bd.epsilon = epsilon; bd.tao_s = tao_s; bd.tao_f = tao_f; bd.tao_0 = tao_0; bd.div_alpha = 1.0 / alpha;
+    bd.E0 = E_0; bd.V0 = V_0; bd.delta_t = (double)b->dt / 1000.0;
+    b->bold_R = n_regions;
+    for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+    return DTB_OK;
+}
+
+int dtb_block_get_bold(dtb_block* b, int field, double* dst, int where)
+{
+    if (!b || !dst || field < 0 || field > 5) return fail(DTB_ERR_ARG, "bad argument");
+    if (b->bold_R == 0) return fail(DTB_ERR_STATE, "no BOLD model attached");
+    DeviceGuard g(b->device);
+    const BoldDev& bd = b->ds.bold;
+    const double* src[6] = {bd.s, bd.q, bd.v, bd.f, bd.out, bd.act};
+    return copy_out(b, dst, src[field], sizeof(double) * b->bold_R, where);
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// Device-side data structures and helpers shared by the kernels of libdtb.
+//
+// Layout in HBM (one network = one handle):
+//   V[N] f32, J[N] float4 {AMPA, NMDA, GABAa, GABAb}, t_last[N] f32,
+//   cls[N] u32 -> ParamClass table (deduplicated property rows),
+//   spike bitmasks: new_active (double buffered by step parity) and active,
+//   ceil(N/128)*4 words each (one warp owns 128 neurons = 4 words),
+//   pull CSR: prow[N+1] i64, pcol[S] u32 (pre | bit31 = GABA pair), pw[S] float2,
+//   push CSR: qrow[N+1] i64, qcol[S] u32 (post | bit31 = GABA pair), qw[S] float2.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dtb {
+
+constexpr uint32_t kKindBit = 0x80000000u;
+constexpr uint32_t kIndexMask = 0x7fffffffu;
+constexpr int kWarpNeurons = 128;      // neurons owned by one warp in the step kernels
+constexpr int kStepThreads = 256;      // 8 warps, 1024 neurons per CTA
+
+// One deduplicated row of the 22-column property matrix
+// (generation/make_block.py:394-432) with the derived constants the step uses.
+struct __align__(16) ParamClass {
+    float4 g;       // g_ui           cols 10-13
+    float4 Vu;      // V_ui           cols 14-17
+    float4 decay;   // exp(-dt/tau_ui), tau cols 18-21
+    float gL;       // col 6
+    float VL;       // col 7
+    float rCdt;     // (1/C) * dt, C col 4 (torch: C.reciprocal() * dt)
+    float Vth;      // col 8
+    float Vreset;   // col 9
+    float Tref;     // col 5
+    float Iext;     // col 2
+    float noise;    // col 0 (per-neuron noise rate, cuda/src/stage/spike.cpp:157)
+    int32_t sub;    // col 3 (subblock index)
+    float C;        // col 4
+    float pad0, pad1;
+};
+static_assert(sizeof(ParamClass) == 96, "ParamClass layout");
+
+// Control block in device memory; read by every step kernel, advanced by the
+// last CTA of each update kernel.
+struct Ctl {
+    unsigned long long steps_done;   // number of completed updates (Philox step counter)
+    // per-run parameters, written by the host as one 16-byte copy
+    unsigned long long run_base;     // steps_done at the start of the current run (stats row 0)
+    float noise_rate;                // >= 0: scalar rate; < 0: per-class rate
+    int32_t isolated;                // block.run(isolated=...)
+    float t;                         // block.t after the last update (float32 accumulation)
+    uint32_t done;                   // CTAs finished in the current update kernel
+    uint32_t stats_cap;              // rows of the per-step stats buffers
+    uint32_t use_isyn_override;      // next update takes I_syn from isyn_override
+    uint32_t err;                    // sticky error flags
+    uint32_t pad;
+};
+static_assert(sizeof(Ctl) == 48, "Ctl layout");
+
+struct RunParams {
+    unsigned long long run_base;
+    float noise_rate;
+    int32_t isolated;
+};
+static_assert(sizeof(RunParams) == 16, "RunParams layout");
+
+struct BoldDev {
+    int n_regions;               // 0: no BOLD attached
+    const int32_t* sub_region;   // [n_sub] -> region or -1
+    const double* region_n;      // [R] neurons in region
+    double* s; double* q; double* v; double* f; double* act; double* out;   // [R]
+    double epsilon, tao_s, tao_f, tao_0, div_alpha, E0, V0, delta_t;
+};
+
+struct DevState {
+    int64_t N;
+    int64_t n_words;            // bitmask words (multiple of 4)
+    float* V;
+    float4* J;
+    float* tlast;
+    float* isyn_override;       // [N] used once after update_property
+    const uint32_t* cls;
+    const ParamClass* pc;
+    uint32_t* bits[2];          // new_active bitmask by step parity
+    uint32_t* abits;            // active bitmask of the latest update
+    const uint32_t* forced_active;   // teacher forcing bitmasks (nullable)
+    const uint32_t* forced_new;
+    // pull CSR
+    const int64_t* prow; const uint32_t* pcol; const float2* pw;
+    // push CSR
+    const int64_t* qrow; const uint32_t* qcol; const float2* qw;
+    // statistics
+    int n_sub;
+    uint32_t* sub_spk;          // [n_sub] accumulators (active)
+    uint32_t* sub_nact;         // [n_sub] accumulators (new_active)
+    double* sub_vsum;           // [n_sub]
+    const uint32_t* sub_count;  // [n_sub] neurons per subblock
+    uint32_t* unmapped_nact;    // new_active of neurons whose subblock is out of range
+    float* st_spk;              // [stats_cap][n_sub]
+    float* st_mean;             // [stats_cap][n_sub]
+    uint32_t* st_nact;          // [stats_cap]
+    Ctl* ctl;
+    uint64_t seed;
+    uint32_t stream_id;
+    float dt;
+    BoldDev bold;
+};
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10, Salmon, Moraes, Dror & Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11 (round function and Weyl key schedule of the paper).
+struct U4 { uint32_t x, y, z, w; };
+
+__host__ __device__ __forceinline__ void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo)
+{
+#ifdef __CUDA_ARCH__
+    hi = __umulhi(a, b);
+    lo = a * b;
+#else
+    uint64_t p = (uint64_t)a * (uint64_t)b;
+    hi = (uint32_t)(p >> 32);
+    lo = (uint32_t)p;
+#endif
+}
+
+__host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo32(0xD2511F53u, c.x, hi0, lo0);
+        mulhilo32(0xCD9E8D57u, c.z, hi1, lo1);
+        U4 n;
+        n.x = hi1 ^ c.y ^ k0;
+        n.y = lo1;
+        n.z = hi0 ^ c.w ^ k1;
+        n.w = lo0;
+        c = n;
+    }
+    return c;
+}
+
+// 24-bit uniform in [0,1), exact in float32.
+__host__ __device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+
+}  // namespace dtb

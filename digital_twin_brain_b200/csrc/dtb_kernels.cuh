@@ -1,0 +1,768 @@
+// Kernels of libdtb (sm_100a).
+//
+// Step pipeline of one time step k (models/block.py:116-150):
+//   update_k  : I_syn(V,J) -> V, threshold, refractory, Philox noise,
+//               bitmask of spikes|noise, J <- J*decay (pending), stats.
+//   propagate : push  — k_scatter: every set bit of the bitmask scatters its
+//               outgoing row with float2 atomics into the pending J;
+//               pull  — k_step<GATHER>: every postsynaptic row sums the
+//               weights of its firing presynaptic neurons in row order
+//               (torch.sparse.mm's order, bit-identical) and adds them to
+//               the pending J.  The pull gather of step k is fused with the
+//               update of step k+1 (k_step<true,true>), so a run of n pull
+//               steps is update, n-1 fused kernels and one gather-only kernel.
+// The last CTA of every update kernel folds the per-subblock statistics,
+// runs the per-region BOLD step when one is attached, and advances the
+// device clock (steps_done, t) — no extra launch per step.
+#pragma once
+
+#include "dtb_device.cuh"
+
+namespace dtb {
+
+// ------------------------------------------------------------ neuron math
+// Operation order of models/block.py:83-111 with round-to-nearest float32
+// intrinsics so that no multiply-add is contracted.
+
+__device__ __forceinline__ float isyn_of(const ParamClass& p, float v, float4 J)
+{
+    const float i0 = __fmul_rn(__fmul_rn(p.g.x, __fsub_rn(p.Vu.x, v)), J.x);
+    const float i1 = __fmul_rn(__fmul_rn(p.g.y, __fsub_rn(p.Vu.y, v)), J.y);
+    const float i2 = __fmul_rn(__fmul_rn(p.g.z, __fsub_rn(p.Vu.z, v)), J.z);
+    const float i3 = __fmul_rn(__fmul_rn(p.g.w, __fsub_rn(p.Vu.w, v)), J.w);
+    return __fadd_rn(__fadd_rn(__fadd_rn(i0, i1), i2), i3);
+}
+
+__device__ __forceinline__ float4 iui_of(const ParamClass& p, float v, float4 J)
+{
+    return make_float4(__fmul_rn(__fmul_rn(p.g.x, __fsub_rn(p.Vu.x, v)), J.x),
+                       __fmul_rn(__fmul_rn(p.g.y, __fsub_rn(p.Vu.y, v)), J.y),
+                       __fmul_rn(__fmul_rn(p.g.z, __fsub_rn(p.Vu.z, v)), J.z),
+                       __fmul_rn(__fmul_rn(p.g.w, __fsub_rn(p.Vu.w, v)), J.w));
+}
+
+__device__ __forceinline__ ParamClass load_class(const ParamClass* __restrict__ pc, uint32_t c)
+{
+    const float4* src = reinterpret_cast<const float4*>(pc + c);
+    ParamClass p;
+    float4* dst = reinterpret_cast<float4*>(&p);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) dst[i] = __ldg(src + i);
+    return p;
+}
+
+__device__ __forceinline__ float4 add4(float4 a, float4 b)
+{
+    return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
+}
+
+__device__ __forceinline__ float4 mul4(float4 a, float4 b)
+{
+    return make_float4(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y), __fmul_rn(a.z, b.z), __fmul_rn(a.w, b.w));
+}
+
+__device__ __forceinline__ bool test_bit(const uint32_t* __restrict__ bits, int64_t n)
+{
+    return (__ldg(bits + (n >> 5)) >> (n & 31)) & 1u;
+}
+
+// ------------------------------------------------------------ pull gather
+// Sum of the weights of row n whose presynaptic neuron is set in `bits`,
+// accumulated strictly in row order from +0 (sparse.mm order). All lanes
+// return the same value.
+__device__ __forceinline__ float4 gather_row(const DevState& s, const uint32_t* __restrict__ bits, int64_t n,
+                                             int lane)
+{
+    const int64_t e0 = __ldg(s.prow + n);
+    const int64_t e1 = __ldg(s.prow + n + 1);
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+    for (int64_t e = e0; e < e1; e += 32) {
+        const int64_t idx = e + lane;
+        const bool valid = idx < e1;
+        const uint32_t c = valid ? __ldg(s.pcol + idx) : 0u;
+        const bool act = valid && test_bit(bits, c & kIndexMask);
+        unsigned m = __ballot_sync(0xffffffffu, act);
+        float2 w = make_float2(0.0f, 0.0f);
+        if (act) w = __ldg(s.pw + idx);
+        while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const float wx = __shfl_sync(0xffffffffu, w.x, l);
+            const float wy = __shfl_sync(0xffffffffu, w.y, l);
+            const uint32_t cl = __shfl_sync(0xffffffffu, c, l);
+            if (cl & kKindBit) { a2 = __fadd_rn(a2, wx); a3 = __fadd_rn(a3, wy); }
+            else { a0 = __fadd_rn(a0, wx); a1 = __fadd_rn(a1, wy); }
+        }
+    }
+    return make_float4(a0, a1, a2, a3);
+}
+
+// ------------------------------------------------------------ epilogue
+// Runs in the last CTA of an update kernel: per-subblock statistics of step
+// `steps_done` (models/block.py:144-150), BOLD (simulation/simulation.py:
+// 269-279 + models/bold_model_pytorch.py:43-78 in float64), clock advance.
+__device__ void step_epilogue(const DevState& s, unsigned long long steps_done, float t)
+{
+    Ctl* ctl = s.ctl;
+    const unsigned long long row = steps_done - ctl->run_base;
+    const bool write = row < (unsigned long long)ctl->stats_cap;
+    __shared__ unsigned long long sh_nact;
+    if (threadIdx.x == 0) sh_nact = atomicExch(s.unmapped_nact, 0u);
+    if (s.bold.n_regions > 0)
+        for (int r = threadIdx.x; r < s.bold.n_regions; r += blockDim.x) s.bold.act[r] = 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < s.n_sub; i += blockDim.x) {
+        const uint32_t spk = atomicExch(s.sub_spk + i, 0u);
+        const uint32_t nact = atomicExch(s.sub_nact + i, 0u);
+        const unsigned long long vb =
+            atomicExch(reinterpret_cast<unsigned long long*>(s.sub_vsum + i), 0ull);
+        const double vsum = __longlong_as_double((long long)vb);
+        const uint32_t cnt = s.sub_count[i];
+        if (write) {
+            s.st_spk[row * s.n_sub + i] = (float)spk;
+            s.st_mean[row * s.n_sub + i] = cnt ? (float)(vsum / (double)cnt) : __int_as_float(0x7fc00000);
+        }
+        atomicAdd(&sh_nact, (unsigned long long)nact);
+        if (s.bold.n_regions > 0) {
+            const int r = s.bold.sub_region[i];
+            if (r >= 0) atomicAdd(s.bold.act + r, (double)spk);
+        }
+    }
+    __syncthreads();
+    if (s.bold.n_regions > 0) {
+        const BoldDev& b = s.bold;
+        for (int r = threadIdx.x; r < b.n_regions; r += blockDim.x) {
+            const double act = b.act[r] / b.region_n[r];
+            b.act[r] = act;
+            const double u = act > 1e-5 ? act : 1e-5;
+            double fi = b.f[r], si = b.s[r], qi = b.q[r], vi = b.v[r];
+            const double ds = ((b.epsilon * u) - si / b.tao_s) - (fi - 1.0) / b.tao_f;
+            const double qpart = fi > 0.0 ? (1.0 - pow(1.0 - b.E0, 1.0 / fi)) : 1.0;
+            const double dq = (((fi * qpart) / b.E0) - qi * pow(vi, b.div_alpha - 1.0)) / b.tao_0;
+            qi = qi + dq * b.delta_t;
+            const double dv = (fi - pow(vi, b.div_alpha)) / b.tao_0;
+            vi = vi + dv * b.delta_t;
+            fi = fi + si * b.delta_t;
+            fi = fi > 0.0 ? fi : 0.0;
+            si = si + ds * b.delta_t;
+            b.s[r] = si; b.q[r] = qi; b.v[r] = vi; b.f[r] = fi;
+            b.out[r] = b.V0 * ((7.0 * b.E0 * (1.0 - qi) + 2.0 * (1.0 - qi / vi)) + (2.0 * b.E0 - 0.2) * (1.0 - vi));
+        }
+    }
+    if (threadIdx.x == 0) {
+        if (write) s.st_nact[row] = (uint32_t)sh_nact;
+        ctl->t = t;
+        ctl->use_isyn_override = 0u;
+        ctl->done = 0u;
+        ctl->steps_done = steps_done + 1ull;
+        __threadfence();
+    }
+}
+
+// ------------------------------------------------------------ step kernel
+// One warp owns neurons n = base + 32 j + lane, j = 0..3 (base = 128 * warp):
+// coalesced loads, one Philox call per lane (words j), one bitmask word per j.
+template <bool GATHER, bool UPDATE, bool FORCED>
+__global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
+{
+    constexpr int kWarps = kStepThreads / 32;
+    __shared__ int sh_sub[kWarps];
+    __shared__ uint32_t sh_spk[kWarps];
+    __shared__ uint32_t sh_nact[kWarps];
+    __shared__ double sh_vsum[kWarps];
+    __shared__ int sh_last;
+
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const int64_t warp_global = (int64_t)blockIdx.x * kWarps + wid;
+    const int64_t base = warp_global * kWarpNeurons;
+    const unsigned long long steps_done = s.ctl->steps_done;
+
+    float4 Jn[4];
+    if (GATHER) {
+        const uint32_t* gbits = s.bits[(steps_done - 1ull) & 1ull];
+        float4 sum[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            sum[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int r = 0; r < 32; ++r) {
+                const int64_t n = base + j * 32 + r;
+                if (n >= s.N) break;
+                const float4 a = gather_row(s, gbits, n, lane);
+                if (lane == r) sum[j] = a;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t n = base + j * 32 + lane;
+            if (n < s.N) Jn[j] = add4(s.J[n], sum[j]);   // models/block.py:71-73
+        }
+        if (!UPDATE) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                if (n < s.N) s.J[n] = Jn[j];
+            }
+            return;
+        }
+    }
+
+    // ---- update of step `steps_done` (models/block.py:133-142)
+    const Ctl* ctl = s.ctl;
+    const float t = __fadd_rn(ctl->t, s.dt);
+    const float noise_rate = ctl->noise_rate;
+    const int isolated = ctl->isolated;
+    const bool use_override = ctl->use_isyn_override != 0u;
+    uint32_t* obits = s.bits[steps_done & 1ull];
+
+    const U4 rnd = philox4x32_10(U4{(uint32_t)(warp_global * 32 + lane), s.stream_id, (uint32_t)steps_done,
+                                    (uint32_t)(steps_done >> 32)},
+                                 (uint32_t)s.seed, (uint32_t)(s.seed >> 32));
+    const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
+
+    int mysub[4];
+    bool act[4], nav[4];
+    double vsum_lane = 0.0;
+    bool any_valid = false;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t n = base + j * 32 + lane;
+        act[j] = false; nav[j] = false; mysub[j] = -1;
+        if (n < s.N) {
+            any_valid = true;
+            const ParamClass p = load_class(s.pc, __ldg(s.cls + n));
+            const float v = s.V[n];
+            const float4 J = GATHER ? Jn[j] : s.J[n];
+            const float tl = s.tlast[n];
+            const float isyn = use_override ? s.isyn_override[n] : isyn_of(p, v, J);
+            const float mainp = __fmul_rn(-p.gL, __fsub_rn(v, p.VL));
+            const float cd = __fadd_rn(__fadd_rn(mainp, isyn), p.Iext);
+            const float vn = __fadd_rn(v, __fmul_rn(p.rCdt, cd));
+            const bool notsat = t >= __fadd_rn(tl, p.Tref);
+            const float vs = notsat ? vn : p.Vreset;
+            bool a = vs >= p.Vth;
+            const float vmin = isnan(vs) ? vs : (isnan(p.Vth) ? p.Vth : (vs < p.Vth ? vs : p.Vth));
+            if (FORCED && s.forced_active) a = (__ldg(s.forced_active + (n >> 5)) >> (n & 31)) & 1u;
+            const float rate = noise_rate >= 0.0f ? noise_rate : p.noise;
+            const bool nz = u01(words[j]) < rate;
+            bool na = isolated ? nz : (nz || a);
+            if (FORCED && s.forced_new) na = (__ldg(s.forced_new + (n >> 5)) >> (n & 31)) & 1u;
+            s.V[n] = vmin;
+            s.J[n] = mul4(J, p.decay);
+            if (a) s.tlast[n] = t;
+            act[j] = a; nav[j] = na; mysub[j] = p.sub;
+            vsum_lane += (double)vmin;
+        }
+    }
+
+    uint32_t cnt_spk = 0, cnt_nact = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t ma = __ballot_sync(0xffffffffu, act[j]);
+        const uint32_t mn = __ballot_sync(0xffffffffu, nav[j]);
+        const int64_t wi = warp_global * 4 + j;
+        if (lane == 0 && wi < s.n_words) { s.abits[wi] = ma; obits[wi] = mn; }
+        cnt_spk += __popc(ma);
+        cnt_nact += __popc(mn);
+    }
+
+    // ---- per-subblock statistics, aggregated per warp then per CTA
+    const bool warp_any = __any_sync(0xffffffffu, any_valid);
+    if (warp_any) {
+        const int sub0 = __shfl_sync(0xffffffffu, mysub[0], 0);
+        bool uni = true;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t n = base + j * 32 + lane;
+            if (n < s.N && mysub[j] != sub0) uni = false;
+        }
+        uni = __all_sync(0xffffffffu, uni) && sub0 >= 0 && sub0 < s.n_sub;
+        if (uni) {
+            double vs = vsum_lane;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) vs += __shfl_xor_sync(0xffffffffu, vs, o);
+            if (lane == 0) { sh_sub[wid] = sub0; sh_spk[wid] = cnt_spk; sh_nact[wid] = cnt_nact; sh_vsum[wid] = vs; }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                if (n >= s.N) continue;
+                const int sb = mysub[j];
+                if (sb >= 0 && sb < s.n_sub) {
+                    if (act[j]) atomicAdd(s.sub_spk + sb, 1u);
+                    if (nav[j]) atomicAdd(s.sub_nact + sb, 1u);
+                    atomicAdd(s.sub_vsum + sb, (double)s.V[n]);
+                } else if (nav[j]) {
+                    atomicAdd(s.unmapped_nact, 1u);
+                }
+            }
+            if (lane == 0) sh_sub[wid] = -1;
+        }
+    } else if (lane == 0) {
+        sh_sub[wid] = -1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int cur = -1; uint32_t cs = 0, cn = 0; double cv = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            const int sb = sh_sub[w];
+            if (sb < 0) continue;
+            if (sb != cur) {
+                if (cur >= 0) {
+                    atomicAdd(s.sub_spk + cur, cs); atomicAdd(s.sub_nact + cur, cn); atomicAdd(s.sub_vsum + cur, cv);
+                }
+                cur = sb; cs = 0; cn = 0; cv = 0.0;
+            }
+            cs += sh_spk[w]; cn += sh_nact[w]; cv += sh_vsum[w];
+        }
+        if (cur >= 0) { atomicAdd(s.sub_spk + cur, cs); atomicAdd(s.sub_nact + cur, cn); atomicAdd(s.sub_vsum + cur, cv); }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned prev = atomicAdd(&s.ctl->done, 1u);
+        sh_last = (prev == gridDim.x - 1u);
+    }
+    __syncthreads();
+    if (sh_last) {
+        __threadfence();
+        step_epilogue(s, steps_done, t);
+    }
+}
+
+// ------------------------------------------------------------ push scatter
+// cuda/src/stage/presynaptic_voltage.cpp:152-266 restated for one device:
+// a warp takes 32 bitmask words (1024 presynaptic neurons), walks their set
+// bits in order and scatters each outgoing row with coalesced index/weight
+// loads and one float2 atomic per synapse into the pending J.
+__global__ void __launch_bounds__(256) k_scatter(DevState s)
+{
+    const unsigned long long steps_done = s.ctl->steps_done;
+    const uint32_t* __restrict__ bits = s.bits[(steps_done - 1ull) & 1ull];
+    const int lane = threadIdx.x & 31;
+    const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t w0 = warp_global * 32;
+    if (w0 >= s.n_words) return;
+    const uint32_t word = (w0 + lane < s.n_words) ? __ldg(bits + w0 + lane) : 0u;
+    unsigned lanes = __ballot_sync(0xffffffffu, word != 0u);
+    while (lanes) {
+        const int l = __ffs(lanes) - 1;
+        lanes &= lanes - 1;
+        uint32_t wl = __shfl_sync(0xffffffffu, word, l);
+        while (wl) {
+            const int b = __ffs(wl) - 1;
+            wl &= wl - 1;
+            const int64_t pre = (w0 + l) * 32 + b;
+            const int64_t e0 = __ldg(s.qrow + pre);
+            const int64_t e1 = __ldg(s.qrow + pre + 1);
+            for (int64_t e = e0 + lane; e < e1; e += 32) {
+                const uint32_t c = __ldg(s.qcol + e);
+                const float2 w = __ldg(s.qw + e);
+                float2* dst = reinterpret_cast<float2*>(s.J + (c & kIndexMask)) + (c >> 31);
+                atomicAdd(dst, w);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ exports
+
+__global__ void k_export_J(const DevState s, float* __restrict__ out)
+{
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= s.N) return;
+    const float4 J = s.J[n];
+    out[n] = J.x; out[s.N + n] = J.y; out[2 * s.N + n] = J.z; out[3 * s.N + n] = J.w;
+}
+
+// I_ui [4][N] and I_syn [N] from the current V and J (models/block.py:83-87).
+__global__ void k_export_current(const DevState s, float* __restrict__ iui, float* __restrict__ isyn)
+{
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= s.N) return;
+    const ParamClass p = load_class(s.pc, s.cls[n]);
+    const float v = s.V[n];
+    const float4 J = s.J[n];
+    if (iui) {
+        const float4 i = iui_of(p, v, J);
+        iui[n] = i.x; iui[s.N + n] = i.y; iui[2 * s.N + n] = i.z; iui[3 * s.N + n] = i.w;
+    }
+    if (isyn) isyn[n] = isyn_of(p, v, J);
+}
+
+__global__ void k_bits_to_u8(const uint32_t* __restrict__ bits, int64_t N, uint8_t* __restrict__ out)
+{
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    out[n] = (uint8_t)((bits[n >> 5] >> (n & 31)) & 1u);
+}
+
+__global__ void k_u8_to_bits(const uint8_t* __restrict__ in, int64_t N, uint32_t* __restrict__ bits, int64_t n_words)
+{
+    const int64_t wi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (wi >= n_words) return;
+    uint32_t w = 0;
+    for (int b = 0; b < 32; ++b) {
+        const int64_t n = wi * 32 + b;
+        if (n < N && in[n]) w |= (1u << b);
+    }
+    bits[wi] = w;
+}
+
+__global__ void k_J_from_planar(DevState s, const float* __restrict__ in)
+{
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= s.N) return;
+    s.J[n] = make_float4(in[n], in[s.N + n], in[2 * s.N + n], in[3 * s.N + n]);
+}
+
+// ------------------------------------------------------------ weights
+// models/block.py:172-177: set channel weights of existing synapses.
+__global__ void k_update_weight(DevState s, int64_t n, const uint8_t* __restrict__ ch,
+                                const uint32_t* __restrict__ post, const uint32_t* __restrict__ pre,
+                                const float* __restrict__ val, float2* pw, float2* qw, unsigned* missing)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t kb = (ch[i] >= 2) ? kKindBit : 0u;
+    const int half = ch[i] & 1;
+    const uint32_t po = post[i], pr = pre[i];
+    bool found = false;
+    if (pw && po < s.N) {
+        for (int64_t e = s.prow[po]; e < s.prow[po + 1]; ++e) {
+            if (s.pcol[e] == (pr | kb)) {
+                float* w = reinterpret_cast<float*>(pw + e);
+                w[half] = val[i];
+                found = true;
+                break;
+            }
+        }
+    }
+    if (qw && pr < s.N) {
+        bool f2 = false;
+        for (int64_t e = s.qrow[pr]; e < s.qrow[pr + 1]; ++e) {
+            if (s.qcol[e] == (po | kb)) {
+                float* w = reinterpret_cast<float*>(qw + e);
+                w[half] = val[i];
+                f2 = true;
+                break;
+            }
+        }
+        found = found || f2;
+    }
+    if (!found) atomicAdd(missing, 1u);
+}
+
+// ------------------------------------------------------------ BOLD
+// models/bold_model_pytorch.py:43-78, one thread per region. Python scalars
+// are rounded to T where the tensor expression consumes them.
+template <typename T>
+struct BoldScalars {
+    T eps, ts, tf, t0, E0, V0, dt, base, exq, exv, k7, k2, one_em5;
+};
+
+__device__ __forceinline__ float dpow(float a, float b) { return powf(a, b); }
+__device__ __forceinline__ double dpow(double a, double b) { return pow(a, b); }
+
+template <typename T>
+__global__ void k_bold_run(int64_t R, const T* __restrict__ u, T* s, T* q, T* v, T* f, T* __restrict__ out,
+                           BoldScalars<T> c)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R) return;
+    T fi = f[i], si = s[i], qi = q[i], vi = v[i];
+    const T one = (T)1;
+    const T ds = ((u[i] * c.eps) - si / c.ts) - (fi - one) / c.tf;
+    const T qpart = fi > (T)0 ? (one - dpow(c.base, (one / fi) * one)) : one;
+    const T dq = (((fi * qpart) / c.E0) - qi * dpow(vi, c.exq)) / c.t0;
+    qi = qi + dq * c.dt;
+    const T dv = (fi - dpow(vi, c.exv)) / c.t0;
+    vi = vi + dv * c.dt;
+    fi = fi + si * c.dt;
+    fi = fi > (T)0 ? fi : (T)0;
+    si = si + ds * c.dt;
+    s[i] = si; q[i] = qi; v[i] = vi; f[i] = fi;
+    out[i] = ((c.k7 * (one - qi) + (one - qi / vi) * (T)2) + c.k2 * (one - vi)) * c.V0;
+}
+
+template <typename T>
+__device__ __forceinline__ T max_nan(T x, T c) { return (x != x) ? x : (x < c ? c : x); }
+
+// bold_model_pytorch.py:34-41
+template <typename T>
+__global__ void k_bold_state_update(int64_t R, int64_t S, const T* __restrict__ w, T* s, T* q, T* v, T* f, T c)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R) return;
+    const T* row = w + i * S;
+    s[i] = row[0];
+    q[i] = max_nan(row[1], c);
+    v[i] = max_nan(row[2], c);
+    f[i] = max_nan(row[3], c);
+}
+
+template <typename T>
+__global__ void k_fill(T* p, int64_t n, T val)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = val;
+}
+
+// ------------------------------------------------------------ generator
+// Counter-based synthetic network, restated on the CPU by
+// oracle/oracle.c:oracle_gen_rows.  One warp per postsynaptic row.
+struct GenArgs {
+    int64_t N;
+    int R;
+    const int64_t* region_start;  // [R+1]
+    const int64_t* region_n_exc;  // [R]
+    const float* cum;             // [R][R]
+    int K, Kp;                    // in-degree, next power of two
+    float w_scale;
+    uint64_t seed;
+    uint32_t* pcol;               // [N*K]
+    float2* pw;                   // [N*K]
+    uint32_t* outdeg;             // [N] (nullable) out-degree counts
+    unsigned* err;                // rows that could not draw K sources
+};
+
+constexpr uint32_t kTagSrc = 0xF0000001u;
+constexpr uint32_t kTagW = 0xF0000002u;
+constexpr int kGenWarps = 4;
+
+__device__ __forceinline__ int region_of(const int64_t* __restrict__ rs, int R, int64_t n)
+{
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(rs + mid) <= n) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kGenWarps * 32) k_gen_rows(GenArgs g)
+{
+    extern __shared__ unsigned long long gsm[];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const int64_t i = (int64_t)blockIdx.x * kGenWarps + wid;
+    if (i >= g.N) return;
+    unsigned long long* chosen = gsm + (size_t)wid * g.Kp;
+    const int ri = region_of(g.region_start, g.R, i);
+    const float* crow = g.cum + (size_t)ri * g.R;
+    const uint32_t k0 = (uint32_t)g.seed, k1 = (uint32_t)(g.seed >> 32);
+    int have = 0;
+    uint32_t attempt = 0;
+    const uint32_t limit = (uint32_t)(64 * g.K + 1024);
+    bool failed = false;
+    while (have < g.K) {
+        if (attempt > limit) { failed = true; break; }
+        const U4 o = philox4x32_10(U4{(uint32_t)i, kTagSrc, attempt, (uint32_t)((uint64_t)i >> 32)}, k0, k1);
+        ++attempt;
+        const uint32_t ws[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (have >= g.K) break;
+            const float ur = u01(ws[2 * h]);
+            int cntr = 0;
+            for (int j = lane; j < g.R - 1; j += 32) cntr += (__ldg(crow + j) <= ur) ? 1 : 0;
+            const int r = __reduce_add_sync(0xffffffffu, cntr);
+            const int64_t rs0 = __ldg(g.region_start + r);
+            const int64_t size = __ldg(g.region_start + r + 1) - rs0;
+            if (size <= 0) continue;
+            const uint64_t off = ((uint64_t)ws[2 * h + 1] * (uint64_t)size) >> 32;
+            const int64_t src = rs0 + (int64_t)off;
+            if (src == i) continue;
+            bool dup = false;
+            for (int k = lane; k < have; k += 32) dup |= ((int64_t)(chosen[k] >> 1) == src);
+            if (__any_sync(0xffffffffu, dup)) continue;
+            const unsigned long long kb = ((int64_t)off >= __ldg(g.region_n_exc + r)) ? 1ull : 0ull;
+            if (lane == 0) chosen[have] = ((unsigned long long)src << 1) | kb;
+            __syncwarp();
+            ++have;
+        }
+    }
+    if (failed) {
+        if (lane == 0) atomicAdd(g.err, 1u);
+        for (int k = have + lane; k < g.K; k += 32) chosen[k] = 0ull;
+        __syncwarp();
+    }
+    for (int k = g.K + lane; k < g.Kp; k += 32) chosen[k] = ~0ull;
+    __syncwarp();
+    // bitonic sort of chosen[0..Kp)
+    for (int size = 2; size <= g.Kp; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int idx = lane; idx < g.Kp; idx += 32) {
+                const int p = idx ^ stride;
+                if (p > idx) {
+                    const unsigned long long a = chosen[idx], b = chosen[p];
+                    const bool up = (idx & size) == 0;
+                    if ((a > b) == up) { chosen[idx] = b; chosen[p] = a; }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    const int64_t rowbase = i * (int64_t)g.K;
+    for (int j = lane; j < g.K; j += 32) {
+        const unsigned long long e = chosen[j];
+        const uint32_t src = (uint32_t)(e >> 1);
+        g.pcol[rowbase + j] = src | ((e & 1ull) ? kKindBit : 0u);
+        const U4 o = philox4x32_10(U4{(uint32_t)i, kTagW, (uint32_t)(j >> 1), (uint32_t)((uint64_t)i >> 32)}, k0, k1);
+        const uint32_t a = (j & 1) ? o.z : o.x;
+        const uint32_t b = (j & 1) ? o.w : o.y;
+        g.pw[rowbase + j] = make_float2(u01(a) * g.w_scale, u01(b) * g.w_scale);
+        if (g.outdeg) atomicAdd(g.outdeg + src, 1u);
+    }
+}
+
+// ------------------------------------------------------------ CSR transpose
+// Exclusive scan of u32 counts into i64 row pointers (three passes).
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ long long block_exclusive_scan(long long v, long long* sh, long long& total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        long long w = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        sh[lane] = w;
+    }
+    __syncthreads();
+    total = sh[(blockDim.x >> 5) - 1];
+    const long long before = wid ? sh[wid - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t* __restrict__ in, int64_t n,
+                                                             int64_t* __restrict__ out, long long* __restrict__ tile_sum)
+{
+    __shared__ long long sh[32];
+    const int64_t t0 = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    long long v[kScanItems];
+    long long local = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = (t0 + k < n) ? (long long)in[t0 + k] : 0;
+        local += v[k];
+    }
+    long long total;
+    long long ex = block_exclusive_scan(local, sh, total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (t0 + k < n) out[t0 + k] = ex;
+        ex += v[k];
+    }
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(long long* tile_sum, int64_t ntiles)
+{
+    __shared__ long long sh[32];
+    long long carry = 0;
+    for (int64_t b = 0; b < ntiles; b += kScanThreads) {
+        const int64_t i = b + threadIdx.x;
+        const long long v = (i < ntiles) ? tile_sum[i] : 0;
+        long long total;
+        const long long ex = block_exclusive_scan(v, sh, total);
+        if (i < ntiles) tile_sum[i] = ex + carry;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) tile_sum[ntiles] = carry;
+}
+
+__global__ void k_scan_add(int64_t* out, int64_t n, const long long* __restrict__ tile_sum, int64_t ntiles)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += tile_sum[i / kScanTile];
+    if (i == 0) out[n] = tile_sum[ntiles];
+}
+
+// Fill the push CSR from the pull CSR (unordered within a row; sorted next).
+__global__ void k_fill_push(int64_t N, const int64_t* __restrict__ prow, const uint32_t* __restrict__ pcol,
+                            const float2* __restrict__ pw, const int64_t* __restrict__ qrow, uint32_t* cursor,
+                            uint32_t* qcol, float2* qw)
+{
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= N) return;
+    for (int64_t e = prow[i] + lane; e < prow[i + 1]; e += 32) {
+        const uint32_t c = pcol[e];
+        const uint32_t src = c & kIndexMask;
+        const uint32_t pos = atomicAdd(cursor + src, 1u);
+        const int64_t d = qrow[src] + pos;
+        qcol[d] = (uint32_t)i | (c & kKindBit);
+        qw[d] = pw[e];
+    }
+}
+
+// Sort every push row by postsynaptic index (warp per row, rows up to
+// kSortCap entries in shared memory; longer rows are flagged).
+constexpr int kSortCap = 2048;
+constexpr int kSortWarps = 4;
+
+__global__ void __launch_bounds__(kSortWarps * 32) k_sort_push_rows(int64_t N, const int64_t* __restrict__ qrow,
+                                                                    uint32_t* qcol, float2* qw, unsigned* too_long)
+{
+    extern __shared__ unsigned long long ssm[];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const int64_t r = (int64_t)blockIdx.x * kSortWarps + wid;
+    if (r >= N) return;
+    const int64_t e0 = qrow[r], e1 = qrow[r + 1];
+    const int64_t len = e1 - e0;
+    if (len <= 1) return;
+    if (len > kSortCap) { if (lane == 0) atomicAdd(too_long, 1u); return; }
+    // key = post << 32 | kind bit | original slot; posts are distinct in a row
+    unsigned long long* key = ssm + (size_t)wid * kSortCap;
+    float2* wtmp = reinterpret_cast<float2*>(ssm + (size_t)kSortWarps * kSortCap) + (size_t)wid * kSortCap;
+    int Kp = 1;
+    while (Kp < len) Kp <<= 1;
+    for (int k = lane; k < Kp; k += 32) {
+        unsigned long long kk = ~0ull;
+        if (k < len) {
+            const uint32_t c = qcol[e0 + k];
+            kk = ((unsigned long long)(c & kIndexMask) << 32) | (unsigned long long)(c & kKindBit) |
+                 (unsigned long long)k;
+            wtmp[k] = qw[e0 + k];
+        }
+        key[k] = kk;
+    }
+    __syncwarp();
+    for (int size = 2; size <= Kp; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int idx = lane; idx < Kp; idx += 32) {
+                const int p = idx ^ stride;
+                if (p > idx) {
+                    const unsigned long long a = key[idx], b = key[p];
+                    const bool up = (idx & size) == 0;
+                    if ((a > b) == up) { key[idx] = b; key[p] = a; }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    for (int k = lane; k < len; k += 32) {
+        const unsigned long long kk = key[k];
+        qcol[e0 + k] = (uint32_t)(kk >> 32) | (uint32_t)(kk & kKindBit);
+        qw[e0 + k] = wtmp[(int)(kk & 0x7fffffffull)];
+    }
+}
+
+}  // namespace dtb

@@ -1,0 +1,155 @@
+"""Seeded synthetic networks in the reference's layout.
+
+The reference builds networks from brain-imaging data with
+``generation/make_block.py`` (unseeded, ``make_block.py:677``); the data are
+not available here, so these generators stand in for them with the shapes,
+sizes and value distributions of the benchmark configurations:
+
+* :func:`single_block` — one population pair (80 % excitatory), K random
+  presynaptic neurons per neuron (the small-block recipe of
+  ``test/test_generation.py:312-330`` with uniform sources);
+* :func:`whole_brain` — regions of log-normal size, 80 % of the synapses
+  inside the region and the rest routed by a seeded log-normal
+  region-connectivity matrix.
+
+A network is defined by a :class:`NetworkSpec`; the GPU generator
+(``dtb_block_create_synthetic``) and the CPU oracle produce identical arrays
+from it.  Property rows follow ``generation/make_block.py:394-432``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# LIF parameters of the single-block configuration (N=2000, K=100).
+LIF = dict(noise_rate=0.01, I_extern_Input=0.0, C=1.0, T_ref=5.0, g_Li=0.03, V_L=-70.0, V_th=-50.0,
+           V_reset=-55.0, g_ui=(0.01, 0.0005, 0.1, 0.005), V_ui=(0.0, 0.0, -70.0, -100.0),
+           tao_ui=(2.0, 40.0, 10.0, 50.0))
+
+
+def property_row(sub_block_idx: int, noise_rate=0.01, I_extern_Input=0.0, C=1.0, T_ref=5.0, g_Li=0.03,
+                 V_L=-70.0, V_th=-50.0, V_reset=-55.0, g_ui=LIF["g_ui"], V_ui=LIF["V_ui"],
+                 tao_ui=LIF["tao_ui"]) -> np.ndarray:
+    """One row of the 22-column property matrix (generation/make_block.py:394-432)."""
+    p = np.zeros(22, np.float32)
+    p[0] = noise_rate
+    p[1] = 0.0
+    p[2] = I_extern_Input
+    p[3] = sub_block_idx
+    p[4] = C
+    p[5] = T_ref
+    p[6] = g_Li
+    p[7] = V_L
+    p[8] = V_th
+    p[9] = V_reset
+    p[10:14] = np.asarray(g_ui, np.float32)
+    p[14:18] = np.asarray(V_ui, np.float32)
+    p[18:22] = np.asarray(tao_ui, np.float32)
+    return p
+
+
+@dataclass
+class NetworkSpec:
+    name: str
+    region_start: np.ndarray          # int64 [R+1]
+    region_n_exc: np.ndarray          # int64 [R]
+    cum: np.ndarray                   # float32 [R,R] cumulative source-region distribution
+    K: int
+    class_property: np.ndarray        # float32 [2R,22]; class 2r excitatory, 2r+1 inhibitory
+    gen_seed: int = 0
+    w_scale: float = 1.0
+    dt: float = 0.1
+    seed: int = 0                     # Philox noise key
+    stream_id: int = 0
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def R(self) -> int:
+        return len(self.region_start) - 1
+
+    @property
+    def N(self) -> int:
+        return int(self.region_start[-1])
+
+    @property
+    def S(self) -> int:
+        return self.N * self.K
+
+    def as_dict(self) -> dict:
+        return dict(region_start=self.region_start, region_n_exc=self.region_n_exc, cum=self.cum, K=self.K,
+                    gen_seed=self.gen_seed, w_scale=self.w_scale)
+
+    def neuron_class(self) -> np.ndarray:
+        """Class (= subblock) of every neuron: 2r excitatory, 2r+1 inhibitory."""
+        cls = np.empty(self.N, np.int64)
+        for r in range(self.R):
+            s0, s1, ne = int(self.region_start[r]), int(self.region_start[r + 1]), int(self.region_n_exc[r])
+            cls[s0:s0 + ne] = 2 * r
+            cls[s0 + ne:s1] = 2 * r + 1
+        return cls
+
+    def property(self) -> np.ndarray:
+        """Per-neuron [N,22] property matrix (subblock index in column 3)."""
+        cls = self.neuron_class()
+        prop = self.class_property[cls].copy()
+        prop[:, 3] = cls.astype(np.float32)
+        return prop
+
+    def sub_to_region(self) -> np.ndarray:
+        return (np.arange(2 * self.R) // 2).astype(np.int32)
+
+
+def _classes(R: int, **lif) -> np.ndarray:
+    return np.stack([property_row(c, **lif) for c in range(2 * R)])
+
+
+def single_block(N: int = 2000, K: int = 100, exc_frac: float = 0.8, gen_seed: int = 0, seed: int = 0,
+                 dt: float = 0.1, noise_rate: float = 0.01, name: str | None = None, **lif) -> NetworkSpec:
+    """One region of N neurons (first exc_frac excitatory), K uniform distinct sources per neuron."""
+    params = dict(LIF)
+    params.update(lif)
+    params["noise_rate"] = noise_rate
+    return NetworkSpec(name=name or f"single_block_N{N}_K{K}",
+                       region_start=np.array([0, N], np.int64),
+                       region_n_exc=np.array([int(round(exc_frac * N))], np.int64),
+                       cum=np.ones((1, 1), np.float32), K=K, class_property=_classes(1, **params),
+                       gen_seed=gen_seed, seed=seed, dt=dt)
+
+
+def whole_brain(R: int = 90, mean_size: float = 2.2e5, sigma: float = 0.5, K: int = 100, intra: float = 0.8,
+                exc_frac: float = 0.8, gen_seed: int = 0, seed: int = 0, dt: float = 0.1,
+                noise_rate: float = 0.01, scale: float = 1.0, name: str | None = None, **lif) -> NetworkSpec:
+    """R regions of log-normal(ln mean_size, sigma) neurons (times `scale`), `intra` of the synapses inside
+    the region, the rest routed by a seeded log-normal(0, 1) region matrix (row-normalised)."""
+    rng = np.random.default_rng(gen_seed)
+    sizes = np.maximum(np.round(rng.lognormal(np.log(mean_size), sigma, R) * scale), 2 * K + 2).astype(np.int64)
+    M = rng.lognormal(0.0, 1.0, (R, R))
+    np.fill_diagonal(M, 0.0)
+    P = (1.0 - intra) * M / M.sum(axis=1, keepdims=True)
+    P[np.arange(R), np.arange(R)] = intra
+    cum = np.cumsum(P, axis=1)
+    cum[:, -1] = 1.0
+    params = dict(LIF)
+    params.update(lif)
+    params["noise_rate"] = noise_rate
+    start = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    return NetworkSpec(name=name or f"whole_brain_R{R}", region_start=start,
+                       region_n_exc=np.round(exc_frac * sizes).astype(np.int64), cum=cum.astype(np.float32), K=K,
+                       class_property=_classes(R, **params), gen_seed=gen_seed, seed=seed, dt=dt)
+
+
+# Benchmark configurations (sizes and parameters of the reference's workloads).
+def config_single_block() -> NetworkSpec:
+    """N=2,000 (1,600 E / 400 I), K=100, dt=0.1 ms, noise p=0.01, Philox seed 0."""
+    return single_block(2000, 100, name="single_block_2k")
+
+
+def config_one_region(noise_rate: float = 0.01) -> NetworkSpec:
+    """N=1,000,000 (80/20), K=100 (1e8 synapses)."""
+    return single_block(1_000_000, 100, noise_rate=noise_rate, name=f"one_region_1M_p{noise_rate}")
+
+
+def config_whole_brain(scale: float = 1.0) -> NetworkSpec:
+    """90 regions, log-normal(ln 2.2e5, 0.5) sizes (~2e7 neurons), K=100 (~2e9 synapses)."""
+    return whole_brain(90, 2.2e5, 0.5, 100, scale=scale, name="whole_brain_90" + ("" if scale == 1.0 else f"_x{scale}"))

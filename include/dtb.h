@@ -1,0 +1,251 @@
+/*
+ * dtb.h — C ABI of the B200-native Digital Twin Brain time-step library
+ * (libdtb.so, built from digital_twin_brain_b200/csrc/).
+ *
+ * One handle (dtb_block) is one network resident on one GPU: neuron state,
+ * parameter classes, pull CSR (by postsynaptic neuron) and push CSR (by
+ * presynaptic neuron).  Every call returns 0 on success or a dtb_status code;
+ * dtb_last_error() gives the message.  No call throws or exits.  The library
+ * owns device memory; the caller owns every buffer it passes.  A handle is
+ * used by one host thread at a time and issues all work on one CUDA stream
+ * (dtb_block_set_stream).
+ *
+ * Pointers tagged `where` are host memory (DTB_HOST) or device memory on the
+ * handle's device (DTB_DEVICE).
+ *
+ * Each entry point names the reference interface it replaces
+ * (yeyeleijun/Digital_twin_brain, file:line).
+ */
+#ifndef DTB_H
+#define DTB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DTB_ABI_VERSION 1
+#define DTB_NPROP 22 /* property columns, generation/make_block.py:394-432 */
+
+typedef enum {
+    DTB_OK = 0,
+    DTB_ERR_ARG = 1,      /* bad argument (null, out of range, inconsistent sizes) */
+    DTB_ERR_CUDA = 2,     /* CUDA runtime error */
+    DTB_ERR_NOMEM = 3,    /* host or device allocation failed */
+    DTB_ERR_IO = 4,       /* file could not be read or written */
+    DTB_ERR_FORMAT = 5,   /* malformed npz / npy / checkpoint */
+    DTB_ERR_STATE = 6,    /* call not valid in the handle's current state */
+    DTB_ERR_LIMIT = 7     /* size beyond a documented limit */
+} dtb_status;
+
+typedef enum { DTB_HOST = 0, DTB_DEVICE = 1 } dtb_where;
+
+/* Propagation method for a run: the per-step choice between the push scatter
+ * (compacted spike list, float2 atomics) and the pull gather (spike bitmask,
+ * row-ordered, bit-identical to torch.sparse.mm's accumulation order). */
+typedef enum { DTB_MODE_AUTO = 0, DTB_MODE_PUSH = 1, DTB_MODE_PULL = 2 } dtb_mode;
+
+typedef enum {
+    DTB_FIELD_V = 0,          /* float[N]      block.V_i          models/block.py:56  */
+    DTB_FIELD_J = 1,          /* float[4][N]   block.J_ui         models/block.py:57  */
+    DTB_FIELD_I_UI = 2,       /* float[4][N]   block.I_ui         models/block.py:84  */
+    DTB_FIELD_I_SYN = 3,      /* float[N]      block.I_syn        models/block.py:86  */
+    DTB_FIELD_T_LAST = 4,     /* float[N]      block.t_ik_last    models/block.py:55  */
+    DTB_FIELD_ACTIVE = 5,     /* uint8[N]      block.active       models/block.py:134 */
+    DTB_FIELD_NEW_ACTIVE = 6, /* uint8[N]      spikes | noise     models/block.py:136 */
+    DTB_FIELD_T = 7,          /* float[1]      block.t            models/block.py:58  */
+    DTB_FIELD_STEP = 8,       /* uint64[1]     steps taken (Philox step counter) */
+    DTB_FIELD_SUB_COUNT = 9   /* uint32[n_sub] neurons per subblock */
+} dtb_field;
+
+typedef struct dtb_block dtb_block;
+typedef struct dtb_bold dtb_bold;
+
+/* Network from host arrays: the in-memory form of generation/read_block.py
+ * (property [N,22] + COO synapses), i.e. models/block.py:30 block(node_property,
+ * w_uij, delta_t).  Synapse e adds weight[e][0] to channel kind[e] and
+ * weight[e][1] to channel kind[e]+1 of neuron post[e] when neuron pre[e]
+ * fires (generation/read_block.py:68-74).  Entries are kept in the given
+ * order inside every row of both CSRs (stable sorts), which is the order
+ * torch.sparse.mm accumulates in. */
+typedef struct {
+    int64_t n_neurons;
+    const float* property;   /* [N][22] row-major, host */
+    const float* decay;      /* [N][4] exp(-dt/tau_ui) per neuron, host; NULL: expf on the host */
+    int64_t n_synapses;
+    const uint32_t* post;    /* [S] host */
+    const uint32_t* pre;     /* [S] host */
+    const uint8_t* kind;     /* [S] 0 = AMPA/NMDA, 2 = GABAa/GABAb, host */
+    const float* weight;     /* [S][2] host */
+    float dt;                /* ms */
+    uint64_t seed;           /* Philox key of the noise stream */
+    uint32_t stream_id;      /* Philox counter word 1 (ensemble member) */
+    int device;              /* CUDA device ordinal */
+    int build_push;          /* nonzero: also build the push CSR */
+} dtb_block_desc;
+
+/* Synthetic network generated on the GPU (counter-based Philox, identical to
+ * the CPU restatement in oracle/oracle.c:oracle_gen_rows).  Regions own
+ * neuron ranges [region_start[r], region_start[r+1]); the first
+ * region_n_exc[r] are excitatory.  Each neuron draws K distinct presynaptic
+ * neurons (never itself): source region from the cumulative row cum[r][*],
+ * then a uniform neuron inside it.  Subblock of a neuron = 2r (excitatory) or
+ * 2r+1 (inhibitory), parameter class = its subblock, class parameters from
+ * class_property[2R][22]. */
+typedef struct {
+    int n_regions;
+    const int64_t* region_start;   /* [R+1] host */
+    const int64_t* region_n_exc;   /* [R] host */
+    const float* cum;              /* [R][R] host, cumulative source-region distribution */
+    int K;                         /* in-degree, 1..1024 */
+    float w_scale;                 /* weights U[0,1) * w_scale */
+    uint64_t gen_seed;
+    const float* class_property;   /* [2R][22] host */
+    const float* class_decay;      /* [2R][4] host; NULL: expf on the host */
+    float dt;
+    uint64_t seed;
+    uint32_t stream_id;
+    int device;
+    int build_push;
+} dtb_synth_desc;
+
+typedef struct {
+    int64_t n_neurons;
+    int64_t n_synapses;
+    int32_t n_subblocks;
+    int32_t n_classes;
+    int32_t has_pull;
+    int32_t has_push;
+    int64_t device_bytes;    /* device memory held by the handle */
+    int64_t max_outdegree;
+    int64_t max_indegree;
+} dtb_block_info;
+
+/* ---- library ------------------------------------------------------------ */
+
+int dtb_abi_version(void);
+/* Copies the calling thread's last error message (NUL-terminated). */
+int dtb_last_error(char* buf, size_t len);
+
+/* ---- block lifecycle ---------------------------------------------------- */
+
+/* models/block.py:30-60 block.__init__; cuda/src/block.cpp:13-180
+ * (BrainBlock ctor, init_connection_table_gpu, init_config_params_gpu,
+ * init_all_stages_gpu); CSR order of cuda/src/configuration.cpp:575-828.
+ * Initial state as block.py: V = (V_th + V_reset)/2, J = 0, t_last = 0, t = 0. */
+int dtb_block_create(const dtb_block_desc* desc, dtb_block** out);
+
+/* generation/make_block.py:206-323 (connect_for_single_sparse_block) +
+ * :326-434 (generate_block_node_property), generated on the device. */
+int dtb_block_create_synthetic(const dtb_synth_desc* desc, dtb_block** out);
+
+/* cuda/src/configuration.cpp:748 parse_conn_table_from_numpy +
+ * :961 parse_params_from_numpy: reads block_0.npz .. block_{n-1}.npz of
+ * generation/make_block.py:473-479 from `dir` (one population per file, as
+ * generation/read_block.py:12-97 reads them). */
+int dtb_block_create_from_npz(const char* dir, float dt, uint64_t seed, uint32_t stream_id,
+                              int device, int build_push, dtb_block** out);
+
+int dtb_block_destroy(dtb_block* b);
+
+/* cuda/src/block.cpp / dist_simulator.cpp:399-400 (the step's stream).
+ * `stream` is a cudaStream_t; NULL selects the legacy default stream. */
+int dtb_block_set_stream(dtb_block* b, void* stream);
+int dtb_block_synchronize(dtb_block* b);
+int dtb_block_get_info(const dtb_block* b, dtb_block_info* info);
+
+/* ---- stepping ----------------------------------------------------------- */
+
+/* n_steps x models/block.py:116-150 block.run(noise_rate, isolated).
+ * noise_rate >= 0: that rate for every neuron (block.py:136);
+ * noise_rate < 0: per-neuron rate from property column 0 (cuda/src/stage/spike.cpp:157).
+ * Outputs per step (nullable): sum_out[n_steps][n_sub] spike count of every
+ * subblock (noise excluded, block.py:148), mean_out[n_steps][n_sub] mean V
+ * (block.py:147; NaN for an empty subblock), nact_out[n_steps] number of
+ * neurons that propagated (spikes | noise).  All three at `where`. */
+int dtb_block_run(dtb_block* b, int n_steps, float noise_rate, int isolated, int mode,
+                  float* sum_out, float* mean_out, uint32_t* nact_out, int where);
+
+/* One block.run in which this step's active and new_active sets are replaced
+ * by the given uint8[N] arrays (teacher forcing; NULL keeps the computed
+ * set).  Used to compare against a reference run step by step. */
+int dtb_block_step_forced(dtb_block* b, float noise_rate, int isolated, int mode,
+                          const uint8_t* forced_active, const uint8_t* forced_new_active,
+                          float* sum_out, float* mean_out, int where);
+
+/* ---- state access ------------------------------------------------------- */
+
+/* Getters of cuda/include/block.hpp:247-562 (get_*_gpu / get_*_cpu) and the
+ * public tensors of models/block.py:55-58,84-86,134. */
+int dtb_block_get(dtb_block* b, int field, void* dst, int where);
+/* Copies the pull (which = 0, rows = postsynaptic neurons) or push (which = 1,
+ * rows = presynaptic neurons) CSR: rowptr[N+1] int64, index[S] uint32 (the
+ * other endpoint; bit 31 set for a GABAa/GABAb synapse), weight[S][2] float.
+ * Any output may be NULL.  The layout of cuda/src/configuration.cpp:783-795
+ * (rowptrs, colinds, float2 vals, connkinds) with the kind folded into bit 31. */
+int dtb_block_get_csr(dtb_block* b, int which, int64_t* rowptr, uint32_t* index, float* weight, int where);
+
+/* Overwrite V, J, T_LAST, T or STEP (checkpoint restore, tests). */
+int dtb_block_set(dtb_block* b, int field, const void* src, int where);
+
+/* models/block.py:152-170 block.update_property: replace the [N][22]
+ * property matrix (and optionally [N][4] decay).  As in the reference, the
+ * synaptic current already computed from the old parameters drives the next
+ * membrane update. */
+int dtb_block_update_property(dtb_block* b, const float* property, const float* decay);
+
+/* cuda/src/stage/property.cpp:146-257 update_prop_cols_kernel,
+ * cuda/python/dist_blockwrapper_pytorch.py:446 mul_property_by_subblk
+ * (accumulate=False): property column col[i] of every neuron in subblock
+ * sub[i] becomes base_value * value[i], base = the value at creation. */
+int dtb_block_scale_property_by_subblock(dtb_block* b, int n, const int32_t* sub, const int32_t* col,
+                                         const float* value);
+
+/* models/block.py:172-177 block.update_conn_weight: set the channel weight
+ * of existing synapses (channel[i], post[i], pre[i]) to value[i]. */
+int dtb_block_update_conn_weight(dtb_block* b, int64_t n, const uint8_t* channel, const uint32_t* post,
+                                 const uint32_t* pre, const float* value);
+
+/* Checkpoint of the dynamic state (V, J, t_last, pending I_syn, t, step).
+ * No counterpart in the reference (it has none, cuda/protos/snn.proto:62
+ * only offsets input-spike timestamps); a restored run continues
+ * bit-identically because the noise counter is the step index. */
+int dtb_block_save(dtb_block* b, const char* path);
+int dtb_block_load(dtb_block* b, const char* path);
+
+/* ---- BOLD (models/bold_model_pytorch.py) --------------------------------- */
+
+/* BOLD.__init__ (bold_model_pytorch.py:12-25). dtype: 0 float32, 1 float64.
+ * State starts as the reference's first run(): s=0, q=0, v=1, f_in=1. */
+int dtb_bold_create(int64_t n_regions, int dtype, double epsilon, double tao_s, double tao_f, double tao_0,
+                    double alpha, double E_0, double V_0, double delta_t, int device, dtb_bold** out);
+int dtb_bold_destroy(dtb_bold* m);
+int dtb_bold_set_stream(dtb_bold* m, void* stream);
+/* BOLD.run (bold_model_pytorch.py:43-78): one Euler step, u -> out, both [R] of the model's dtype. */
+int dtb_bold_run(dtb_bold* m, const void* u, void* out, int where);
+/* BOLD.state_update (bold_model_pytorch.py:34-41): w is [E][Rp][S] of the
+ * model's dtype with E*Rp == R; s = w[..,0], q = max(w[..,1],1e-5),
+ * v = max(w[..,2],1e-5), f_in = max(w[..,3],1e-5). */
+int dtb_bold_state_update(dtb_bold* m, const void* w, int64_t E, int64_t Rp, int64_t S, int where);
+/* field: 0 s, 1 q, 2 v, 3 f_in; dst [R] of the model's dtype. */
+int dtb_bold_get(dtb_bold* m, int field, void* dst, int where);
+int dtb_bold_set(dtb_bold* m, int field, const void* src, int where);
+
+/* Per-step BOLD driven by the block (simulation/simulation.py:269-279):
+ * after every step, act[r] = (spikes of the subblocks mapped to region r) /
+ * (neurons of those subblocks); BOLD.run(max(act, 1e-5)) in float64 with
+ * delta_t = dt/1000 s.  sub_to_region[n_sub] (host) maps subblocks to
+ * regions (-1: not in any region). */
+int dtb_block_attach_bold(dtb_block* b, int n_regions, const int32_t* sub_to_region,
+                          double epsilon, double tao_s, double tao_f, double tao_0, double alpha,
+                          double E_0, double V_0);
+/* field: 0 s, 1 q, 2 v, 3 f_in, 4 bold output of the last step, 5 act of the last step; double[R]. */
+int dtb_block_get_bold(dtb_block* b, int field, double* dst, int where);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DTB_H */
