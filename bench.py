@@ -1,0 +1,321 @@
+"""Benchmark of the Digital Twin Brain time-step path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one dt = 0.1 ms time step of the whole-brain workload: 90 regions
+of log-normal size (~2.2e7 neurons), K = 100 presynaptic neurons each
+(~2.2e9 synapses), 80 % intra-region, Poisson noise p = 0.01, per-region
+Balloon-Windkessel BOLD.  Synthetic network (seeded), since the reference's
+imaging-derived inputs are not available.
+
+value = synaptic events/s (sum over steps of the out-degrees of every neuron
+that propagated, i.e. spike | noise, divided by device time), timed with CUDA
+events on the network's stream over exactly K steps after W warm-up steps,
+max over ranks.  The state (1 GB) and synapse tables (27 GB per direction)
+are far larger than L2, so no flush is needed.  With N GPUs every rank runs
+an independent replica (the path does not shard across GPUs).
+
+--impl reference times the reference's algorithm on the host cores (the CPU
+oracle restating models/block.py, OpenMP) on a bounded sample of the same
+workload and prints the same line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "synaptic events/s & sim-s/wall-s at 2B syn; DA window time surrogate vs plain"
+UNIT = "events/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="tune", choices=["tune", "auto", "push", "pull"])
+    ap.add_argument("--scale", type=float, default=1.0, help="whole-brain size scale (1.0 = ~2.2e9 synapses)")
+    ap.add_argument("--noise", type=float, default=0.01)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=400)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_sample(scale: float, noise: float, seconds: float, max_steps: int, warmup: int = 2):
+    """The reference algorithm (oracle port of models/block.py, OpenMP) on a scaled whole-brain network."""
+    from oracle import oracle as O
+    from digital_twin_brain_b200 import synthetic
+    import torch
+    threads = min(os.cpu_count() or 1, 64)
+    spec = synthetic.whole_brain(scale=scale, noise_rate=noise, name="cpu_sample")
+    rowptr, pre, kind, w = O.gen_network(spec.as_dict())
+    prop = spec.property()
+    tau = torch.from_numpy(prop).transpose(0, 1)[18:22]
+    decay = torch.exp(-spec.dt / tau).numpy().copy()
+    ob = O.OracleBlock(prop, decay, rowptr, pre, kind, w, spec.dt, spec.seed, nthreads=threads)
+    outdeg = np.bincount(pre, minlength=spec.N).astype(np.int64)
+    for _ in range(warmup):
+        ob.run(noise)
+    events = 0
+    steps = 0
+    t0 = time.perf_counter()
+    while steps < max_steps and (time.perf_counter() - t0) < seconds:
+        ob.run(noise)
+        events += int(outdeg[ob.new_active.astype(bool)].sum())
+        steps += 1
+    dt = time.perf_counter() - t0
+    return dict(value=events / dt, unit=UNIT, cores=threads, kind="port", steps=steps, seconds=dt,
+                sim_s_per_wall_s=steps * spec.dt / 1000.0 / dt,
+                sample=(f"oracle port of models/block.py step (sparse gather over all {spec.S} synapses, "
+                        f"{threads} OpenMP threads) on the whole-brain network at scale {scale}: "
+                        f"N={spec.N}, S={spec.S}, {steps} steps after {warmup} warm-up"))
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    budget = 60.0
+    r = cpu_sample(scale=1 / 64, noise=args.noise, seconds=budget, max_steps=max(args.steps, 1),
+                   warmup=min(args.warmup, 3))
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": r["steps"],
+            "warmup": min(args.warmup, 3), "ms_per_step": 1000.0 * r["seconds"] / max(r["steps"], 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "whole_brain_90 (90 regions, K=100, dt=0.1 ms, p=0.01) at scale 1/64 on CPU",
+                       "parallelism": "host cores"},
+            "sim_s_per_wall_s": r["sim_s_per_wall_s"],
+            "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import torch.distributed as dist
+    from digital_twin_brain_b200 import Network, synthetic
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    spec = synthetic.config_whole_brain(args.scale) if args.scale != 1.0 else synthetic.config_whole_brain()
+    spec.seed = 1000 + rank              # independent replica noise per rank
+    spec.extra["noise"] = args.noise
+    t_build = time.perf_counter()
+    net = Network.from_spec(spec, device=dev, build_push=True)
+    net.attach_bold(spec.sub_to_region(), spec.R)
+    stream = torch.cuda.Stream(device=dev)
+    net.set_stream(stream)
+    torch.cuda.synchronize(dev)
+    t_build = time.perf_counter() - t_build
+    info = net.info()
+
+    # warm-up (also passes the initial refractory period) and method choice
+    W = max(args.warmup, 3)
+    net.run(W, noise_rate=args.noise, mode="auto", out=None)
+    tune = {}
+    if args.mode == "tune":
+        for m in ("push", "pull"):
+            tune[m] = net.time_kernels(32, noise_rate=args.noise, mode=m)
+        mode = min(tune, key=lambda m: tune[m]["step_ms"])
+    else:
+        mode = args.mode
+    kt = net.time_kernels(64, noise_rate=args.noise, mode=mode)
+    torch.cuda.synchronize(dev)
+
+    # ---- timed region: exactly K steps on the device
+    K = args.steps
+    ev0 = net.get(10)  # FIELD_EVENTS
+    l0 = net.info().kernel_launches
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(dev) as clk:
+        start.record(stream)
+        net.run(K, noise_rate=args.noise, mode=mode, out=None)
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    events = net.get(10) - ev0
+    launches = net.info().kernel_launches - l0
+    t = torch.tensor([ms, float(events)], dtype=torch.float64, device=f"cuda:{dev}")
+    if world > 1:
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        tot = t.clone()
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        ms_max, events_all = float(mx[0]), float(tot[1])
+    else:
+        ms_max, events_all = ms, float(events)
+    value = events_all / (ms_max / 1000.0)
+    sim_ratio = K * spec.dt / 1000.0 / (ms_max / 1000.0)
+
+    # ---- end to end through the public API: per step, host->device run parameters and the
+    #      per-subblock results (spike sums, mean V, propagated count) back to host memory
+    E = min(args.e2e_steps, K)
+    ev_a = net.get(10)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(E):
+        net.run(1, noise_rate=args.noise, mode=mode, out="host")
+    t_e2e = time.perf_counter() - t0
+    ev_e2e = net.get(10) - ev_a
+    e2e_value = ev_e2e / t_e2e
+    h2d = 16                                  # run parameters (base step, noise rate, isolated)
+    d2h = 2 * 4 * net.n_sub + 4               # spike sums + mean V per subblock + propagated count
+
+    # ---- roofline of the dominant kernel
+    N, S = spec.N, spec.S
+    evs = kt["events_per_step"]
+    nact = evs / spec.K
+    upd_bytes = N * (4 + 16 + 4 + 4) + N * (4 + 16) + 2 * N / 8          # V,J,t_last,class r; V,J w; 2 bitmasks
+    if mode == "push":
+        prop_bytes = N / 8 + 16 * nact + 12 * evs                          # bitmask, row pointers, (post, w) of rows
+        kernels = {"update": (kt["update_ms"], upd_bytes), "scatter": (kt["propagate_ms"], prop_bytes)}
+    else:
+        fused = upd_bytes + 8 * N + 4 * S + 8 * evs                        # + row ptrs, all indices, active weights
+        kernels = {"gather+update": (kt["update_ms"], fused)}
+    dom = max(kernels, key=lambda k: kernels[k][0])
+    d_ms, d_bytes = kernels[dom]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = d_bytes / (d_ms * 1e-3) / 1e9 if d_ms > 0 else 0.0
+    step_bytes = sum(b for _, b in kernels.values())
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": dom, "algorithmic_bytes_per_launch": d_bytes, "launch_ms": d_ms,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_sample(scale=1 / 64, noise=args.noise, seconds=15.0, max_steps=10_000)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]}
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+                "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": (f"whole_brain_90: 90 regions lognormal(ln 2.2e5, 0.5) x{args.scale}, "
+                                        f"N={N}, S={S}, K={spec.K}, 80% intra-region, dt=0.1 ms, "
+                                        f"noise p={args.noise}, fp32 weights, BOLD per region"),
+                           "method": mode, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                           "l2": "inputs larger than L2 (state ~1 GB, synapses ~27 GB per CSR)"},
+                "value_metric": "synaptic events/s", "sim_s_per_wall_s": sim_ratio,
+                "events_per_step": events_all / world / K, "firing": {
+                    "propagated_per_step": evs / spec.K, "propagated_frac": evs / spec.K / N},
+                "kernel_ms": kt, "tune": tune, "build_s": t_build, "device_gb": info.device_bytes / 1e9,
+                "gpu_launches": int(launches),
+                "roofline": roofline,
+                "step_roofline": {"bytes_per_step": step_bytes, "ms": kt["step_ms"],
+                                  "achieved_gbs": step_bytes / (kt["step_ms"] * 1e-3) / 1e9 if kt["step_ms"] else 0},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "steps": E, "ms_per_step": 1000.0 * t_e2e / E,
+                        "api": "Network.run(1, out='host') per step (ctypes -> dtb_block_run, DTB_HOST)"},
+                "clocks": clocks}
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    net.close()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

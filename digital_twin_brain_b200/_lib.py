@@ -20,7 +20,7 @@ MODE_AUTO, MODE_PUSH, MODE_PULL = 0, 1, 2
 MODES = {"auto": MODE_AUTO, "push": MODE_PUSH, "pull": MODE_PULL}
 
 FIELD_V, FIELD_J, FIELD_I_UI, FIELD_I_SYN, FIELD_T_LAST, FIELD_ACTIVE, FIELD_NEW_ACTIVE, FIELD_T, FIELD_STEP, \
-    FIELD_SUB_COUNT = range(10)
+    FIELD_SUB_COUNT, FIELD_EVENTS = range(11)
 
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "out of memory", 4: "I/O error", 5: "format error",
           6: "invalid state", 7: "limit exceeded"}
@@ -48,7 +48,8 @@ class SynthDesc(ctypes.Structure):
 class BlockInfo(ctypes.Structure):
     _fields_ = [("n_neurons", c_i64), ("n_synapses", c_i64), ("n_subblocks", ctypes.c_int32),
                 ("n_classes", ctypes.c_int32), ("has_pull", ctypes.c_int32), ("has_push", ctypes.c_int32),
-                ("device_bytes", c_i64), ("max_outdegree", c_i64), ("max_indegree", c_i64)]
+                ("device_bytes", c_i64), ("max_outdegree", c_i64), ("max_indegree", c_i64),
+                ("kernel_launches", c_i64)]
 
 
 # name -> (argtypes)
@@ -64,6 +65,7 @@ _SIGS = {
     "dtb_block_get_info": [c_vp, ctypes.POINTER(BlockInfo)],
     "dtb_block_run": [c_vp, c_int, c_f32, c_int, c_int, c_vp, c_vp, c_vp, c_int],
     "dtb_block_step_forced": [c_vp, c_f32, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_int],
+    "dtb_block_time_kernels": [c_vp, c_int, c_f32, c_int, c_int, c_vp],
     "dtb_block_get": [c_vp, c_int, c_vp, c_int],
     "dtb_block_set": [c_vp, c_int, c_vp, c_int],
     "dtb_block_get_csr": [c_vp, c_int, c_vp, c_vp, c_vp, c_int],

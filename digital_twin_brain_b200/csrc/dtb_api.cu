@@ -152,6 +152,7 @@ struct dtb_block {
     size_t pinned_bytes = 0;
     RunParams* h_run = nullptr;   // pinned
     // auto mode
+    int64_t launches = 0;
     double last_frac = -1.0;
     double pull_threshold = 0.05;
     int chunk = 32;
@@ -443,6 +444,7 @@ static int launch_update(dtb_block* b, const DevState& s, bool gather, bool forc
         else k_step<false, true, false><<<grid, kStepThreads, 0, b->stream>>>(s);
     }
     CK(cudaGetLastError());
+    b->launches++;
     return DTB_OK;
 }
 
@@ -452,6 +454,7 @@ static int launch_gather_only(dtb_block* b, const DevState& s)
     if (grid == 0) return DTB_OK;
     k_step<true, false, false><<<grid, kStepThreads, 0, b->stream>>>(s);
     CK(cudaGetLastError());
+    b->launches++;
     return DTB_OK;
 }
 
@@ -462,6 +465,7 @@ static int launch_scatter(dtb_block* b, const DevState& s)
     if (grid == 0) return DTB_OK;
     k_scatter<<<grid, 256, 0, b->stream>>>(s);
     CK(cudaGetLastError());
+    b->launches++;
     return DTB_OK;
 }
 
@@ -489,8 +493,11 @@ static int enqueue_chunk(dtb_block* b, int n, int mode)
     cudaGraphExec_t& ge = b->graph[mode];
     if (!ge) {
         cudaGraph_t g = nullptr;
+        const int64_t before = b->launches;
         CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         int rc = enqueue_steps(b, n, mode);
+        b->graph_len[mode] = (int)(b->launches - before);
+        b->launches = before;
         cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
         if (rc != DTB_OK) { if (g) cudaGraphDestroy(g); return rc; }
         if (ce != cudaSuccess) return fail(DTB_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
@@ -499,6 +506,7 @@ static int enqueue_chunk(dtb_block* b, int n, int mode)
         if (ce != cudaSuccess) { ge = nullptr; return fail(DTB_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce)); }
     }
     CK(cudaGraphLaunch(ge, b->stream));
+    b->launches += b->graph_len[mode];
     return DTB_OK;
 }
 
@@ -893,6 +901,7 @@ int dtb_block_get_info(const dtb_block* b, dtb_block_info* info)
     info->device_bytes = b->dev_bytes;
     info->max_outdegree = b->max_out;
     info->max_indegree = b->max_in;
+    info->kernel_launches = b->launches;
     return DTB_OK;
 }
 
@@ -924,6 +933,61 @@ int dtb_block_run(dtb_block* b, int n_steps, float noise_rate, int isolated, int
         }
         done += n;
     }
+    return DTB_OK;
+}
+
+int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isolated, int mode, float* out_ms)
+{
+    if (!b || !out_ms || n_steps <= 0) return fail(DTB_ERR_ARG, "bad argument");
+    DeviceGuard g(b->device);
+    const int m = choose_mode(b, mode);
+    RET(ensure_stats(b, (uint32_t)n_steps));
+    RET(set_run_params(b, noise_rate, isolated));
+    unsigned long long ev0 = 0, ev1 = 0;
+    CK(cudaStreamSynchronize(b->stream));
+    CK(cudaMemcpy(&ev0, &b->ds.ctl->events, 8, cudaMemcpyDeviceToHost));
+    const int n_ev = 4 * n_steps + 4;
+    std::vector<cudaEvent_t> ev((size_t)n_ev);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    std::vector<int> kind;  // 0 update kernel, 1 propagation-only kernel
+    int k = 0;
+    auto rec = [&](int i) { return cudaEventRecord(ev[(size_t)i], b->stream); };
+    int rc = DTB_OK;
+    if (m == DTB_MODE_PUSH) {
+        for (int st = 0; st < n_steps && rc == DTB_OK; ++st) {
+            rec(k); rc = launch_update(b, b->ds, false, false); rec(k + 1); kind.push_back(0); k += 2;
+            if (rc != DTB_OK) break;
+            rec(k); rc = launch_scatter(b, b->ds); rec(k + 1); kind.push_back(1); k += 2;
+            if (k + 2 > n_ev) break;
+        }
+    } else {
+        rec(k); rc = launch_update(b, b->ds, false, false); rec(k + 1); kind.push_back(0); k += 2;
+        for (int st = 1; st < n_steps && rc == DTB_OK && k + 4 <= n_ev; ++st) {
+            rec(k); rc = launch_update(b, b->ds, true, false); rec(k + 1); kind.push_back(0); k += 2;
+        }
+        if (rc == DTB_OK) { rec(k); rc = launch_gather_only(b, b->ds); rec(k + 1); kind.push_back(1); k += 2; }
+    }
+    const int done_steps = (m == DTB_MODE_PUSH) ? (int)(kind.size() / 2) : (int)kind.size() - 1;
+    b->steps += (uint64_t)done_steps;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    double sum[2] = {0.0, 0.0};
+    int cnt[2] = {0, 0};
+    for (size_t i = 0; i < kind.size() && e == cudaSuccess; ++i) {
+        float ms = 0.0f;
+        e = cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+        sum[kind[i]] += ms;
+        cnt[kind[i]]++;
+    }
+    float total = 0.0f;
+    if (e == cudaSuccess && k >= 2) e = cudaEventElapsedTime(&total, ev[0], ev[(size_t)k - 1]);
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (rc != DTB_OK) return rc;
+    if (e != cudaSuccess) return fail(DTB_ERR_CUDA, "event timing: %s", cudaGetErrorString(e));
+    CK(cudaMemcpy(&ev1, &b->ds.ctl->events, 8, cudaMemcpyDeviceToHost));
+    out_ms[0] = cnt[0] ? (float)(sum[0] / cnt[0]) : 0.0f;
+    out_ms[1] = cnt[1] ? (float)(sum[1] / cnt[1]) : 0.0f;
+    out_ms[2] = done_steps ? total / (float)done_steps : 0.0f;
+    out_ms[3] = done_steps ? (float)((double)(ev1 - ev0) / done_steps) : 0.0f;
     return DTB_OK;
 }
 
@@ -1007,6 +1071,7 @@ int dtb_block_get(dtb_block* b, int field, void* dst, int where)
         if (where == DTB_HOST) { std::memcpy(dst, &b->steps, sizeof(uint64_t)); return DTB_OK; }
         return copy_out(b, dst, &s.ctl->steps_done, sizeof(uint64_t), where);
     }
+    case DTB_FIELD_EVENTS: return copy_out(b, dst, &s.ctl->events, sizeof(unsigned long long), where);
     case DTB_FIELD_SUB_COUNT:
         if (where == DTB_HOST) { if (b->n_sub) std::memcpy(dst, b->sub_count.data(), sizeof(uint32_t) * b->n_sub); return DTB_OK; }
         return copy_out(b, dst, s.sub_count, sizeof(uint32_t) * b->n_sub, where);

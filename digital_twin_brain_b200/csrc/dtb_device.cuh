@@ -53,8 +53,9 @@ struct Ctl {
     uint32_t use_isyn_override;      // next update takes I_syn from isyn_override
     uint32_t err;                    // sticky error flags
     uint32_t pad;
+    unsigned long long events;       // synaptic events propagated since creation
 };
-static_assert(sizeof(Ctl) == 48, "Ctl layout");
+static_assert(sizeof(Ctl) == 56, "Ctl layout");
 
 struct RunParams {
     unsigned long long run_base;
@@ -124,7 +125,6 @@ __host__ __device__ __forceinline__ void mulhilo32(uint32_t a, uint32_t b, uint3
 
 __host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1)
 {
-#pragma unroll
     for (int r = 0; r < 10; ++r) {
         if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
         uint32_t hi0, lo0, hi1, lo1;

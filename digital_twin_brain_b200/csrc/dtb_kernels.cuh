@@ -71,7 +71,7 @@ __device__ __forceinline__ bool test_bit(const uint32_t* __restrict__ bits, int6
 // accumulated strictly in row order from +0 (sparse.mm order). All lanes
 // return the same value.
 __device__ __forceinline__ float4 gather_row(const DevState& s, const uint32_t* __restrict__ bits, int64_t n,
-                                             int lane)
+                                             int lane, uint32_t& events)
 {
     const int64_t e0 = __ldg(s.prow + n);
     const int64_t e1 = __ldg(s.prow + n + 1);
@@ -82,6 +82,7 @@ __device__ __forceinline__ float4 gather_row(const DevState& s, const uint32_t* 
         const uint32_t c = valid ? __ldg(s.pcol + idx) : 0u;
         const bool act = valid && test_bit(bits, c & kIndexMask);
         unsigned m = __ballot_sync(0xffffffffu, act);
+        events += __popc(m);
         float2 w = make_float2(0.0f, 0.0f);
         if (act) w = __ldg(s.pw + idx);
         while (m) {
@@ -159,6 +160,19 @@ __device__ void step_epilogue(const DevState& s, unsigned long long steps_done, 
     }
 }
 
+// Adds a warp-uniform event count (lane 0's copy) to the CTA total and, once
+// per CTA, to the device counter.
+__device__ __forceinline__ void cta_add_events(const DevState& s, uint32_t events, int lane, int wid)
+{
+    __shared__ unsigned long long sh_ev;
+    if (threadIdx.x == 0) sh_ev = 0ull;
+    __syncthreads();
+    if (lane == 0 && events) atomicAdd(&sh_ev, (unsigned long long)events);
+    __syncthreads();
+    if (threadIdx.x == 0 && sh_ev) atomicAdd(&s.ctl->events, sh_ev);
+    (void)wid;
+}
+
 // ------------------------------------------------------------ step kernel
 // One warp owns neurons n = base + 32 j + lane, j = 0..3 (base = 128 * warp):
 // coalesced loads, one Philox call per lane (words j), one bitmask word per j.
@@ -182,16 +196,18 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
     if (GATHER) {
         const uint32_t* gbits = s.bits[(steps_done - 1ull) & 1ull];
         float4 sum[4];
+        uint32_t events = 0;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             sum[j] = make_float4(0.f, 0.f, 0.f, 0.f);
             for (int r = 0; r < 32; ++r) {
                 const int64_t n = base + j * 32 + r;
                 if (n >= s.N) break;
-                const float4 a = gather_row(s, gbits, n, lane);
+                const float4 a = gather_row(s, gbits, n, lane, events);
                 if (lane == r) sum[j] = a;
             }
         }
+        cta_add_events(s, events, lane, wid);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int64_t n = base + j * 32 + lane;
@@ -342,9 +358,12 @@ __global__ void __launch_bounds__(256) k_scatter(DevState s)
     const int lane = threadIdx.x & 31;
     const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t w0 = warp_global * 32;
-    if (w0 >= s.n_words) return;
+    __shared__ unsigned long long sh_ev;
+    if (threadIdx.x == 0) sh_ev = 0ull;
+    __syncthreads();
     const uint32_t word = (w0 + lane < s.n_words) ? __ldg(bits + w0 + lane) : 0u;
     unsigned lanes = __ballot_sync(0xffffffffu, word != 0u);
+    unsigned long long events = 0;
     while (lanes) {
         const int l = __ffs(lanes) - 1;
         lanes &= lanes - 1;
@@ -355,6 +374,7 @@ __global__ void __launch_bounds__(256) k_scatter(DevState s)
             const int64_t pre = (w0 + l) * 32 + b;
             const int64_t e0 = __ldg(s.qrow + pre);
             const int64_t e1 = __ldg(s.qrow + pre + 1);
+            events += (unsigned long long)(e1 - e0);
             for (int64_t e = e0 + lane; e < e1; e += 32) {
                 const uint32_t c = __ldg(s.qcol + e);
                 const float2 w = __ldg(s.qw + e);
@@ -363,6 +383,9 @@ __global__ void __launch_bounds__(256) k_scatter(DevState s)
             }
         }
     }
+    if (lane == 0 && events) atomicAdd(&sh_ev, events);
+    __syncthreads();
+    if (threadIdx.x == 0 && sh_ev) atomicAdd(&s.ctl->events, sh_ev);
 }
 
 // ------------------------------------------------------------ exports

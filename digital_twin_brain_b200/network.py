@@ -12,8 +12,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import (DTB_DEVICE, DTB_HOST, FIELD_ACTIVE, FIELD_I_SYN, FIELD_I_UI, FIELD_J, FIELD_NEW_ACTIVE,
-                   FIELD_STEP, FIELD_SUB_COUNT, FIELD_T, FIELD_T_LAST, FIELD_V, MODES)
+from ._lib import (DTB_DEVICE, DTB_HOST, FIELD_ACTIVE, FIELD_EVENTS, FIELD_I_SYN, FIELD_I_UI, FIELD_J,
+                   FIELD_NEW_ACTIVE, FIELD_STEP, FIELD_SUB_COUNT, FIELD_T, FIELD_T_LAST, FIELD_V, MODES)
 from .synthetic import NetworkSpec
 
 _FIELD_SHAPE = {FIELD_V: (1, np.float32), FIELD_J: (4, np.float32), FIELD_I_UI: (4, np.float32),
@@ -137,6 +137,20 @@ class Network:
                   DTB_HOST)
         return s, mn, na
 
+    def set_stream(self, stream):
+        """Issue all of this network's work on `stream` (a torch.cuda.Stream or a raw cudaStream_t int)."""
+        raw = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        _lib.call("dtb_block_set_stream", self._h, ctypes.c_void_p(raw))
+
+    def time_kernels(self, n_steps: int, noise_rate: float | None = 0.01, isolated: bool = False,
+                     mode: str = "auto") -> dict:
+        """Per-kernel CUDA-event timing of n_steps (no graphs)."""
+        out = np.zeros(4, np.float32)
+        rate = -1.0 if noise_rate is None else float(noise_rate)
+        _lib.call("dtb_block_time_kernels", self._h, int(n_steps), rate, int(bool(isolated)), MODES[mode], _ptr(out))
+        return dict(update_ms=float(out[0]), propagate_ms=float(out[1]), step_ms=float(out[2]),
+                    events_per_step=float(out[3]))
+
     def step_forced(self, forced_active=None, forced_new_active=None, noise_rate: float | None = 0.01,
                     isolated: bool = False, mode: str = "pull"):
         """One step with this step's active / new_active sets replaced (teacher forcing)."""
@@ -156,7 +170,7 @@ class Network:
             out = np.zeros(1, np.float32)
             _lib.call("dtb_block_get", self._h, field, _ptr(out), DTB_HOST)
             return float(out[0])
-        if field == FIELD_STEP:
+        if field in (FIELD_STEP, FIELD_EVENTS):
             out = np.zeros(1, np.uint64)
             _lib.call("dtb_block_get", self._h, field, _ptr(out), DTB_HOST)
             return int(out[0])

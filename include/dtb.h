@@ -57,7 +57,8 @@ typedef enum {
     DTB_FIELD_NEW_ACTIVE = 6, /* uint8[N]      spikes | noise     models/block.py:136 */
     DTB_FIELD_T = 7,          /* float[1]      block.t            models/block.py:58  */
     DTB_FIELD_STEP = 8,       /* uint64[1]     steps taken (Philox step counter) */
-    DTB_FIELD_SUB_COUNT = 9   /* uint32[n_sub] neurons per subblock */
+    DTB_FIELD_SUB_COUNT = 9,  /* uint32[n_sub] neurons per subblock */
+    DTB_FIELD_EVENTS = 10     /* uint64[1]     synaptic events propagated since creation */
 } dtb_field;
 
 typedef struct dtb_block dtb_block;
@@ -121,6 +122,7 @@ typedef struct {
     int64_t device_bytes;    /* device memory held by the handle */
     int64_t max_outdegree;
     int64_t max_indegree;
+    int64_t kernel_launches; /* kernels enqueued so far (graph nodes counted) */
 } dtb_block_info;
 
 /* ---- library ------------------------------------------------------------ */
@@ -174,6 +176,15 @@ int dtb_block_run(dtb_block* b, int n_steps, float noise_rate, int isolated, int
 int dtb_block_step_forced(dtb_block* b, float noise_rate, int isolated, int mode,
                           const uint8_t* forced_active, const uint8_t* forced_new_active,
                           float* sum_out, float* mean_out, int where);
+
+/* Measurement hook (the per-iteration timers of cuda/tools/benchmark.cpp:
+ * 2289-2316, per kernel): runs n_steps with CUDA events around every kernel
+ * launch (no graphs) and writes out_ms[0] = mean duration of the kernels that
+ * update neurons (fused with the gather in pull mode), out_ms[1] = mean
+ * duration of the propagation-only kernels (push scatter, final gather),
+ * out_ms[2] = mean wall time of a step on the stream, out_ms[3] = mean
+ * synaptic events per step. */
+int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isolated, int mode, float* out_ms);
 
 /* ---- state access ------------------------------------------------------- */
 
