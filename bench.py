@@ -185,9 +185,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     net.run(W, noise_rate=args.noise, mode="auto", out=None)
     tune = {}
     if args.mode == "tune":
-        for m in ("push", "pull"):
-            tune[m] = net.time_kernels(32, noise_rate=args.noise, mode=m)
-        mode = min(tune, key=lambda m: tune[m]["step_ms"])
+        tune = net.autotune(32, noise_rate=args.noise)
+        mode = "push" if tune["push_ms"] <= tune["pull_ms"] else "pull"
     else:
         mode = args.mode
     kt = net.time_kernels(64, noise_rate=args.noise, mode=mode)

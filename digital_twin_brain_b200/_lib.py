@@ -22,6 +22,8 @@ MODES = {"auto": MODE_AUTO, "push": MODE_PUSH, "pull": MODE_PULL}
 FIELD_V, FIELD_J, FIELD_I_UI, FIELD_I_SYN, FIELD_T_LAST, FIELD_ACTIVE, FIELD_NEW_ACTIVE, FIELD_T, FIELD_STEP, \
     FIELD_SUB_COUNT, FIELD_EVENTS = range(11)
 
+TUNE_SCATTER_WORDS, TUNE_CHUNK, TUNE_PULL_THRESHOLD_PPM, TUNE_USE_GRAPHS = range(4)
+
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "out of memory", 4: "I/O error", 5: "format error",
           6: "invalid state", 7: "limit exceeded"}
 
@@ -66,6 +68,9 @@ _SIGS = {
     "dtb_block_run": [c_vp, c_int, c_f32, c_int, c_int, c_vp, c_vp, c_vp, c_int],
     "dtb_block_step_forced": [c_vp, c_f32, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_int],
     "dtb_block_time_kernels": [c_vp, c_int, c_f32, c_int, c_int, c_vp],
+    "dtb_block_set_tuning": [c_vp, c_int, c_i64],
+    "dtb_block_get_tuning": [c_vp, c_int, ctypes.POINTER(c_i64)],
+    "dtb_block_autotune": [c_vp, c_int, c_f32, c_vp],
     "dtb_block_get": [c_vp, c_int, c_vp, c_int],
     "dtb_block_set": [c_vp, c_int, c_vp, c_int],
     "dtb_block_get_csr": [c_vp, c_int, c_vp, c_vp, c_vp, c_int],

@@ -156,6 +156,7 @@ struct dtb_block {
     double last_frac = -1.0;
     double pull_threshold = 0.05;
     int chunk = 32;
+    int scatter_wpw = 32;         // bitmask words per warp in the push scatter
     // graphs: [mode][isolated-agnostic] chunk graphs
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
     int graph_len[3] = {0, 0, 0};
@@ -460,10 +461,11 @@ static int launch_gather_only(dtb_block* b, const DevState& s)
 
 static int launch_scatter(dtb_block* b, const DevState& s)
 {
-    const int64_t warps = (s.n_words + 31) / 32;
+    const int wpw = b->scatter_wpw;
+    const int64_t warps = (s.n_words + wpw - 1) / wpw;
     const unsigned grid = grid_for(warps * 32, 256);
     if (grid == 0) return DTB_OK;
-    k_scatter<<<grid, 256, 0, b->stream>>>(s);
+    k_scatter<<<grid, 256, 0, b->stream>>>(s, wpw);
     CK(cudaGetLastError());
     b->launches++;
     return DTB_OK;
@@ -988,6 +990,81 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
     out_ms[1] = cnt[1] ? (float)(sum[1] / cnt[1]) : 0.0f;
     out_ms[2] = done_steps ? total / (float)done_steps : 0.0f;
     out_ms[3] = done_steps ? (float)((double)(ev1 - ev0) / done_steps) : 0.0f;
+    return DTB_OK;
+}
+
+static void drop_graphs(dtb_block* b)
+{
+    for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+}
+
+int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
+{
+    if (!b) return fail(DTB_ERR_ARG, "null handle");
+    switch (key) {
+    case DTB_TUNE_SCATTER_WORDS:
+        if (value < 1 || value > 32) return fail(DTB_ERR_ARG, "scatter words per warp must be 1..32");
+        b->scatter_wpw = (int)value;
+        break;
+    case DTB_TUNE_CHUNK:
+        if (value < 1 || value > 4096) return fail(DTB_ERR_ARG, "chunk must be 1..4096");
+        b->chunk = (int)value;
+        break;
+    case DTB_TUNE_PULL_THRESHOLD_PPM:
+        if (value < 0) return fail(DTB_ERR_ARG, "threshold must be >= 0");
+        b->pull_threshold = (double)value * 1e-6;
+        break;
+    case DTB_TUNE_USE_GRAPHS: b->use_graphs = value != 0; break;
+    default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
+    }
+    drop_graphs(b);
+    return DTB_OK;
+}
+
+int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value)
+{
+    if (!b || !value) return fail(DTB_ERR_ARG, "null argument");
+    switch (key) {
+    case DTB_TUNE_SCATTER_WORDS: *value = b->scatter_wpw; break;
+    case DTB_TUNE_CHUNK: *value = b->chunk; break;
+    case DTB_TUNE_PULL_THRESHOLD_PPM: *value = (int64_t)std::llround(b->pull_threshold * 1e6); break;
+    case DTB_TUNE_USE_GRAPHS: *value = b->use_graphs ? 1 : 0; break;
+    default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
+    }
+    return DTB_OK;
+}
+
+int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* report)
+{
+    if (!b || n_steps < 2) return fail(DTB_ERR_ARG, "bad argument");
+    float best_ms = 1e30f, push_ms = 0.0f, pull_ms = 0.0f, ev = 0.0f;
+    int best_w = b->scatter_wpw;
+    if (b->has_push) {
+        const int cand[6] = {1, 2, 4, 8, 16, 32};
+        for (int w : cand) {
+            b->scatter_wpw = w;
+            float o[4];
+            RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PUSH, o));
+            if (o[2] < best_ms) { best_ms = o[2]; best_w = w; ev = o[3]; }
+        }
+        b->scatter_wpw = best_w;
+        push_ms = best_ms;
+    }
+    if (b->has_pull) {
+        float o[4];
+        RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PULL, o));
+        pull_ms = o[2];
+        if (!b->has_push) ev = o[3];
+    }
+    // activity fraction of the tuned steps; push cost grows with it, pull cost hardly does
+    const double deg = b->N ? (double)b->S / (double)b->N : 1.0;
+    const double f = deg > 0 ? (double)ev / deg / (double)std::max<int64_t>(1, b->N) : 0.0;
+    if (b->has_push && b->has_pull && push_ms > 0.0f) b->pull_threshold = f * (double)pull_ms / (double)push_ms;
+    drop_graphs(b);
+    if (report) {
+        report[0] = (float)best_w; report[1] = push_ms; report[2] = pull_ms; report[3] = (float)f;
+        report[4] = (float)b->pull_threshold;
+    }
     return DTB_OK;
 }
 

@@ -236,25 +236,44 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
                                  (uint32_t)s.seed, (uint32_t)(s.seed >> 32));
     const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
 
+    // Phase 1: issue every load of the lane's four neurons before any store, so
+    // their memory latencies overlap (the stores below could alias them).
+    bool valid[4];
+    float v_in[4], tl_in[4];
+    float4 J_in[4];
+    uint32_t c_in[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t n = base + j * 32 + lane;
+        valid[j] = n < s.N;
+        if (valid[j]) {
+            v_in[j] = s.V[n];
+            tl_in[j] = s.tlast[n];
+            c_in[j] = __ldg(s.cls + n);
+            if (!GATHER) J_in[j] = s.J[n];
+        }
+    }
+    // Phase 2: arithmetic (models/block.py:83-111 order).
     int mysub[4];
     bool act[4], nav[4];
+    float v_out[4];
+    float4 J_out[4];
     double vsum_lane = 0.0;
     bool any_valid = false;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int64_t n = base + j * 32 + lane;
         act[j] = false; nav[j] = false; mysub[j] = -1;
-        if (n < s.N) {
+        if (valid[j]) {
             any_valid = true;
-            const ParamClass p = load_class(s.pc, __ldg(s.cls + n));
-            const float v = s.V[n];
-            const float4 J = GATHER ? Jn[j] : s.J[n];
-            const float tl = s.tlast[n];
+            const ParamClass p = load_class(s.pc, c_in[j]);
+            const float v = v_in[j];
+            const float4 J = GATHER ? Jn[j] : J_in[j];
             const float isyn = use_override ? s.isyn_override[n] : isyn_of(p, v, J);
             const float mainp = __fmul_rn(-p.gL, __fsub_rn(v, p.VL));
             const float cd = __fadd_rn(__fadd_rn(mainp, isyn), p.Iext);
             const float vn = __fadd_rn(v, __fmul_rn(p.rCdt, cd));
-            const bool notsat = t >= __fadd_rn(tl, p.Tref);
+            const bool notsat = t >= __fadd_rn(tl_in[j], p.Tref);
             const float vs = notsat ? vn : p.Vreset;
             bool a = vs >= p.Vth;
             const float vmin = isnan(vs) ? vs : (isnan(p.Vth) ? p.Vth : (vs < p.Vth ? vs : p.Vth));
@@ -263,11 +282,20 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
             const bool nz = u01(words[j]) < rate;
             bool na = isolated ? nz : (nz || a);
             if (FORCED && s.forced_new) na = (__ldg(s.forced_new + (n >> 5)) >> (n & 31)) & 1u;
-            s.V[n] = vmin;
-            s.J[n] = mul4(J, p.decay);
-            if (a) s.tlast[n] = t;
+            v_out[j] = vmin;
+            J_out[j] = mul4(J, p.decay);
             act[j] = a; nav[j] = na; mysub[j] = p.sub;
             vsum_lane += (double)vmin;
+        }
+    }
+    // Phase 3: stores.
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t n = base + j * 32 + lane;
+        if (valid[j]) {
+            s.V[n] = v_out[j];
+            s.J[n] = J_out[j];
+            if (act[j]) s.tlast[n] = t;
         }
     }
 
@@ -307,7 +335,7 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
                 if (sb >= 0 && sb < s.n_sub) {
                     if (act[j]) atomicAdd(s.sub_spk + sb, 1u);
                     if (nav[j]) atomicAdd(s.sub_nact + sb, 1u);
-                    atomicAdd(s.sub_vsum + sb, (double)s.V[n]);
+                    atomicAdd(s.sub_vsum + sb, (double)v_out[j]);
                 } else if (nav[j]) {
                     atomicAdd(s.unmapped_nact, 1u);
                 }
@@ -348,20 +376,23 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
 
 // ------------------------------------------------------------ push scatter
 // cuda/src/stage/presynaptic_voltage.cpp:152-266 restated for one device:
-// a warp takes 32 bitmask words (1024 presynaptic neurons), walks their set
-// bits in order and scatters each outgoing row with coalesced index/weight
-// loads and one float2 atomic per synapse into the pending J.
-__global__ void __launch_bounds__(256) k_scatter(DevState s)
+// a warp takes `wpw` bitmask words (32*wpw presynaptic neurons), walks their
+// set bits in order and scatters each outgoing row with coalesced
+// index/weight loads and one float2 atomic per synapse into the pending J.
+// Small `wpw` keeps the rows being scattered at any moment inside a narrow
+// window of neurons, so the destination J lines of intra-region synapses stay
+// in L2; the autotuner picks it.
+__global__ void __launch_bounds__(256) k_scatter(DevState s, int wpw)
 {
     const unsigned long long steps_done = s.ctl->steps_done;
     const uint32_t* __restrict__ bits = s.bits[(steps_done - 1ull) & 1ull];
     const int lane = threadIdx.x & 31;
     const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t w0 = warp_global * 32;
+    const int64_t w0 = warp_global * wpw;
     __shared__ unsigned long long sh_ev;
     if (threadIdx.x == 0) sh_ev = 0ull;
     __syncthreads();
-    const uint32_t word = (w0 + lane < s.n_words) ? __ldg(bits + w0 + lane) : 0u;
+    const uint32_t word = (lane < wpw && w0 + lane < s.n_words) ? __ldg(bits + w0 + lane) : 0u;
     unsigned lanes = __ballot_sync(0xffffffffu, word != 0u);
     unsigned long long events = 0;
     while (lanes) {

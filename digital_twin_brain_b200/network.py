@@ -151,6 +151,21 @@ class Network:
         return dict(update_ms=float(out[0]), propagate_ms=float(out[1]), step_ms=float(out[2]),
                     events_per_step=float(out[3]))
 
+    def set_tuning(self, key: int, value: int):
+        _lib.call("dtb_block_set_tuning", self._h, int(key), int(value))
+
+    def get_tuning(self, key: int) -> int:
+        v = ctypes.c_int64()
+        _lib.call("dtb_block_get_tuning", self._h, int(key), ctypes.byref(v))
+        return int(v.value)
+
+    def autotune(self, n_steps: int = 32, noise_rate: float = 0.01) -> dict:
+        """Pick the scatter launch shape and the push/pull threshold by measurement (advances the run)."""
+        r = np.zeros(5, np.float32)
+        _lib.call("dtb_block_autotune", self._h, int(n_steps), float(noise_rate), _ptr(r))
+        return dict(scatter_words=int(r[0]), push_ms=float(r[1]), pull_ms=float(r[2]), activity=float(r[3]),
+                    pull_threshold=float(r[4]))
+
     def step_forced(self, forced_active=None, forced_new_active=None, noise_rate: float | None = 0.01,
                     isolated: bool = False, mode: str = "pull"):
         """One step with this step's active / new_active sets replaced (teacher forcing)."""

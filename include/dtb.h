@@ -186,6 +186,25 @@ int dtb_block_step_forced(dtb_block* b, float noise_rate, int isolated, int mode
  * synaptic events per step. */
 int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isolated, int mode, float* out_ms);
 
+/* Schedule knobs (new: the reference has a fixed launch shape per kernel).
+ * DTB_TUNE_SCATTER_WORDS   bitmask words per warp in the push scatter (1..32)
+ * DTB_TUNE_CHUNK           steps per captured CUDA graph (1..4096)
+ * DTB_TUNE_PULL_THRESHOLD_PPM  activity fraction (parts per million of the
+ *                          neurons propagating per step) above which
+ *                          DTB_MODE_AUTO pulls instead of pushing
+ * DTB_TUNE_USE_GRAPHS      capture chunks in CUDA graphs (0/1) */
+enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3 };
+int dtb_block_set_tuning(dtb_block* b, int key, int64_t value);
+int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value);
+
+/* Autotuner: times the push scatter at 1, 2, 4, ..., 32 bitmask words per
+ * warp and the pull gather on the live network (n_steps each; the
+ * simulation advances), keeps the fastest scatter shape and sets the
+ * AUTO push/pull threshold from the measured costs at the current activity.
+ * report (nullable, 5 floats): words per warp, push ms/step, pull ms/step,
+ * activity fraction, threshold. */
+int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* report);
+
 /* ---- state access ------------------------------------------------------- */
 
 /* Getters of cuda/include/block.hpp:247-562 (get_*_gpu / get_*_cpu) and the

@@ -161,6 +161,36 @@ def _oracle_for(spec):
     return O.OracleBlock(prop, decay_like_reference(prop, spec.dt), rowptr, pre, kind, w, spec.dt, spec.seed)
 
 
+def test_autotune_and_tuning_knobs():
+    from digital_twin_brain_b200._lib import TUNE_CHUNK, TUNE_SCATTER_WORDS
+    spec = synthetic.single_block(20000, 100, name="n20k_tune")
+    net = Network.from_spec(spec, device=0)
+    net.run(60, out=None)
+    r = net.autotune(8)
+    assert r["scatter_words"] in (1, 2, 4, 8, 16, 32) and r["push_ms"] > 0 and r["pull_ms"] > 0
+    assert net.get_tuning(TUNE_SCATTER_WORDS) == r["scatter_words"]
+    net.set_tuning(TUNE_CHUNK, 7)
+    assert net.get_tuning(TUNE_CHUNK) == 7
+    with pytest.raises(Exception):
+        net.set_tuning(TUNE_SCATTER_WORDS, 0)
+
+
+@pytest.mark.parametrize("wpw", [1, 4, 32])
+def test_scatter_shapes_agree_with_pull_under_forcing(wpw):
+    """One push step from identical state at several launch shapes vs the exact pull step."""
+    from digital_twin_brain_b200._lib import TUNE_SCATTER_WORDS
+    spec = synthetic.single_block(8000, 100, name="n8k")
+    a = Network.from_spec(spec, device=0)
+    b = Network.from_spec(spec, device=0)
+    a.set_tuning(TUNE_SCATTER_WORDS, wpw)
+    for _ in range(80):
+        a.run(1, mode="push")
+        b.run(1, mode="pull")
+        # resynchronise b onto a's state so every step starts identical
+        b.set(FIELD_V, a.get(FIELD_V)); b.set(FIELD_J, a.get(FIELD_J)); b.set(FIELD_T_LAST, a.get(FIELD_T_LAST))
+    np.testing.assert_allclose(a.get(FIELD_J), b.get(FIELD_J), rtol=1e-5, atol=1e-6)
+
+
 def test_chunked_and_graph_runs_are_identical():
     spec = synthetic.single_block(5000, 50, name="n5k")
     a = Network.from_spec(spec, device=0)
@@ -257,8 +287,9 @@ def test_attached_bold_matches_oracle():
     for k in range(300):
         act = np.array([s[k].sum() / spec.N], np.float64)
         out = O.bold_step(np.maximum(act, 1e-5), *st, params, spec.dt / 1000.0)
-    np.testing.assert_allclose(net.get_bold("bold"), out, rtol=1e-12)
-    np.testing.assert_allclose(net.get_bold("q"), st[1], rtol=1e-12)
+    # float64 on both sides; device pow and host pow differ in the last bits, which 300 steps accumulate
+    np.testing.assert_allclose(net.get_bold("bold"), out, rtol=1e-8)
+    np.testing.assert_allclose(net.get_bold("q"), st[1], rtol=1e-8)
 
 
 # ---------------------------------------------------------------- BOLD drop-in
