@@ -274,6 +274,73 @@ int dtb_block_attach_bold(dtb_block* b, int n_regions, const int32_t* sub_to_reg
 /* field: 0 s, 1 q, 2 v, 3 f_in, 4 bold output of the last step, 5 act of the last step; double[R]. */
 int dtb_block_get_bold(dtb_block* b, int field, double* dst, int where);
 
+/* ---- one step without any allocation ------------------------------------ */
+
+/* One parameter class (a deduplicated property row with its derived
+ * constants), in the layout the step kernels read.  rC_dt = (1.0f / C) * dt
+ * and decay[c] = expf(-dt / tau_c) (as float32 operations, tau_c = property
+ * cols 18-21) reproduce models/block.py:71,92. */
+typedef struct {
+    float g[4];      /* g_ui (property cols 10-13) */
+    float V_ui[4];   /* cols 14-17 */
+    float decay[4];  /* exp(-dt / tau_ui), tau = cols 18-21 */
+    float g_L, V_L;  /* cols 6, 7 */
+    float rC_dt;     /* (1 / C) * dt, C = col 4 */
+    float V_th, V_reset, T_ref, I_ext, noise_rate;  /* cols 8, 9, 5, 2, 0 */
+    int32_t subblock;                               /* col 3, -1 when not a whole number >= 0 */
+    float C, pad0, pad1;
+} dtb_param_class;
+
+/* A network whose device arrays all belong to the caller. */
+typedef struct {
+    int64_t n_neurons;                /* <= DTB_PREALLOC_MAX_NEURONS */
+    int32_t n_subblocks;              /* <= DTB_PREALLOC_MAX_SUBBLOCKS */
+    int32_t device;
+    float* V;                         /* [N] in/out */
+    float* J;                         /* [N][4] in/out (AMPA, NMDA, GABAa, GABAb per neuron) */
+    float* t_last;                    /* [N] in/out */
+    const uint32_t* cls;              /* [N] class of every neuron */
+    const dtb_param_class* classes;   /* class table */
+    const uint32_t* sub_count;        /* [n_subblocks] neurons per subblock (divides the mean V) */
+    const int64_t* rowptr;            /* pull CSR: [N+1], rows = postsynaptic neurons */
+    const uint32_t* index;            /* [S] presynaptic neuron | bit 31 for a GABAa/GABAb synapse */
+    const float* weight;              /* [S][2] */
+    float dt;
+    uint64_t seed;
+    uint32_t stream_id;
+} dtb_prealloc_net;
+
+#define DTB_PREALLOC_MAX_NEURONS (1 << 22)
+#define DTB_PREALLOC_MAX_SUBBLOCKS 1024
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory themselves or let a library do it: code that runs inside another
+ * framework's fixed memory pool or budget, or a real-time loop in which an
+ * allocation (and the device-wide synchronisation cudaMalloc/cudaFree can
+ * bring) is not allowed.  It advances such a caller-owned network by one time
+ * step, exactly as dtb_block_run(..., DTB_MODE_PULL, ...) advances a handle
+ * (bit-identical results), and calls no cudaMalloc, cudaFree or allocating
+ * library routine.
+ *
+ * Its scratch memory (spike bitmasks, subblock accumulators, control block;
+ * about 1.05 MB) is one fixed static device array inside libdtb.so, which
+ * every GPU that loads the library holds until the process exits; hence the
+ * limits DTB_PREALLOC_MAX_NEURONS and DTB_PREALLOC_MAX_SUBBLOCKS, beyond which
+ * the call returns DTB_ERR_LIMIT (bad pointers or dt: DTB_ERR_ARG; a failed
+ * launch: DTB_ERR_CUDA; this call reports by status code only).  The first call on a device looks up the
+ * array's device address (with that device current); make that first call
+ * before any stream capture.  All calls share the array and every call
+ * re-initialises what it uses, but calls whose work overlaps on the GPU (two
+ * streams, two host threads) race on it: serialise them.
+ *
+ * t is block.t before the step and step the number of steps already taken
+ * (the noise counter); after the call block.t is float32(t + dt).  sum_out /
+ * mean_out (device, [n_subblocks], nullable) receive the step's spike count
+ * and mean V per subblock.  Work is issued on `stream` (a cudaStream_t,
+ * NULL = legacy default stream); the call does not synchronise. */
+int dtb_step_preallocated(const dtb_prealloc_net* net, float t, uint64_t step, float noise_rate, int isolated,
+                          float* sum_out, float* mean_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
