@@ -87,7 +87,7 @@ _SIGS = {
     "dtb_bold_state_update": [c_vp, c_vp, c_i64, c_i64, c_i64, c_int],
     "dtb_bold_get": [c_vp, c_int, c_vp, c_int],
     "dtb_bold_set": [c_vp, c_int, c_vp, c_int],
-    "dtb_block_attach_bold": [c_vp, c_int, c_vp, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64],
+    "dtb_block_attach_bold": [c_vp, c_int, c_vp, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64],
     "dtb_block_get_bold": [c_vp, c_int, c_vp, c_int],
     "dtb_step_preallocated": [c_vp, c_f32, c_u64, c_f32, c_int, c_vp, c_vp, c_vp],
 }

@@ -463,9 +463,9 @@ static int launch_scatter(dtb_block* b, const DevState& s)
 {
     const int wpw = b->scatter_wpw;
     const int64_t warps = (s.n_words + wpw - 1) / wpw;
-    const unsigned grid = grid_for(warps * 32, 256);
+    const unsigned grid = grid_for(warps * 32, kScatterThreads);
     if (grid == 0) return DTB_OK;
-    k_scatter<<<grid, 256, 0, b->stream>>>(s, wpw);
+    k_scatter<<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
     CK(cudaGetLastError());
     b->launches++;
     return DTB_OK;
@@ -1510,9 +1510,9 @@ int dtb_bold_set(dtb_bold* m, int field, const void* srcp, int where)
 
 // ------------------------------------------------------------ block-attached BOLD
 int dtb_block_attach_bold(dtb_block* b, int n_regions, const int32_t* sub_to_region, double epsilon, double tao_s,
-                          double tao_f, double tao_0, double alpha, double E_0, double V_0)
+                          double tao_f, double tao_0, double alpha, double E_0, double V_0, double delta_t)
 {
-    if (!b || n_regions <= 0 || !sub_to_region) return fail(DTB_ERR_ARG, "bad argument");
+    if (!b || n_regions <= 0 || !sub_to_region || !(delta_t > 0.0)) return fail(DTB_ERR_ARG, "bad argument");
     DeviceGuard g(b->device);
     std::vector<double> rn((size_t)n_regions, 0.0);
     for (int i = 0; i < b->n_sub; ++i) {
@@ -1536,7 +1536,7 @@ int dtb_block_attach_bold(dtb_block* b, int n_regions, const int32_t* sub_to_reg
     bd.s = st; bd.q = st + n_regions; bd.v = st + 2 * n_regions; bd.f = st + 3 * n_regions;
     bd.act = st + 4 * n_regions; bd.out = st + 5 * n_regions;
     bd.epsilon = epsilon; bd.tao_s = tao_s; bd.tao_f = tao_f; bd.tao_0 = tao_0; bd.div_alpha = 1.0 / alpha;
-    bd.E0 = E_0; bd.V0 = V_0; bd.delta_t = (double)b->dt / 1000.0;
+    bd.E0 = E_0; bd.V0 = V_0; bd.delta_t = delta_t;
     b->bold_R = n_regions;
     for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
     return DTB_OK;

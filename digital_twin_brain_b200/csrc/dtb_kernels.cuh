@@ -246,6 +246,7 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
     for (int j = 0; j < 4; ++j) {
         const int64_t n = base + j * 32 + lane;
         valid[j] = n < s.N;
+        c_in[j] = 0u;              // class 0 exists whenever N > 0: keeps the shuffle below in bounds
         if (valid[j]) {
             v_in[j] = s.V[n];
             tl_in[j] = s.tlast[n];
@@ -253,40 +254,53 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
             if (!GATHER) J_in[j] = s.J[n];
         }
     }
-    // Phase 2: arithmetic (models/block.py:83-111 order).
+    // Phase 2: arithmetic (models/block.py:83-111 order).  When the warp's 128
+    // neurons share one parameter class (the usual case: classes are region x
+    // E/I ranges), the class is loaded once for the warp.
     int mysub[4];
     bool act[4], nav[4];
     float v_out[4];
     float4 J_out[4];
     double vsum_lane = 0.0;
     bool any_valid = false;
+    auto neuron = [&](int j, const ParamClass& p) {
+        const int64_t n = base + j * 32 + lane;
+        const float v = v_in[j];
+        const float4 J = GATHER ? Jn[j] : J_in[j];
+        const float isyn = use_override ? s.isyn_override[n] : isyn_of(p, v, J);
+        const float mainp = __fmul_rn(-p.gL, __fsub_rn(v, p.VL));
+        const float cd = __fadd_rn(__fadd_rn(mainp, isyn), p.Iext);
+        const float vn = __fadd_rn(v, __fmul_rn(p.rCdt, cd));
+        const bool notsat = t >= __fadd_rn(tl_in[j], p.Tref);
+        const float vs = notsat ? vn : p.Vreset;
+        bool a = vs >= p.Vth;
+        const float vmin = isnan(vs) ? vs : (isnan(p.Vth) ? p.Vth : (vs < p.Vth ? vs : p.Vth));
+        if (FORCED && s.forced_active) a = (__ldg(s.forced_active + (n >> 5)) >> (n & 31)) & 1u;
+        const float rate = noise_rate >= 0.0f ? noise_rate : p.noise;
+        const bool nz = u01(words[j]) < rate;
+        bool na = isolated ? nz : (nz || a);
+        if (FORCED && s.forced_new) na = (__ldg(s.forced_new + (n >> 5)) >> (n & 31)) & 1u;
+        v_out[j] = vmin;
+        J_out[j] = mul4(J, p.decay);
+        act[j] = a; nav[j] = na; mysub[j] = p.sub;
+        vsum_lane += (double)vmin;
+    };
+    const uint32_t c0 = __shfl_sync(0xffffffffu, c_in[0], 0);
+    bool same = true;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const int64_t n = base + j * 32 + lane;
         act[j] = false; nav[j] = false; mysub[j] = -1;
-        if (valid[j]) {
-            any_valid = true;
-            const ParamClass p = load_class(s.pc, c_in[j]);
-            const float v = v_in[j];
-            const float4 J = GATHER ? Jn[j] : J_in[j];
-            const float isyn = use_override ? s.isyn_override[n] : isyn_of(p, v, J);
-            const float mainp = __fmul_rn(-p.gL, __fsub_rn(v, p.VL));
-            const float cd = __fadd_rn(__fadd_rn(mainp, isyn), p.Iext);
-            const float vn = __fadd_rn(v, __fmul_rn(p.rCdt, cd));
-            const bool notsat = t >= __fadd_rn(tl_in[j], p.Tref);
-            const float vs = notsat ? vn : p.Vreset;
-            bool a = vs >= p.Vth;
-            const float vmin = isnan(vs) ? vs : (isnan(p.Vth) ? p.Vth : (vs < p.Vth ? vs : p.Vth));
-            if (FORCED && s.forced_active) a = (__ldg(s.forced_active + (n >> 5)) >> (n & 31)) & 1u;
-            const float rate = noise_rate >= 0.0f ? noise_rate : p.noise;
-            const bool nz = u01(words[j]) < rate;
-            bool na = isolated ? nz : (nz || a);
-            if (FORCED && s.forced_new) na = (__ldg(s.forced_new + (n >> 5)) >> (n & 31)) & 1u;
-            v_out[j] = vmin;
-            J_out[j] = mul4(J, p.decay);
-            act[j] = a; nav[j] = na; mysub[j] = p.sub;
-            vsum_lane += (double)vmin;
-        }
+        if (valid[j]) { any_valid = true; same = same && (c_in[j] == c0); }
+    }
+    if (__all_sync(0xffffffffu, same)) {
+        const ParamClass p = load_class(s.pc, c0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (valid[j]) neuron(j, p);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (valid[j]) neuron(j, load_class(s.pc, c_in[j]));
     }
     // Phase 3: stores.
 #pragma unroll
@@ -340,6 +354,7 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
                     atomicAdd(s.unmapped_nact, 1u);
                 }
             }
+            __threadfence();   // this lane's atomics before the CTA's done-count
             if (lane == 0) sh_sub[wid] = -1;
         }
     } else if (lane == 0) {
@@ -360,10 +375,7 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
             cs += sh_spk[w]; cn += sh_nact[w]; cv += sh_vsum[w];
         }
         if (cur >= 0) { atomicAdd(s.sub_spk + cur, cs); atomicAdd(s.sub_nact + cur, cn); atomicAdd(s.sub_vsum + cur, cv); }
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
+        __threadfence();   // the CTA's statistics before its done-count
         const unsigned prev = atomicAdd(&s.ctl->done, 1u);
         sh_last = (prev == gridDim.x - 1u);
     }
@@ -375,42 +387,97 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
 }
 
 // ------------------------------------------------------------ push scatter
-// cuda/src/stage/presynaptic_voltage.cpp:152-266 restated for one device:
-// a warp takes `wpw` bitmask words (32*wpw presynaptic neurons), walks their
-// set bits in order and scatters each outgoing row with coalesced
-// index/weight loads and one float2 atomic per synapse into the pending J.
-// Small `wpw` keeps the rows being scattered at any moment inside a narrow
-// window of neurons, so the destination J lines of intra-region synapses stay
-// in L2; the autotuner picks it.
-__global__ void __launch_bounds__(256) k_scatter(DevState s, int wpw)
+// cuda/src/stage/presynaptic_voltage.cpp:152-266 restated for one device.
+// A warp owns `wpw` bitmask words (32*wpw presynaptic neurons).  It lists the
+// set bits in shared memory, then takes them 32 rows at a time: every lane
+// loads one row's bounds, a warp scan turns the row lengths into offsets, and
+// the lanes walk the concatenated synapses of the 32 rows together (four
+// independent index/weight loads in flight per lane), each synapse adding its
+// weight pair to the pending J with one float2 atomic.  Small `wpw` keeps the
+// rows scattered at any moment inside a narrow window of neurons, so the
+// destination J lines of intra-region synapses stay in L2.
+constexpr int kScatterThreads = 256;
+constexpr int kScatterMaxWords = 32;
+
+__global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw)
 {
+    __shared__ uint32_t sh_rows[kScatterThreads / 32][kScatterMaxWords * 32];
+    __shared__ unsigned long long sh_ev;
     const unsigned long long steps_done = s.ctl->steps_done;
     const uint32_t* __restrict__ bits = s.bits[(steps_done - 1ull) & 1ull];
     const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
     const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t w0 = warp_global * wpw;
-    __shared__ unsigned long long sh_ev;
     if (threadIdx.x == 0) sh_ev = 0ull;
     __syncthreads();
-    const uint32_t word = (lane < wpw && w0 + lane < s.n_words) ? __ldg(bits + w0 + lane) : 0u;
-    unsigned lanes = __ballot_sync(0xffffffffu, word != 0u);
+    uint32_t* rows = sh_rows[wid];
+    uint32_t word = (lane < wpw && w0 + lane < s.n_words) ? __ldg(bits + w0 + lane) : 0u;
+    // list the set bits of the window in neuron order
+    const int cnt = __popc(word);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    int pos = incl - cnt;
+    while (word) {
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        rows[pos++] = (uint32_t)((w0 + lane) * 32 + b);
+    }
+    __syncwarp();
     unsigned long long events = 0;
-    while (lanes) {
-        const int l = __ffs(lanes) - 1;
-        lanes &= lanes - 1;
-        uint32_t wl = __shfl_sync(0xffffffffu, word, l);
-        while (wl) {
-            const int b = __ffs(wl) - 1;
-            wl &= wl - 1;
-            const int64_t pre = (w0 + l) * 32 + b;
-            const int64_t e0 = __ldg(s.qrow + pre);
-            const int64_t e1 = __ldg(s.qrow + pre + 1);
-            events += (unsigned long long)(e1 - e0);
-            for (int64_t e = e0 + lane; e < e1; e += 32) {
-                const uint32_t c = __ldg(s.qcol + e);
-                const float2 w = __ldg(s.qw + e);
-                float2* dst = reinterpret_cast<float2*>(s.J + (c & kIndexMask)) + (c >> 31);
-                atomicAdd(dst, w);
+    for (int r0 = 0; r0 < total; r0 += 32) {
+        const bool has = r0 + lane < total;
+        int64_t e0 = 0, len = 0;
+        if (has) {
+            const uint32_t pre = rows[r0 + lane];
+            e0 = __ldg(s.qrow + pre);
+            len = __ldg(s.qrow + pre + 1) - e0;
+        }
+        // inclusive scan of the row lengths
+        int64_t off = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, off, o);
+            if (lane >= o) off += y;
+        }
+        const int64_t T = __shfl_sync(0xffffffffu, off, 31);
+        events += (unsigned long long)T;
+        const int64_t start = off - len;           // exclusive offset of this lane's row
+        for (int64_t v0 = 0; v0 < T; v0 += 128) {
+            uint32_t c[4];
+            float2 w[4];
+            bool ok[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int64_t v = v0 + u * 32 + lane;
+                // row of v: number of rows whose inclusive offset is <= v
+                int lo = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int64_t val = __shfl_sync(0xffffffffu, off, lo + step - 1);
+                    if (val <= v) lo += step;
+                }
+                const int src = lo < 31 ? lo : 31;
+                const int64_t rs = __shfl_sync(0xffffffffu, start, src);
+                const int64_t re0 = __shfl_sync(0xffffffffu, e0, src);
+                ok[u] = v < T;
+                if (ok[u]) {
+                    const int64_t e = re0 + (v - rs);
+                    c[u] = __ldg(s.qcol + e);
+                    w[u] = __ldg(s.qw + e);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (ok[u]) {
+                    float2* dst = reinterpret_cast<float2*>(s.J + (c[u] & kIndexMask)) + (c[u] >> 31);
+                    atomicAdd(dst, w[u]);
+                }
             }
         }
     }

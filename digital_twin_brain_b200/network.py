@@ -33,9 +33,10 @@ def _ptr(a):
 class Network:
     """A network of LIF neurons on one CUDA device (handle of ``dtb_block``)."""
 
-    def __init__(self, handle: ctypes.c_void_p, device: int):
+    def __init__(self, handle: ctypes.c_void_p, device: int, dt: float):
         self._h = handle
         self.device = int(device)
+        self.dt = float(dt)
         info = self.info()
         self.N = int(info.n_neurons)
         self.S = int(info.n_synapses)
@@ -61,7 +62,7 @@ class Network:
                            build_push=int(bool(build_push)))
         h = ctypes.c_void_p()
         _lib.call("dtb_block_create", ctypes.byref(d), ctypes.byref(h))
-        return cls(h, device)
+        return cls(h, device, dt)
 
     @classmethod
     def from_spec(cls, spec: NetworkSpec, device: int = 0, build_push: bool = True,
@@ -78,7 +79,7 @@ class Network:
                            stream_id=int(spec.stream_id), device=int(device), build_push=int(bool(build_push)))
         h = ctypes.c_void_p()
         _lib.call("dtb_block_create_synthetic", ctypes.byref(d), ctypes.byref(h))
-        return cls(h, device)
+        return cls(h, device, spec.dt)
 
     @classmethod
     def from_npz(cls, directory: str, dt: float, seed: int = 0, device: int = 0, build_push: bool = True,
@@ -87,7 +88,7 @@ class Network:
         h = ctypes.c_void_p()
         _lib.call("dtb_block_create_from_npz", directory.encode(), float(dt), int(seed), int(stream_id),
                   int(device), int(bool(build_push)), ctypes.byref(h))
-        return cls(h, device)
+        return cls(h, device, dt)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -247,10 +248,12 @@ class Network:
 
     # ------------------------------------------------------------ BOLD
     def attach_bold(self, sub_to_region, n_regions: int, epsilon=200, tao_s=0.8, tao_f=0.4, tao_0=1, alpha=0.2,
-                    E_0=0.8, V_0=0.02):
+                    E_0=0.8, V_0=0.02, delta_t: float | None = None):
+        """simulation/simulation.py:269-279 per step; delta_t defaults to dt / 1000 (seconds per step)."""
         s2r = np.ascontiguousarray(sub_to_region, np.int32)
+        dts = self.dt / 1000.0 if delta_t is None else float(delta_t)
         _lib.call("dtb_block_attach_bold", self._h, int(n_regions), _ptr(s2r), float(epsilon), float(tao_s),
-                  float(tao_f), float(tao_0), float(alpha), float(E_0), float(V_0))
+                  float(tao_f), float(tao_0), float(alpha), float(E_0), float(V_0), dts)
         self.n_regions = int(n_regions)
 
     def get_bold(self, field: str = "bold") -> np.ndarray:

@@ -265,12 +265,12 @@ int dtb_bold_set(dtb_bold* m, int field, const void* src, int where);
 
 /* Per-step BOLD driven by the block (simulation/simulation.py:269-279):
  * after every step, act[r] = (spikes of the subblocks mapped to region r) /
- * (neurons of those subblocks); BOLD.run(max(act, 1e-5)) in float64 with
- * delta_t = dt/1000 s.  sub_to_region[n_sub] (host) maps subblocks to
- * regions (-1: not in any region). */
+ * (neurons of those subblocks); BOLD.run(max(act, 1e-5)) in float64 with the
+ * given delta_t (seconds per step, e.g. 1e-4 for dt = 0.1 ms).
+ * sub_to_region[n_sub] (host) maps subblocks to regions (-1: none). */
 int dtb_block_attach_bold(dtb_block* b, int n_regions, const int32_t* sub_to_region,
                           double epsilon, double tao_s, double tao_f, double tao_0, double alpha,
-                          double E_0, double V_0);
+                          double E_0, double V_0, double delta_t);
 /* field: 0 s, 1 q, 2 v, 3 f_in, 4 bold output of the last step, 5 act of the last step; double[R]. */
 int dtb_block_get_bold(dtb_block* b, int field, double* dst, int where);
 

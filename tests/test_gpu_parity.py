@@ -287,9 +287,9 @@ def test_attached_bold_matches_oracle():
     for k in range(300):
         act = np.array([s[k].sum() / spec.N], np.float64)
         out = O.bold_step(np.maximum(act, 1e-5), *st, params, spec.dt / 1000.0)
-    # float64 on both sides; device pow and host pow differ in the last bits, which 300 steps accumulate
-    np.testing.assert_allclose(net.get_bold("bold"), out, rtol=1e-8)
-    np.testing.assert_allclose(net.get_bold("q"), st[1], rtol=1e-8)
+    # float64 on both sides; device pow and host pow may differ in the last bits
+    np.testing.assert_allclose(net.get_bold("bold"), out, rtol=1e-11)
+    np.testing.assert_allclose(net.get_bold("q"), st[1], rtol=1e-11)
 
 
 # ---------------------------------------------------------------- BOLD drop-in
