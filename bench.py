@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="tune", choices=["tune", "auto", "push", "pull"])
     ap.add_argument("--scale", type=float, default=1.0, help="whole-brain size scale (1.0 = ~2.2e9 synapses)")
+    ap.add_argument("--config", default="whole_brain", choices=["whole_brain", "one_region", "single_block"],
+                    help="whole_brain: 90 regions ~2.2e9 synapses (the headline); one_region: N=1e6, K=100; "
+                         "single_block: N=2000, K=100")
     ap.add_argument("--noise", type=float, default=0.01)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=400)
@@ -168,12 +171,17 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     dev = local_rank
     torch.cuda.set_device(dev)
-    spec = synthetic.config_whole_brain(args.scale) if args.scale != 1.0 else synthetic.config_whole_brain()
+    if args.config == "one_region":
+        spec = synthetic.config_one_region(args.noise)
+    elif args.config == "single_block":
+        spec = synthetic.config_single_block()
+    else:
+        spec = synthetic.config_whole_brain(args.scale) if args.scale != 1.0 else synthetic.config_whole_brain()
     spec.seed = 1000 + rank              # independent replica noise per rank
     spec.extra["noise"] = args.noise
     t_build = time.perf_counter()
     net = Network.from_spec(spec, device=dev, build_push=True)
-    net.attach_bold(spec.sub_to_region(), spec.R)
+    net.attach_bold(spec.sub_to_region(), spec.R, delta_t=spec.dt / 1000.0)
     stream = torch.cuda.Stream(device=dev)
     net.set_stream(stream)
     torch.cuda.synchronize(dev)
@@ -272,8 +280,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
                 "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
-                "config": {"workload": (f"whole_brain_90: 90 regions lognormal(ln 2.2e5, 0.5) x{args.scale}, "
-                                        f"N={N}, S={S}, K={spec.K}, 80% intra-region, dt=0.1 ms, "
+                "config": {"workload": (f"{spec.name}: {spec.R} regions"
+                                        + (f" lognormal(ln 2.2e5, 0.5) x{args.scale}" if args.config == "whole_brain" else "")
+                                        + f", N={N}, S={S}, K={spec.K}, 80% intra-region, dt=0.1 ms, "
                                         f"noise p={args.noise}, fp32 weights, BOLD per region"),
                            "method": mode, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                            "l2": "inputs larger than L2 (state ~1 GB, synapses ~27 GB per CSR)"},

@@ -122,6 +122,7 @@ struct dtb_block {
     int64_t N = 0, S = 0;
     int n_sub = 0, n_classes = 0;
     int pc_cap = 0, sub_cap = 0;
+    int n_sm = 148;
     ParamClass* d_pc = nullptr;
     uint32_t* d_sub_count = nullptr;
     float dt = 0.1f;
@@ -157,6 +158,7 @@ struct dtb_block {
     double pull_threshold = 0.05;
     int chunk = 32;
     int scatter_wpw = 32;         // bitmask words per warp in the push scatter
+    int step_variant = 0;         // 0: 2 resident CTAs/SM register budget, 1: 3
     // graphs: [mode][isolated-agnostic] chunk graphs
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
     int graph_len[3] = {0, 0, 0};
@@ -433,16 +435,56 @@ static int finish_create(dtb_block* b)
 }
 
 // ------------------------------------------------------------ launches
+// Persistent step kernels: as many CTAs as are resident at once, each warp
+// streaming a contiguous run of tiles.
+template <bool G, bool U, bool F, int M>
+static int step_blocks_per_sm()
+{
+    static int v = 0;
+    if (!v) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_step<G, U, F, M>, kStepThreads, 0);
+        if (v < 1) v = 1;
+    }
+    return v;
+}
+
+static void step_grid(const dtb_block* b, int per_sm, unsigned& grid, int& tiles_per_warp)
+{
+    const int64_t ntiles = (b->N + kWarpNeurons - 1) / kWarpNeurons;
+    const int warps = kStepThreads / 32;
+    const int64_t max_blocks = (int64_t)std::max(1, b->n_sm) * per_sm;
+    int64_t blocks = std::min<int64_t>((ntiles + warps - 1) / warps, max_blocks);
+    if (blocks < 1) blocks = 1;
+    const int64_t tpw = (ntiles + blocks * warps - 1) / (blocks * warps);
+    tiles_per_warp = (int)std::max<int64_t>(1, tpw);
+    grid = (unsigned)((ntiles + (int64_t)tiles_per_warp * warps - 1) / ((int64_t)tiles_per_warp * warps));
+}
+
+template <bool G, bool U, bool F, int M>
+static void launch_step_m(dtb_block* b, const DevState& s)
+{
+    unsigned grid;
+    int tpw;
+    step_grid(b, step_blocks_per_sm<G, U, F, M>(), grid, tpw);
+    k_step<G, U, F, M><<<grid, kStepThreads, 0, b->stream>>>(s, tpw);
+}
+
+template <bool G, bool U, bool F>
+static void launch_step(dtb_block* b, const DevState& s)
+{
+    if (b->step_variant == 1) launch_step_m<G, U, F, 3>(b, s);
+    else launch_step_m<G, U, F, 2>(b, s);
+}
+
 static int launch_update(dtb_block* b, const DevState& s, bool gather, bool forced)
 {
-    const unsigned grid = grid_for(s.N, kWarpNeurons * (kStepThreads / 32));
-    if (grid == 0) return DTB_OK;
+    if (s.N <= 0) return DTB_OK;
     if (forced) {
-        if (gather) k_step<true, true, true><<<grid, kStepThreads, 0, b->stream>>>(s);
-        else k_step<false, true, true><<<grid, kStepThreads, 0, b->stream>>>(s);
+        if (gather) launch_step<true, true, true>(b, s);
+        else launch_step<false, true, true>(b, s);
     } else {
-        if (gather) k_step<true, true, false><<<grid, kStepThreads, 0, b->stream>>>(s);
-        else k_step<false, true, false><<<grid, kStepThreads, 0, b->stream>>>(s);
+        if (gather) launch_step<true, true, false>(b, s);
+        else launch_step<false, true, false>(b, s);
     }
     CK(cudaGetLastError());
     b->launches++;
@@ -451,9 +493,8 @@ static int launch_update(dtb_block* b, const DevState& s, bool gather, bool forc
 
 static int launch_gather_only(dtb_block* b, const DevState& s)
 {
-    const unsigned grid = grid_for(s.N, kWarpNeurons * (kStepThreads / 32));
-    if (grid == 0) return DTB_OK;
-    k_step<true, false, false><<<grid, kStepThreads, 0, b->stream>>>(s);
+    if (s.N <= 0) return DTB_OK;
+    launch_step<true, false, false>(b, s);
     CK(cudaGetLastError());
     b->launches++;
     return DTB_OK;
@@ -601,6 +642,7 @@ static int create_common(dtb_block* b, int device, float dt, uint64_t seed, uint
     b->seed = seed;
     b->stream_id = stream_id;
     CK(cudaSetDevice(device));
+    CK(cudaDeviceGetAttribute(&b->n_sm, cudaDevAttrMultiProcessorCount, device));
     CK(cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking));
     b->stream = b->own_stream;
     return DTB_OK;
@@ -1015,6 +1057,10 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         b->pull_threshold = (double)value * 1e-6;
         break;
     case DTB_TUNE_USE_GRAPHS: b->use_graphs = value != 0; break;
+    case DTB_TUNE_STEP_VARIANT:
+        if (value < 0 || value > 1) return fail(DTB_ERR_ARG, "step variant must be 0 or 1");
+        b->step_variant = (int)value;
+        break;
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
     }
     drop_graphs(b);
@@ -1029,6 +1075,7 @@ int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value)
     case DTB_TUNE_CHUNK: *value = b->chunk; break;
     case DTB_TUNE_PULL_THRESHOLD_PPM: *value = (int64_t)std::llround(b->pull_threshold * 1e6); break;
     case DTB_TUNE_USE_GRAPHS: *value = b->use_graphs ? 1 : 0; break;
+    case DTB_TUNE_STEP_VARIANT: *value = b->step_variant; break;
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
     }
     return DTB_OK;
@@ -1039,6 +1086,18 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
     if (!b || n_steps < 2) return fail(DTB_ERR_ARG, "bad argument");
     float best_ms = 1e30f, push_ms = 0.0f, pull_ms = 0.0f, ev = 0.0f;
     int best_w = b->scatter_wpw;
+    {   // register budget of the update kernel
+        const int mode = b->has_push ? DTB_MODE_PUSH : DTB_MODE_PULL;
+        float best_u = 1e30f;
+        int best_v = 0;
+        for (int v = 0; v < 2; ++v) {
+            b->step_variant = v;
+            float o[4];
+            RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, mode, o));
+            if (o[0] < best_u) { best_u = o[0]; best_v = v; }
+        }
+        b->step_variant = best_v;
+    }
     if (b->has_push) {
         const int cand[6] = {1, 2, 4, 8, 16, 32};
         for (int w : cand) {
@@ -1063,7 +1122,7 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
     drop_graphs(b);
     if (report) {
         report[0] = (float)best_w; report[1] = push_ms; report[2] = pull_ms; report[3] = (float)f;
-        report[4] = (float)b->pull_threshold;
+        report[4] = (float)b->pull_threshold; report[5] = (float)b->step_variant;
     }
     return DTB_OK;
 }

@@ -160,212 +160,221 @@ __device__ void step_epilogue(const DevState& s, unsigned long long steps_done, 
     }
 }
 
-// Adds a warp-uniform event count (lane 0's copy) to the CTA total and, once
-// per CTA, to the device counter.
-__device__ __forceinline__ void cta_add_events(const DevState& s, uint32_t events, int lane, int wid)
-{
-    __shared__ unsigned long long sh_ev;
-    if (threadIdx.x == 0) sh_ev = 0ull;
-    __syncthreads();
-    if (lane == 0 && events) atomicAdd(&sh_ev, (unsigned long long)events);
-    __syncthreads();
-    if (threadIdx.x == 0 && sh_ev) atomicAdd(&s.ctl->events, sh_ev);
-    (void)wid;
-}
-
 // ------------------------------------------------------------ step kernel
-// One warp owns neurons n = base + 32 j + lane, j = 0..3 (base = 128 * warp):
-// coalesced loads, one Philox call per lane (words j), one bitmask word per j.
-template <bool GATHER, bool UPDATE, bool FORCED>
-__global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
+// Persistent: the grid is sized to the resident CTAs, and every warp streams a
+// contiguous run of 128-neuron tiles (tiles_per_warp of them).  In a tile a
+// lane owns neurons n = base + 32 j + lane, j = 0..3: coalesced loads, one
+// Philox call per lane (its four words), one bitmask word per j.  Per-subblock
+// statistics are kept in registers while consecutive tiles stay in one
+// subblock, so the CTA-wide barrier and the done-count happen once per CTA.
+// MINB = resident CTAs per SM the register budget is sized for (2: no spills,
+// 3: more warps, a few spills); the autotuner picks per network.
+template <bool GATHER, bool UPDATE, bool FORCED, int MINB = 2>
+__global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int tiles_per_warp)
 {
     constexpr int kWarps = kStepThreads / 32;
     __shared__ int sh_sub[kWarps];
     __shared__ uint32_t sh_spk[kWarps];
     __shared__ uint32_t sh_nact[kWarps];
     __shared__ double sh_vsum[kWarps];
+    __shared__ unsigned long long sh_ev[kWarps];
     __shared__ int sh_last;
 
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
-    const int64_t warp_global = (int64_t)blockIdx.x * kWarps + wid;
-    const int64_t base = warp_global * kWarpNeurons;
+    const int64_t warp_id = (int64_t)blockIdx.x * kWarps + wid;
     const unsigned long long steps_done = s.ctl->steps_done;
+    const int64_t ntiles = (s.N + kWarpNeurons - 1) / kWarpNeurons;
+    const int64_t tile0 = warp_id * tiles_per_warp;
+    const int64_t tile1 = tile0 + tiles_per_warp < ntiles ? tile0 + tiles_per_warp : ntiles;
 
-    float4 Jn[4];
-    if (GATHER) {
-        const uint32_t* gbits = s.bits[(steps_done - 1ull) & 1ull];
-        float4 sum[4];
-        uint32_t events = 0;
+    // update-phase constants (models/block.py:133-142)
+    const Ctl* ctl = s.ctl;
+    const float t = UPDATE ? __fadd_rn(ctl->t, s.dt) : 0.0f;
+    const float noise_rate = ctl->noise_rate;
+    const int isolated = ctl->isolated;
+    const bool use_override = UPDATE && ctl->use_isyn_override != 0u;
+    uint32_t* obits = s.bits[steps_done & 1ull];
+    const uint32_t* gbits = s.bits[(steps_done - 1ull) & 1ull];
+
+    // warp-level statistics carried across tiles (identical in every lane)
+    int cur_sub = -1;
+    uint32_t acc_spk = 0, acc_nact = 0;
+    double acc_v = 0.0;
+    unsigned long long acc_ev = 0;
+    bool flushed = false;
+
+    for (int64_t tile = tile0; tile < tile1; ++tile) {
+        const int64_t base = tile * kWarpNeurons;
+        float4 Jn[4];
+        if (GATHER) {
+            float4 sum[4];
+            uint32_t events = 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            sum[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int r = 0; r < 32; ++r) {
-                const int64_t n = base + j * 32 + r;
-                if (n >= s.N) break;
-                const float4 a = gather_row(s, gbits, n, lane, events);
-                if (lane == r) sum[j] = a;
+            for (int j = 0; j < 4; ++j) {
+                sum[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int r = 0; r < 32; ++r) {
+                    const int64_t n = base + j * 32 + r;
+                    if (n >= s.N) break;
+                    const float4 a = gather_row(s, gbits, n, lane, events);
+                    if (lane == r) sum[j] = a;
+                }
             }
-        }
-        cta_add_events(s, events, lane, wid);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int64_t n = base + j * 32 + lane;
-            if (n < s.N) Jn[j] = add4(s.J[n], sum[j]);   // models/block.py:71-73
-        }
-        if (!UPDATE) {
+            if (!s.qrow) acc_ev += events;   // no push rows to count from in the update
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int64_t n = base + j * 32 + lane;
-                if (n < s.N) s.J[n] = Jn[j];
+                if (n < s.N) Jn[j] = add4(__ldcs(s.J + n), sum[j]);   // models/block.py:71-73
             }
-            return;
+            if (!UPDATE) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t n = base + j * 32 + lane;
+                    if (n < s.N) __stcs(s.J + n, Jn[j]);
+                }
+                continue;
+            }
         }
-    }
 
-    // ---- update of step `steps_done` (models/block.py:133-142)
-    const Ctl* ctl = s.ctl;
-    const float t = __fadd_rn(ctl->t, s.dt);
-    const float noise_rate = ctl->noise_rate;
-    const int isolated = ctl->isolated;
-    const bool use_override = ctl->use_isyn_override != 0u;
-    uint32_t* obits = s.bits[steps_done & 1ull];
+        // ---- update of step `steps_done`
+        const U4 rnd = philox4x32_10(U4{(uint32_t)(tile * 32 + lane), s.stream_id, (uint32_t)steps_done,
+                                        (uint32_t)(steps_done >> 32)},
+                                     (uint32_t)s.seed, (uint32_t)(s.seed >> 32));
+        const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
 
-    const U4 rnd = philox4x32_10(U4{(uint32_t)(warp_global * 32 + lane), s.stream_id, (uint32_t)steps_done,
-                                    (uint32_t)(steps_done >> 32)},
-                                 (uint32_t)s.seed, (uint32_t)(s.seed >> 32));
-    const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
-
-    // Phase 1: issue every load of the lane's four neurons before any store, so
-    // their memory latencies overlap (the stores below could alias them).
-    bool valid[4];
-    float v_in[4], tl_in[4];
-    float4 J_in[4];
-    uint32_t c_in[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int64_t n = base + j * 32 + lane;
-        valid[j] = n < s.N;
-        c_in[j] = 0u;              // class 0 exists whenever N > 0: keeps the shuffle below in bounds
-        if (valid[j]) {
-            v_in[j] = s.V[n];
-            tl_in[j] = s.tlast[n];
-            c_in[j] = __ldg(s.cls + n);
-            if (!GATHER) J_in[j] = s.J[n];
-        }
-    }
-    // Phase 2: arithmetic (models/block.py:83-111 order).  When the warp's 128
-    // neurons share one parameter class (the usual case: classes are region x
-    // E/I ranges), the class is loaded once for the warp.
-    int mysub[4];
-    bool act[4], nav[4];
-    float v_out[4];
-    float4 J_out[4];
-    double vsum_lane = 0.0;
-    bool any_valid = false;
-    auto neuron = [&](int j, const ParamClass& p) {
-        const int64_t n = base + j * 32 + lane;
-        const float v = v_in[j];
-        const float4 J = GATHER ? Jn[j] : J_in[j];
-        const float isyn = use_override ? s.isyn_override[n] : isyn_of(p, v, J);
-        const float mainp = __fmul_rn(-p.gL, __fsub_rn(v, p.VL));
-        const float cd = __fadd_rn(__fadd_rn(mainp, isyn), p.Iext);
-        const float vn = __fadd_rn(v, __fmul_rn(p.rCdt, cd));
-        const bool notsat = t >= __fadd_rn(tl_in[j], p.Tref);
-        const float vs = notsat ? vn : p.Vreset;
-        bool a = vs >= p.Vth;
-        const float vmin = isnan(vs) ? vs : (isnan(p.Vth) ? p.Vth : (vs < p.Vth ? vs : p.Vth));
-        if (FORCED && s.forced_active) a = (__ldg(s.forced_active + (n >> 5)) >> (n & 31)) & 1u;
-        const float rate = noise_rate >= 0.0f ? noise_rate : p.noise;
-        const bool nz = u01(words[j]) < rate;
-        bool na = isolated ? nz : (nz || a);
-        if (FORCED && s.forced_new) na = (__ldg(s.forced_new + (n >> 5)) >> (n & 31)) & 1u;
-        v_out[j] = vmin;
-        J_out[j] = mul4(J, p.decay);
-        act[j] = a; nav[j] = na; mysub[j] = p.sub;
-        vsum_lane += (double)vmin;
-    };
-    const uint32_t c0 = __shfl_sync(0xffffffffu, c_in[0], 0);
-    bool same = true;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        act[j] = false; nav[j] = false; mysub[j] = -1;
-        if (valid[j]) { any_valid = true; same = same && (c_in[j] == c0); }
-    }
-    if (__all_sync(0xffffffffu, same)) {
-        const ParamClass p = load_class(s.pc, c0);
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (valid[j]) neuron(j, p);
-    } else {
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (valid[j]) neuron(j, load_class(s.pc, c_in[j]));
-    }
-    // Phase 3: stores.
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int64_t n = base + j * 32 + lane;
-        if (valid[j]) {
-            s.V[n] = v_out[j];
-            s.J[n] = J_out[j];
-            if (act[j]) s.tlast[n] = t;
-        }
-    }
-
-    uint32_t cnt_spk = 0, cnt_nact = 0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const uint32_t ma = __ballot_sync(0xffffffffu, act[j]);
-        const uint32_t mn = __ballot_sync(0xffffffffu, nav[j]);
-        const int64_t wi = warp_global * 4 + j;
-        if (lane == 0 && wi < s.n_words) { s.abits[wi] = ma; obits[wi] = mn; }
-        cnt_spk += __popc(ma);
-        cnt_nact += __popc(mn);
-    }
-
-    // ---- per-subblock statistics, aggregated per warp then per CTA
-    const bool warp_any = __any_sync(0xffffffffu, any_valid);
-    if (warp_any) {
-        const int sub0 = __shfl_sync(0xffffffffu, mysub[0], 0);
-        bool uni = true;
+        // Phase 1: every load of the lane's four neurons before any store, so their
+        // latencies overlap (the stores below could alias them).  Streaming hints:
+        // the state is touched once per step.
+        bool valid[4];
+        float v_in[4], tl_in[4];
+        float4 J_in[4];
+        uint32_t c_in[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int64_t n = base + j * 32 + lane;
-            if (n < s.N && mysub[j] != sub0) uni = false;
+            valid[j] = n < s.N;
+            c_in[j] = 0u;          // class 0 exists whenever N > 0: keeps the shuffle below in bounds
+            if (valid[j]) {
+                v_in[j] = __ldcs(s.V + n);
+                tl_in[j] = __ldcs(s.tlast + n);
+                c_in[j] = __ldcs(s.cls + n);
+                if (!GATHER) J_in[j] = __ldcs(s.J + n);
+            }
         }
-        uni = __all_sync(0xffffffffu, uni) && sub0 >= 0 && sub0 < s.n_sub;
+        // Phase 2: arithmetic (models/block.py:83-111 order), each neuron stored as
+        // soon as it is computed (all loads were issued above).  When the tile's 128
+        // neurons share one parameter class (classes are region x E/I ranges), the
+        // class is loaded once for the warp.
+        uint32_t act_m = 0, nav_m = 0;      // bit j: neuron j of this lane
+        int mysub0 = -1;
+        bool lane_uni = true;               // all of this lane's valid neurons in mysub0
+        double vsum_lane = 0.0;
+        uint32_t ev_lane = 0;
+        auto neuron = [&](int j, const ParamClass& p) {
+            const int64_t n = base + j * 32 + lane;
+            const float v = v_in[j];
+            const float4 J = GATHER ? Jn[j] : J_in[j];
+            const float isyn = use_override ? s.isyn_override[n] : isyn_of(p, v, J);
+            const float mainp = __fmul_rn(-p.gL, __fsub_rn(v, p.VL));
+            const float cd = __fadd_rn(__fadd_rn(mainp, isyn), p.Iext);
+            const float vn = __fadd_rn(v, __fmul_rn(p.rCdt, cd));
+            const bool notsat = t >= __fadd_rn(tl_in[j], p.Tref);
+            const float vs = notsat ? vn : p.Vreset;
+            bool a = vs >= p.Vth;
+            const float vmin = isnan(vs) ? vs : (isnan(p.Vth) ? p.Vth : (vs < p.Vth ? vs : p.Vth));
+            if (FORCED && s.forced_active) a = (__ldg(s.forced_active + (n >> 5)) >> (n & 31)) & 1u;
+            const float rate = noise_rate >= 0.0f ? noise_rate : p.noise;
+            const bool nz = u01(words[j]) < rate;
+            bool na = isolated ? nz : (nz || a);
+            if (FORCED && s.forced_new) na = (__ldg(s.forced_new + (n >> 5)) >> (n & 31)) & 1u;
+            __stcs(s.V + n, vmin);
+            __stcs(s.J + n, mul4(J, p.decay));
+            if (a) s.tlast[n] = t;
+            // synaptic events of this step: out-degree of every propagating neuron
+            if (na && s.qrow) ev_lane += (uint32_t)(__ldg(s.qrow + n + 1) - __ldg(s.qrow + n));
+            act_m |= (uint32_t)a << j;
+            nav_m |= (uint32_t)na << j;
+            if (j == 0) mysub0 = p.sub;
+            else if (p.sub != mysub0) lane_uni = false;
+            vsum_lane += (double)vmin;
+            if (p.sub < 0 || p.sub >= s.n_sub) {
+                lane_uni = false;
+                if (na) atomicAdd(s.unmapped_nact, 1u);
+            }
+        };
+        const uint32_t c0 = __shfl_sync(0xffffffffu, c_in[0], 0);
+        bool same = true;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (valid[j]) same = same && (c_in[j] == c0);
+        if (__all_sync(0xffffffffu, same)) {
+            const ParamClass p = load_class(s.pc, c0);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (valid[j]) neuron(j, p);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (valid[j]) neuron(j, load_class(s.pc, c_in[j]));
+        }
+        acc_ev += (unsigned long long)__reduce_add_sync(0xffffffffu, ev_lane);
+
+        uint32_t cnt_spk = 0, cnt_nact = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t ma = __ballot_sync(0xffffffffu, (act_m >> j) & 1u);
+            const uint32_t mn = __ballot_sync(0xffffffffu, (nav_m >> j) & 1u);
+            const int64_t wi = tile * 4 + j;
+            if (lane == 0) { s.abits[wi] = ma; obits[wi] = mn; }
+            cnt_spk += __popc(ma);
+            cnt_nact += __popc(mn);
+        }
+
+        // ---- per-subblock statistics
+        const int sub0 = __shfl_sync(0xffffffffu, mysub0, 0);
+        const bool uni = __all_sync(0xffffffffu, lane_uni && (mysub0 == sub0 || !valid[0])) && sub0 >= 0 &&
+                         sub0 < s.n_sub;
         if (uni) {
             double vs = vsum_lane;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) vs += __shfl_xor_sync(0xffffffffu, vs, o);
-            if (lane == 0) { sh_sub[wid] = sub0; sh_spk[wid] = cnt_spk; sh_nact[wid] = cnt_nact; sh_vsum[wid] = vs; }
+            if (sub0 != cur_sub) {
+                if (cur_sub >= 0 && lane == 0) {
+                    atomicAdd(s.sub_spk + cur_sub, acc_spk);
+                    atomicAdd(s.sub_nact + cur_sub, acc_nact);
+                    atomicAdd(s.sub_vsum + cur_sub, acc_v);
+                    flushed = true;
+                }
+                cur_sub = sub0; acc_spk = 0; acc_nact = 0; acc_v = 0.0;
+            }
+            acc_spk += cnt_spk; acc_nact += cnt_nact; acc_v += vs;
         } else {
+            // mixed subblocks in this tile: per-neuron atomics (classes re-read from L1)
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const int64_t n = base + j * 32 + lane;
-                if (n >= s.N) continue;
-                const int sb = mysub[j];
+                if (!valid[j]) continue;
+                const int sb = s.pc[c_in[j]].sub;
                 if (sb >= 0 && sb < s.n_sub) {
-                    if (act[j]) atomicAdd(s.sub_spk + sb, 1u);
-                    if (nav[j]) atomicAdd(s.sub_nact + sb, 1u);
-                    atomicAdd(s.sub_vsum + sb, (double)v_out[j]);
-                } else if (nav[j]) {
-                    atomicAdd(s.unmapped_nact, 1u);
+                    if ((act_m >> j) & 1u) atomicAdd(s.sub_spk + sb, 1u);
+                    if ((nav_m >> j) & 1u) atomicAdd(s.sub_nact + sb, 1u);
+                    atomicAdd(s.sub_vsum + sb, (double)__ldcg(s.V + base + j * 32 + lane));
                 }
             }
             __threadfence();   // this lane's atomics before the CTA's done-count
-            if (lane == 0) sh_sub[wid] = -1;
         }
-    } else if (lane == 0) {
-        sh_sub[wid] = -1;
     }
+    if (flushed) __threadfence();
+
+    // ---- CTA merge: one barrier, one set of atomics, one done-count per CTA
+    if (lane == 0) { sh_sub[wid] = cur_sub; sh_spk[wid] = acc_spk; sh_nact[wid] = acc_nact; sh_vsum[wid] = acc_v; sh_ev[wid] = acc_ev; }
     __syncthreads();
     if (threadIdx.x == 0) {
+        unsigned long long ev = 0;
         int cur = -1; uint32_t cs = 0, cn = 0; double cv = 0.0;
         for (int w = 0; w < kWarps; ++w) {
+            ev += sh_ev[w];
             const int sb = sh_sub[w];
-            if (sb < 0) continue;
+            if (!UPDATE || sb < 0) continue;
             if (sb != cur) {
                 if (cur >= 0) {
                     atomicAdd(s.sub_spk + cur, cs); atomicAdd(s.sub_nact + cur, cn); atomicAdd(s.sub_vsum + cur, cv);
@@ -375,10 +384,14 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
             cs += sh_spk[w]; cn += sh_nact[w]; cv += sh_vsum[w];
         }
         if (cur >= 0) { atomicAdd(s.sub_spk + cur, cs); atomicAdd(s.sub_nact + cur, cn); atomicAdd(s.sub_vsum + cur, cv); }
-        __threadfence();   // the CTA's statistics before its done-count
-        const unsigned prev = atomicAdd(&s.ctl->done, 1u);
-        sh_last = (prev == gridDim.x - 1u);
+        if (ev) atomicAdd(&s.ctl->events, ev);
+        if (UPDATE) {
+            __threadfence();   // the CTA's statistics before its done-count
+            const unsigned prev = atomicAdd(&s.ctl->done, 1u);
+            sh_last = (prev == gridDim.x - 1u);
+        }
     }
+    if (!UPDATE) return;
     __syncthreads();
     if (sh_last) {
         __threadfence();
@@ -393,26 +406,25 @@ __global__ void __launch_bounds__(kStepThreads) k_step(DevState s)
 // loads one row's bounds, a warp scan turns the row lengths into offsets, and
 // the lanes walk the concatenated synapses of the 32 rows together (four
 // independent index/weight loads in flight per lane), each synapse adding its
-// weight pair to the pending J with one float2 atomic.  Small `wpw` keeps the
-// rows scattered at any moment inside a narrow window of neurons, so the
-// destination J lines of intra-region synapses stay in L2.
+// weight pair to the pending J with one float2 atomic.  The synapse stream is
+// read with evict-first hints so it does not push the J lines out of L2; a
+// small `wpw` keeps the rows scattered at any moment inside a narrow window
+// of neurons, whose intra-region targets then share L2-resident J lines.  No
+// CTA-wide barrier: the events are counted by the update kernel.
 constexpr int kScatterThreads = 256;
 constexpr int kScatterMaxWords = 32;
 
 __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw)
 {
     __shared__ uint32_t sh_rows[kScatterThreads / 32][kScatterMaxWords * 32];
-    __shared__ unsigned long long sh_ev;
     const unsigned long long steps_done = s.ctl->steps_done;
     const uint32_t* __restrict__ bits = s.bits[(steps_done - 1ull) & 1ull];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t w0 = warp_global * wpw;
-    if (threadIdx.x == 0) sh_ev = 0ull;
-    __syncthreads();
     uint32_t* rows = sh_rows[wid];
-    uint32_t word = (lane < wpw && w0 + lane < s.n_words) ? __ldg(bits + w0 + lane) : 0u;
+    uint32_t word = (lane < wpw && w0 + lane < s.n_words) ? __ldcs(bits + w0 + lane) : 0u;
     // list the set bits of the window in neuron order
     const int cnt = __popc(word);
     int incl = cnt;
@@ -429,14 +441,13 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
         rows[pos++] = (uint32_t)((w0 + lane) * 32 + b);
     }
     __syncwarp();
-    unsigned long long events = 0;
     for (int r0 = 0; r0 < total; r0 += 32) {
         const bool has = r0 + lane < total;
         int64_t e0 = 0, len = 0;
         if (has) {
             const uint32_t pre = rows[r0 + lane];
-            e0 = __ldg(s.qrow + pre);
-            len = __ldg(s.qrow + pre + 1) - e0;
+            e0 = __ldcs(s.qrow + pre);
+            len = __ldcs(s.qrow + pre + 1) - e0;
         }
         // inclusive scan of the row lengths
         int64_t off = len;
@@ -446,7 +457,6 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
             if (lane >= o) off += y;
         }
         const int64_t T = __shfl_sync(0xffffffffu, off, 31);
-        events += (unsigned long long)T;
         const int64_t start = off - len;           // exclusive offset of this lane's row
         for (int64_t v0 = 0; v0 < T; v0 += 128) {
             uint32_t c[4];
@@ -468,8 +478,8 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
                 ok[u] = v < T;
                 if (ok[u]) {
                     const int64_t e = re0 + (v - rs);
-                    c[u] = __ldg(s.qcol + e);
-                    w[u] = __ldg(s.qw + e);
+                    c[u] = __ldcs(s.qcol + e);
+                    w[u] = __ldcs(s.qw + e);
                 }
             }
 #pragma unroll
@@ -481,9 +491,6 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
             }
         }
     }
-    if (lane == 0 && events) atomicAdd(&sh_ev, events);
-    __syncthreads();
-    if (threadIdx.x == 0 && sh_ev) atomicAdd(&s.ctl->events, sh_ev);
 }
 
 // ------------------------------------------------------------ exports

@@ -164,9 +164,10 @@ int dtb_step_preallocated(const dtb_prealloc_net* net, float t, uint64_t step, f
     k_prealloc_setup<<<setup_grid, setup_threads, 0, st>>>(s.ctl, s.sub_spk, s.sub_nact, s.sub_vsum,
                                                            s.unmapped_nact, net->n_subblocks,
                                                            (unsigned long long)step, t, noise_rate, isolated ? 1 : 0);
+    // one tile of 128 neurons per warp (the kernels also take longer runs of tiles)
     const unsigned grid = (unsigned)((N + kWarpNeurons * (kStepThreads / 32) - 1) / (kWarpNeurons * (kStepThreads / 32)));
-    k_step<false, true, false><<<grid, kStepThreads, 0, st>>>(s);   // update (models/block.py:133-142)
-    k_step<true, false, false><<<grid, kStepThreads, 0, st>>>(s);   // pull gather, bit-identical order
+    k_step<false, true, false><<<grid, kStepThreads, 0, st>>>(s, 1);   // update (models/block.py:133-142)
+    k_step<true, false, false><<<grid, kStepThreads, 0, st>>>(s, 1);   // pull gather, bit-identical order
     const cudaError_t e = cudaGetLastError();
     if (prev >= 0 && prev != net->device) cudaSetDevice(prev);
     if (e != cudaSuccess) return err(DTB_ERR_CUDA, "launch failed: %s", cudaGetErrorString(e));

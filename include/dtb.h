@@ -192,17 +192,20 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  * DTB_TUNE_PULL_THRESHOLD_PPM  activity fraction (parts per million of the
  *                          neurons propagating per step) above which
  *                          DTB_MODE_AUTO pulls instead of pushing
- * DTB_TUNE_USE_GRAPHS      capture chunks in CUDA graphs (0/1) */
-enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3 };
+ * DTB_TUNE_USE_GRAPHS      capture chunks in CUDA graphs (0/1)
+ * DTB_TUNE_STEP_VARIANT    register budget of the step kernels: 0 = two
+ *                          resident CTAs per SM (no spills), 1 = three */
+enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,
+       DTB_TUNE_STEP_VARIANT = 4 };
 int dtb_block_set_tuning(dtb_block* b, int key, int64_t value);
 int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value);
 
-/* Autotuner: times the push scatter at 1, 2, 4, ..., 32 bitmask words per
+/* Autotuner: times the step kernel's two register budgets, the push scatter at 1, 2, 4, ..., 32 bitmask words per
  * warp and the pull gather on the live network (n_steps each; the
  * simulation advances), keeps the fastest scatter shape and sets the
  * AUTO push/pull threshold from the measured costs at the current activity.
- * report (nullable, 5 floats): words per warp, push ms/step, pull ms/step,
- * activity fraction, threshold. */
+ * report (nullable, 6 floats): words per warp, push ms/step, pull ms/step,
+ * activity fraction, threshold, step variant. */
 int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* report);
 
 /* ---- state access ------------------------------------------------------- */
