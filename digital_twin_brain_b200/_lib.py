@@ -44,7 +44,9 @@ class SynthDesc(ctypes.Structure):
     _fields_ = [("n_regions", c_int), ("region_start", c_vp), ("region_n_exc", c_vp), ("cum", c_vp),
                 ("K", c_int), ("w_scale", c_f32), ("gen_seed", c_u64), ("class_property", c_vp),
                 ("class_decay", c_vp), ("dt", c_f32), ("seed", c_u64), ("stream_id", c_u32), ("device", c_int),
-                ("build_push", c_int)]
+                ("build_push", c_int), ("src_base", c_vp), ("src_count", c_vp), ("cum_off", c_vp), ("cum_flat", c_vp),
+                ("n_members", ctypes.c_int32), ("region_member", c_vp), ("member_start", c_vp),
+                ("member_seed", c_vp)]
 
 
 class BlockInfo(ctypes.Structure):

@@ -99,6 +99,7 @@ ParamClass make_class(const float* prop, const float* decay, float dt)
     const float s = prop[3];
     p.sub = (s >= 0.0f && s < 2147483647.0f && std::floor(s) == s) ? (int32_t)s : -1;
     p.C = prop[4];
+    p.member = -1;
     return p;
 }
 
@@ -279,7 +280,9 @@ static int alloc_state(dtb_block* b)
     s.N = N;
     s.n_words = ((N + 127) / 128) * 4;
     RET(dalloc(b, &s.V, (size_t)N));
-    RET(dalloc(b, &s.J, (size_t)N));
+    RET(dalloc(b, &s.J2, 2 * (size_t)N));
+    s.j_ps = N;   // split layout: excitatory pairs, then inhibitory pairs
+    s.j_es = 1;
     RET(dalloc(b, &s.tlast, (size_t)N));
     RET(dalloc(b, &s.isyn_override, (size_t)N));
     for (int p = 0; p < 2; ++p) RET(dalloc(b, &s.bits[p], (size_t)s.n_words));
@@ -287,7 +290,7 @@ static int alloc_state(dtb_block* b)
     RET(dalloc(b, &s.ctl, 1));
     RET(dalloc(b, &s.unmapped_nact, 1));
     RET(dalloc(b, &b->d_err, 4));
-    CK(cudaMemsetAsync(s.J, 0, sizeof(float4) * (size_t)N, b->stream));
+    CK(cudaMemsetAsync(s.J2, 0, sizeof(float2) * 2 * (size_t)N, b->stream));
     CK(cudaMemsetAsync(s.tlast, 0, sizeof(float) * (size_t)N, b->stream));
     for (int p = 0; p < 2; ++p) CK(cudaMemsetAsync(s.bits[p], 0, sizeof(uint32_t) * (size_t)s.n_words, b->stream));
     CK(cudaMemsetAsync(s.abits, 0, sizeof(uint32_t) * (size_t)s.n_words, b->stream));
@@ -696,7 +699,7 @@ int dtb_block_create_synthetic(const dtb_synth_desc* d, dtb_block** out)
     if (!d || !out) return fail(DTB_ERR_ARG, "null argument");
     *out = nullptr;
     const int R = d->n_regions;
-    if (R <= 0 || !d->region_start || !d->region_n_exc || !d->cum || !d->class_property)
+    if (R <= 0 || !d->region_start || !d->region_n_exc || !d->class_property || (!d->cum && !d->src_count))
         return fail(DTB_ERR_ARG, "bad synthetic description");
     if (d->K < 1 || d->K > 1024) return fail(DTB_ERR_LIMIT, "K must be in [1, 1024]");
     const int64_t N = d->region_start[R];
@@ -707,6 +710,40 @@ int dtb_block_create_synthetic(const dtb_synth_desc* d, dtb_block** out)
             return fail(DTB_ERR_ARG, "region_n_exc out of range");
     }
     const int64_t S = N * (int64_t)d->K;
+    // source-region tables: explicit (ensembles) or derived from cum[R][R]
+    std::vector<int32_t> src_base(R), src_count(R), region_member(R);
+    std::vector<int64_t> cum_off(R), member_start;
+    std::vector<uint64_t> member_seed;
+    std::vector<float> cum_flat;
+    const bool ens = d->src_count != nullptr;
+    if (ens) {
+        if (!d->src_base || !d->cum_off || !d->cum_flat || d->n_members <= 0 || !d->region_member ||
+            !d->member_start || !d->member_seed)
+            return fail(DTB_ERR_ARG, "ensemble tables incomplete");
+        int64_t flat = 0;
+        for (int r = 0; r < R; ++r) {
+            src_base[r] = d->src_base[r]; src_count[r] = d->src_count[r]; cum_off[r] = d->cum_off[r];
+            region_member[r] = d->region_member[r];
+            if (src_count[r] < 1 || src_base[r] < 0 || src_base[r] + src_count[r] > R || cum_off[r] < 0 ||
+                region_member[r] < 0 || region_member[r] >= d->n_members)
+                return fail(DTB_ERR_ARG, "region %d: bad source table or member", r);
+            flat = std::max<int64_t>(flat, cum_off[r] + src_count[r]);
+        }
+        cum_flat.assign(d->cum_flat, d->cum_flat + flat);
+        member_start.assign(d->member_start, d->member_start + d->n_members);
+        member_seed.assign(d->member_seed, d->member_seed + d->n_members);
+        for (int m = 0; m < d->n_members; ++m)
+            if (member_start[m] % kWarpNeurons != 0 || member_start[m] < 0 || member_start[m] > N)
+                return fail(DTB_ERR_ARG, "member %d must start on a multiple of %d neurons", m, kWarpNeurons);
+        for (int r = 0; r < R; ++r)
+            if (d->region_start[r] < member_start[region_member[r]])
+                return fail(DTB_ERR_ARG, "region %d starts before its member", r);
+    } else {
+        for (int r = 0; r < R; ++r) { src_base[r] = 0; src_count[r] = R; cum_off[r] = (int64_t)r * R; region_member[r] = 0; }
+        cum_flat.assign(d->cum, d->cum + (size_t)R * R);
+        member_start.assign(1, 0);
+        member_seed.assign(1, d->gen_seed);
+    }
     dtb_block* b = new dtb_block();
     DeviceGuard guard(d->device < 0 ? 0 : d->device);
     int rc = create_common(b, d->device, d->dt, d->seed, d->stream_id);
@@ -714,33 +751,44 @@ int dtb_block_create_synthetic(const dtb_synth_desc* d, dtb_block** out)
     if (rc == DTB_OK) {
         b->N = N;
         b->S = S;
-        // classes = subblocks 2r (excitatory) / 2r+1 (inhibitory)
+        // classes 2r (excitatory) / 2r+1 (inhibitory); subblock from property column 3
         const int nc = 2 * R;
         b->classes.clear(); b->class_prop.clear(); b->class_decay.clear();
+        int max_sub = -1;
         for (int c = 0; c < nc; ++c) {
             const float* pr = d->class_property + (size_t)c * DTB_NPROP;
             float dc[4];
             if (d->class_decay) std::memcpy(dc, d->class_decay + (size_t)c * 4, sizeof(dc));
             else default_decay(pr, b->dt, dc);
             ParamClass p = make_class(pr, dc, b->dt);
-            p.sub = c;
+            p.member = ens ? region_member[c / 2] : -1;
+            max_sub = std::max(max_sub, p.sub);
             b->classes.push_back(p);
-            std::array<float, 22> row; std::memcpy(row.data(), pr, sizeof(float) * 22); row[3] = (float)c;
+            std::array<float, 22> row; std::memcpy(row.data(), pr, sizeof(float) * 22);
             b->class_prop.push_back(row);
             b->class_decay.push_back({dc[0], dc[1], dc[2], dc[3]});
         }
         b->n_classes = nc;
-        b->n_sub = nc;
-        b->sub_count.assign((size_t)nc, 0u);
+        b->n_sub = max_sub + 1;
+        b->sub_count.assign((size_t)std::max(0, b->n_sub), 0u);
         cls.resize((size_t)N);
         for (int r = 0; r < R; ++r) {
             const int64_t s0 = d->region_start[r], s1 = d->region_start[r + 1], ne = d->region_n_exc[r];
             for (int64_t i = s0; i < s1; ++i) cls[(size_t)i] = (uint32_t)(2 * r + ((i - s0) >= ne ? 1 : 0));
-            b->sub_count[(size_t)(2 * r)] = (uint32_t)ne;
-            b->sub_count[(size_t)(2 * r + 1)] = (uint32_t)(s1 - s0 - ne);
+            const int se = b->classes[(size_t)(2 * r)].sub, si = b->classes[(size_t)(2 * r + 1)].sub;
+            if (se >= 0) b->sub_count[(size_t)se] += (uint32_t)ne;
+            if (si >= 0) b->sub_count[(size_t)si] += (uint32_t)(s1 - s0 - ne);
         }
         rc = alloc_state(b);
         if (rc == DTB_OK) rc = upload_classes(b, cls, true);
+        if (rc == DTB_OK && ens) {
+            int64_t* ms = nullptr;
+            rc = dalloc(b, &ms, member_start.size());
+            if (rc == DTB_OK) {
+                cudaMemcpy(ms, member_start.data(), sizeof(int64_t) * member_start.size(), cudaMemcpyHostToDevice);
+                b->ds.member_start = ms;
+            }
+        }
     }
     // generate the pull CSR on the device
     if (rc == DTB_OK) {
@@ -750,19 +798,39 @@ int dtb_block_create_synthetic(const dtb_synth_desc* d, dtb_block** out)
         if (rc == DTB_OK) rc = dalloc(b, &pcol, (size_t)S);
         if (rc == DTB_OK) rc = dalloc(b, &pw, (size_t)S);
         // temporaries (freed at the end of creation)
-        void *t_rs = nullptr, *t_ne = nullptr, *t_cum = nullptr, *t_out = nullptr;
+        void *t_rs = nullptr, *t_ne = nullptr, *t_cum = nullptr, *t_out = nullptr, *t_tab = nullptr;
+        const size_t tab_bytes = sizeof(int32_t) * 3 * R + sizeof(int64_t) * R + sizeof(int64_t) * member_start.size() +
+                                 sizeof(uint64_t) * member_seed.size() + 64;
         if (rc == DTB_OK) {
             cudaError_t e = cudaMalloc(&t_rs, sizeof(int64_t) * (R + 1));
             if (e == cudaSuccess) e = cudaMalloc(&t_ne, sizeof(int64_t) * R);
-            if (e == cudaSuccess) e = cudaMalloc(&t_cum, sizeof(float) * (size_t)R * R);
+            if (e == cudaSuccess) e = cudaMalloc(&t_cum, sizeof(float) * std::max<size_t>(1, cum_flat.size()));
             if (e == cudaSuccess) e = cudaMalloc(&t_out, sizeof(uint32_t) * (size_t)(N + 1));
+            if (e == cudaSuccess) e = cudaMalloc(&t_tab, tab_bytes);
             if (e != cudaSuccess) { cudaGetLastError(); rc = fail(DTB_ERR_NOMEM, "generator temporaries: %s", cudaGetErrorString(e)); }
             rs = (int64_t*)t_rs; ne = (int64_t*)t_ne; cum = (float*)t_cum; outdeg = (uint32_t*)t_out;
+        }
+        int64_t* d_cum_off = nullptr; int64_t* d_mstart = nullptr; uint64_t* d_mseed = nullptr;
+        int32_t* d_sbase = nullptr; int32_t* d_scount = nullptr; int32_t* d_rmem = nullptr;
+        if (rc == DTB_OK) {
+            char* tp = (char*)t_tab;
+            d_cum_off = (int64_t*)tp; tp += sizeof(int64_t) * R;
+            d_mstart = (int64_t*)tp; tp += sizeof(int64_t) * member_start.size();
+            d_mseed = (uint64_t*)tp; tp += sizeof(uint64_t) * member_seed.size();
+            d_sbase = (int32_t*)tp; tp += sizeof(int32_t) * R;
+            d_scount = (int32_t*)tp; tp += sizeof(int32_t) * R;
+            d_rmem = (int32_t*)tp;
+            cudaMemcpy(d_cum_off, cum_off.data(), sizeof(int64_t) * R, cudaMemcpyHostToDevice);
+            cudaMemcpy(d_mstart, member_start.data(), sizeof(int64_t) * member_start.size(), cudaMemcpyHostToDevice);
+            cudaMemcpy(d_mseed, member_seed.data(), sizeof(uint64_t) * member_seed.size(), cudaMemcpyHostToDevice);
+            cudaMemcpy(d_sbase, src_base.data(), sizeof(int32_t) * R, cudaMemcpyHostToDevice);
+            cudaMemcpy(d_scount, src_count.data(), sizeof(int32_t) * R, cudaMemcpyHostToDevice);
+            cudaMemcpy(d_rmem, region_member.data(), sizeof(int32_t) * R, cudaMemcpyHostToDevice);
         }
         if (rc == DTB_OK) {
             cudaMemcpy(rs, d->region_start, sizeof(int64_t) * (R + 1), cudaMemcpyHostToDevice);
             cudaMemcpy(ne, d->region_n_exc, sizeof(int64_t) * R, cudaMemcpyHostToDevice);
-            cudaMemcpy(cum, d->cum, sizeof(float) * (size_t)R * R, cudaMemcpyHostToDevice);
+            cudaMemcpy(cum, cum_flat.data(), sizeof(float) * cum_flat.size(), cudaMemcpyHostToDevice);
             cudaMemset(outdeg, 0, sizeof(uint32_t) * (size_t)(N + 1));
             cudaMemset(b->d_err, 0, 16);
             // rowptr = i*K
@@ -770,9 +838,11 @@ int dtb_block_create_synthetic(const dtb_synth_desc* d, dtb_block** out)
             for (int64_t i = 0; i <= N; ++i) hrow[(size_t)i] = i * d->K;
             cudaMemcpy(prow, hrow.data(), sizeof(int64_t) * hrow.size(), cudaMemcpyHostToDevice);
             GenArgs g;
-            g.N = N; g.R = R; g.region_start = rs; g.region_n_exc = ne; g.cum = cum; g.K = d->K;
+            g.N = N; g.R = R; g.region_start = rs; g.region_n_exc = ne; g.K = d->K;
+            g.src_base = d_sbase; g.src_count = d_scount; g.cum_off = d_cum_off; g.cum_flat = cum;
+            g.region_member = d_rmem; g.member_start = d_mstart; g.member_seed = d_mseed;
             int Kp = 1; while (Kp < d->K) Kp <<= 1;
-            g.Kp = Kp; g.w_scale = d->w_scale; g.seed = d->gen_seed; g.pcol = pcol; g.pw = pw;
+            g.Kp = Kp; g.w_scale = d->w_scale; g.pcol = pcol; g.pw = pw;
             g.outdeg = d->build_push ? outdeg : nullptr; g.err = b->d_err;
             const size_t smem = sizeof(unsigned long long) * (size_t)Kp * kGenWarps;
             cudaFuncSetAttribute(k_gen_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -828,7 +898,7 @@ int dtb_block_create_synthetic(const dtb_synth_desc* d, dtb_block** out)
             b->ds.qrow = qrow; b->ds.qcol = qcol; b->ds.qw = qw;
             b->has_push = (rc == DTB_OK);
         }
-        cudaFree(t_rs); cudaFree(t_ne); cudaFree(t_cum); cudaFree(t_out);
+        cudaFree(t_rs); cudaFree(t_ne); cudaFree(t_cum); cudaFree(t_out); cudaFree(t_tab);
     }
     if (rc == DTB_OK) rc = finish_create(b);
     if (rc != DTB_OK) { destroy_block(b); return rc; }
@@ -1349,7 +1419,8 @@ int dtb_block_update_conn_weight(dtb_block* b, int64_t n, const uint8_t* channel
 }
 
 // Checkpoint format: "DTBCKPT1", N (i64), steps (u64), t (f32), override flag (u32),
-// then V[N], J[N] float4, t_last[N], and I_syn override[N] if the flag is set.
+// then V[N], J as stored (excitatory pairs [N] float2, then inhibitory pairs),
+// t_last[N], and I_syn override[N] if the flag is set.
 int dtb_block_save(dtb_block* b, const char* path)
 {
     if (!b || !path) return fail(DTB_ERR_ARG, "null argument");
@@ -1360,7 +1431,7 @@ int dtb_block_save(dtb_block* b, const char* path)
     float t = 0.0f;
     CK(cudaStreamSynchronize(b->stream));
     CK(cudaMemcpy(V.data(), b->ds.V, 4 * N, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(J.data(), b->ds.J, 16 * N, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(J.data(), b->ds.J2, 16 * N, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(T.data(), b->ds.tlast, 4 * N, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&t, &b->ds.ctl->t, 4, cudaMemcpyDeviceToHost));
     const uint32_t ov = b->override_pending ? 1u : 0u;
@@ -1403,7 +1474,7 @@ int dtb_block_load(dtb_block* b, const char* path)
     if (!ok) return fail(DTB_ERR_FORMAT, "truncated checkpoint %s", path);
     CK(cudaStreamSynchronize(b->stream));
     CK(cudaMemcpy(b->ds.V, V.data(), 4 * N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->ds.J, J.data(), 16 * N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->ds.J2, J.data(), 16 * N, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b->ds.tlast, T.data(), 4 * N, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(&b->ds.ctl->t, &t, 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(&b->ds.ctl->steps_done, &steps, 8, cudaMemcpyHostToDevice));

@@ -1,7 +1,9 @@
 // Device-side data structures and helpers shared by the kernels of libdtb.
 //
 // Layout in HBM (one network = one handle):
-//   V[N] f32, J[N] float4 {AMPA, NMDA, GABAa, GABAb}, t_last[N] f32,
+//   V[N] f32, J as two float2 planes (AMPA/NMDA pairs, then GABAa/GABAb pairs:
+//   one 32-byte sector holds four neurons' pair, which the push atomics hit),
+//   t_last[N] f32,
 //   cls[N] u32 -> ParamClass table (deduplicated property rows),
 //   spike bitmasks: new_active (double buffered by step parity) and active,
 //   ceil(N/128)*4 words each (one warp owns 128 neurons = 4 words),
@@ -35,7 +37,8 @@ struct __align__(16) ParamClass {
     float noise;    // col 0 (per-neuron noise rate, cuda/src/stage/spike.cpp:157)
     int32_t sub;    // col 3 (subblock index)
     float C;        // col 4
-    float pad0, pad1;
+    int32_t member; // ensemble member (noise stream offset), -1 outside ensembles
+    float pad1;
 };
 static_assert(sizeof(ParamClass) == 96, "ParamClass layout");
 
@@ -76,11 +79,14 @@ struct DevState {
     int64_t N;
     int64_t n_words;            // bitmask words (multiple of 4)
     float* V;
-    float4* J;
+    float2* J2;                 // receptor pairs: pair p of neuron n at J2[p * j_ps + n * j_es]
+    int64_t j_ps;               // plane stride (float2 units): N for the split layout, 1 for [N][4]
+    int64_t j_es;               // neuron stride (float2 units): 1 for the split layout, 2 for [N][4]
     float* tlast;
     float* isyn_override;       // [N] used once after update_property
     const uint32_t* cls;
     const ParamClass* pc;
+    const int64_t* member_start;  // [M] first neuron of every ensemble member (nullable)
     uint32_t* bits[2];          // new_active bitmask by step parity
     uint32_t* abits;            // active bitmask of the latest update
     const uint32_t* forced_active;   // teacher forcing bitmasks (nullable)

@@ -61,6 +61,20 @@ __device__ __forceinline__ float4 mul4(float4 a, float4 b)
     return make_float4(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y), __fmul_rn(a.z, b.z), __fmul_rn(a.w, b.w));
 }
 
+// J of neuron n as {AMPA, NMDA, GABAa, GABAb} (streaming access: once per step).
+__device__ __forceinline__ float4 load_J(const DevState& s, int64_t n)
+{
+    const float2 a = __ldcs(s.J2 + n * s.j_es);
+    const float2 b = __ldcs(s.J2 + s.j_ps + n * s.j_es);
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ void store_J(const DevState& s, int64_t n, float4 J)
+{
+    __stcs(s.J2 + n * s.j_es, make_float2(J.x, J.y));
+    __stcs(s.J2 + s.j_ps + n * s.j_es, make_float2(J.z, J.w));
+}
+
 __device__ __forceinline__ bool test_bit(const uint32_t* __restrict__ bits, int64_t n)
 {
     return (__ldg(bits + (n >> 5)) >> (n & 31)) & 1u;
@@ -133,7 +147,7 @@ __device__ void step_epilogue(const DevState& s, unsigned long long steps_done, 
     if (s.bold.n_regions > 0) {
         const BoldDev& b = s.bold;
         for (int r = threadIdx.x; r < b.n_regions; r += blockDim.x) {
-            const double act = b.act[r] / b.region_n[r];
+            const double act = b.region_n[r] > 0.0 ? b.act[r] / b.region_n[r] : 0.0;
             b.act[r] = act;
             const double u = act > 1e-5 ? act : 1e-5;
             double fi = b.f[r], si = b.s[r], qi = b.q[r], vi = b.v[r];
@@ -224,24 +238,19 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int64_t n = base + j * 32 + lane;
-                if (n < s.N) Jn[j] = add4(__ldcs(s.J + n), sum[j]);   // models/block.py:71-73
+                if (n < s.N) Jn[j] = add4(load_J(s, n), sum[j]);   // models/block.py:71-73
             }
             if (!UPDATE) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int64_t n = base + j * 32 + lane;
-                    if (n < s.N) __stcs(s.J + n, Jn[j]);
+                    if (n < s.N) store_J(s, n, Jn[j]);
                 }
                 continue;
             }
         }
 
         // ---- update of step `steps_done`
-        const U4 rnd = philox4x32_10(U4{(uint32_t)(tile * 32 + lane), s.stream_id, (uint32_t)steps_done,
-                                        (uint32_t)(steps_done >> 32)},
-                                     (uint32_t)s.seed, (uint32_t)(s.seed >> 32));
-        const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
-
         // Phase 1: every load of the lane's four neurons before any store, so their
         // latencies overlap (the stores below could alias them).  Streaming hints:
         // the state is touched once per step.
@@ -258,9 +267,27 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 v_in[j] = __ldcs(s.V + n);
                 tl_in[j] = __ldcs(s.tlast + n);
                 c_in[j] = __ldcs(s.cls + n);
-                if (!GATHER) J_in[j] = __ldcs(s.J + n);
+                if (!GATHER) J_in[j] = load_J(s, n);
             }
         }
+        // Noise words: counter {tile*32 + lane, stream, step}; inside an ensemble the
+        // tile and stream are the member's own (members start on 128-neuron tiles),
+        // so a member draws the same noise as when it is simulated alone.
+        const uint32_t c0 = __shfl_sync(0xffffffffu, c_in[0], 0);
+        uint64_t qtile = (uint64_t)tile;
+        uint32_t stream = s.stream_id;
+        if (s.member_start) {
+            const int m = __ldg(&s.pc[c0].member);
+            if (m >= 0) {
+                qtile = (uint64_t)((base - __ldg(s.member_start + m)) / kWarpNeurons);
+                stream += (uint32_t)m;
+            }
+        }
+        const U4 rnd = philox4x32_10(U4{(uint32_t)(qtile * 32 + lane), stream, (uint32_t)steps_done,
+                                        (uint32_t)(steps_done >> 32)},
+                                     (uint32_t)s.seed, (uint32_t)(s.seed >> 32));
+        const uint32_t words[4] = {rnd.x, rnd.y, rnd.z, rnd.w};
+
         // Phase 2: arithmetic (models/block.py:83-111 order), each neuron stored as
         // soon as it is computed (all loads were issued above).  When the tile's 128
         // neurons share one parameter class (classes are region x E/I ranges), the
@@ -288,7 +315,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             bool na = isolated ? nz : (nz || a);
             if (FORCED && s.forced_new) na = (__ldg(s.forced_new + (n >> 5)) >> (n & 31)) & 1u;
             __stcs(s.V + n, vmin);
-            __stcs(s.J + n, mul4(J, p.decay));
+            store_J(s, n, mul4(J, p.decay));
             if (a) s.tlast[n] = t;
             // synaptic events of this step: out-degree of every propagating neuron
             if (na && s.qrow) ev_lane += (uint32_t)(__ldg(s.qrow + n + 1) - __ldg(s.qrow + n));
@@ -302,7 +329,6 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 if (na) atomicAdd(s.unmapped_nact, 1u);
             }
         };
-        const uint32_t c0 = __shfl_sync(0xffffffffu, c_in[0], 0);
         bool same = true;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -485,7 +511,7 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 if (ok[u]) {
-                    float2* dst = reinterpret_cast<float2*>(s.J + (c[u] & kIndexMask)) + (c[u] >> 31);
+                    float2* dst = s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + (int64_t)(c[u] & kIndexMask) * s.j_es;
                     atomicAdd(dst, w[u]);
                 }
             }
@@ -499,7 +525,7 @@ __global__ void k_export_J(const DevState s, float* __restrict__ out)
 {
     const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= s.N) return;
-    const float4 J = s.J[n];
+    const float4 J = load_J(s, n);
     out[n] = J.x; out[s.N + n] = J.y; out[2 * s.N + n] = J.z; out[3 * s.N + n] = J.w;
 }
 
@@ -510,7 +536,7 @@ __global__ void k_export_current(const DevState s, float* __restrict__ iui, floa
     if (n >= s.N) return;
     const ParamClass p = load_class(s.pc, s.cls[n]);
     const float v = s.V[n];
-    const float4 J = s.J[n];
+    const float4 J = load_J(s, n);
     if (iui) {
         const float4 i = iui_of(p, v, J);
         iui[n] = i.x; iui[s.N + n] = i.y; iui[2 * s.N + n] = i.z; iui[3 * s.N + n] = i.w;
@@ -541,7 +567,7 @@ __global__ void k_J_from_planar(DevState s, const float* __restrict__ in)
 {
     const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= s.N) return;
-    s.J[n] = make_float4(in[n], in[s.N + n], in[2 * s.N + n], in[3 * s.N + n]);
+    store_J(s, n, make_float4(in[n], in[s.N + n], in[2 * s.N + n], in[3 * s.N + n]));
 }
 
 // ------------------------------------------------------------ weights
@@ -644,10 +670,15 @@ struct GenArgs {
     int R;
     const int64_t* region_start;  // [R+1]
     const int64_t* region_n_exc;  // [R]
-    const float* cum;             // [R][R]
+    const int32_t* src_base;      // [R] first candidate source region of a row of region r
+    const int32_t* src_count;     // [R] number of candidate source regions
+    const int64_t* cum_off;       // [R] offset of region r's cumulative row in cum_flat
+    const float* cum_flat;
+    const int32_t* region_member; // [R]
+    const int64_t* member_start;  // [M] first neuron of every member
+    const uint64_t* member_seed;  // [M] generator key of every member
     int K, Kp;                    // in-degree, next power of two
     float w_scale;
-    uint64_t seed;
     uint32_t* pcol;               // [N*K]
     float2* pw;                   // [N*K]
     uint32_t* outdeg;             // [N] (nullable) out-degree counts
@@ -677,15 +708,19 @@ __global__ void __launch_bounds__(kGenWarps * 32) k_gen_rows(GenArgs g)
     if (i >= g.N) return;
     unsigned long long* chosen = gsm + (size_t)wid * g.Kp;
     const int ri = region_of(g.region_start, g.R, i);
-    const float* crow = g.cum + (size_t)ri * g.R;
-    const uint32_t k0 = (uint32_t)g.seed, k1 = (uint32_t)(g.seed >> 32);
+    const float* crow = g.cum_flat + __ldg(g.cum_off + ri);
+    const int cnt_src = __ldg(g.src_count + ri), base_src = __ldg(g.src_base + ri);
+    const int mem = __ldg(g.region_member + ri);
+    const uint64_t li = (uint64_t)(i - __ldg(g.member_start + mem));   // member-local row index
+    const uint64_t key = __ldg(g.member_seed + mem);
+    const uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
     int have = 0;
     uint32_t attempt = 0;
     const uint32_t limit = (uint32_t)(64 * g.K + 1024);
     bool failed = false;
     while (have < g.K) {
         if (attempt > limit) { failed = true; break; }
-        const U4 o = philox4x32_10(U4{(uint32_t)i, kTagSrc, attempt, (uint32_t)((uint64_t)i >> 32)}, k0, k1);
+        const U4 o = philox4x32_10(U4{(uint32_t)li, kTagSrc, attempt, (uint32_t)(li >> 32)}, k0, k1);
         ++attempt;
         const uint32_t ws[4] = {o.x, o.y, o.z, o.w};
 #pragma unroll
@@ -693,8 +728,8 @@ __global__ void __launch_bounds__(kGenWarps * 32) k_gen_rows(GenArgs g)
             if (have >= g.K) break;
             const float ur = u01(ws[2 * h]);
             int cntr = 0;
-            for (int j = lane; j < g.R - 1; j += 32) cntr += (__ldg(crow + j) <= ur) ? 1 : 0;
-            const int r = __reduce_add_sync(0xffffffffu, cntr);
+            for (int j = lane; j < cnt_src - 1; j += 32) cntr += (__ldg(crow + j) <= ur) ? 1 : 0;
+            const int r = base_src + __reduce_add_sync(0xffffffffu, cntr);
             const int64_t rs0 = __ldg(g.region_start + r);
             const int64_t size = __ldg(g.region_start + r + 1) - rs0;
             if (size <= 0) continue;
@@ -736,7 +771,7 @@ __global__ void __launch_bounds__(kGenWarps * 32) k_gen_rows(GenArgs g)
         const unsigned long long e = chosen[j];
         const uint32_t src = (uint32_t)(e >> 1);
         g.pcol[rowbase + j] = src | ((e & 1ull) ? kKindBit : 0u);
-        const U4 o = philox4x32_10(U4{(uint32_t)i, kTagW, (uint32_t)(j >> 1), (uint32_t)((uint64_t)i >> 32)}, k0, k1);
+        const U4 o = philox4x32_10(U4{(uint32_t)li, kTagW, (uint32_t)(j >> 1), (uint32_t)(li >> 32)}, k0, k1);
         const uint32_t a = (j & 1) ? o.z : o.x;
         const uint32_t b = (j & 1) ? o.w : o.y;
         g.pw[rowbase + j] = make_float2(u01(a) * g.w_scale, u01(b) * g.w_scale);

@@ -131,7 +131,9 @@ int dtb_step_preallocated(const dtb_prealloc_net* net, float t, uint64_t step, f
     s.N = N;
     s.n_words = ((N + 127) / 128) * 4;
     s.V = net->V;
-    s.J = reinterpret_cast<float4*>(net->J);
+    s.J2 = reinterpret_cast<float2*>(net->J);   // caller layout [N][4]: pairs interleaved per neuron
+    s.j_ps = 1;
+    s.j_es = 2;
     s.tlast = net->t_last;
     s.isyn_override = nullptr;
     s.cls = net->cls;

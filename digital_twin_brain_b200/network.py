@@ -77,6 +77,20 @@ class Network:
                            w_scale=float(spec.w_scale), gen_seed=int(spec.gen_seed), class_property=_ptr(cp),
                            class_decay=_ptr(cd), dt=float(spec.dt), seed=int(spec.seed),
                            stream_id=int(spec.stream_id), device=int(device), build_push=int(bool(build_push)))
+        keep = []
+        if spec.members is not None:
+            t = spec.members
+            arrs = dict(src_base=np.ascontiguousarray(t["src_base"], np.int32),
+                        src_count=np.ascontiguousarray(t["src_count"], np.int32),
+                        cum_off=np.ascontiguousarray(t["cum_off"], np.int64),
+                        cum_flat=np.ascontiguousarray(t["cum_flat"], np.float32),
+                        region_member=np.ascontiguousarray(t["region_member"], np.int32),
+                        member_start=np.ascontiguousarray(t["member_start"], np.int64),
+                        member_seed=np.ascontiguousarray(t["member_seed"], np.uint64))
+            keep.append(arrs)
+            for k, v in arrs.items():
+                setattr(d, k, _ptr(v))
+            d.n_members = len(arrs["member_start"])
         h = ctypes.c_void_p()
         _lib.call("dtb_block_create_synthetic", ctypes.byref(d), ctypes.byref(h))
         return cls(h, device, spec.dt)

@@ -62,6 +62,7 @@ class NetworkSpec:
     dt: float = 0.1
     seed: int = 0                     # Philox noise key
     stream_id: int = 0
+    members: dict | None = None       # ensemble tables (see ensemble()); None for one network
     extra: dict = field(default_factory=dict)
 
     @property
@@ -77,8 +78,11 @@ class NetworkSpec:
         return self.N * self.K
 
     def as_dict(self) -> dict:
-        return dict(region_start=self.region_start, region_n_exc=self.region_n_exc, cum=self.cum, K=self.K,
-                    gen_seed=self.gen_seed, w_scale=self.w_scale)
+        d = dict(region_start=self.region_start, region_n_exc=self.region_n_exc, cum=self.cum, K=self.K,
+                 gen_seed=self.gen_seed, w_scale=self.w_scale)
+        if self.members is not None:
+            d.update(self.members)
+        return d
 
     def neuron_class(self) -> np.ndarray:
         """Class (= subblock) of every neuron: 2r excitatory, 2r+1 inhibitory."""
@@ -91,13 +95,11 @@ class NetworkSpec:
 
     def property(self) -> np.ndarray:
         """Per-neuron [N,22] property matrix (subblock index in column 3)."""
-        cls = self.neuron_class()
-        prop = self.class_property[cls].copy()
-        prop[:, 3] = cls.astype(np.float32)
-        return prop
+        return self.class_property[self.neuron_class()].copy()
 
     def sub_to_region(self) -> np.ndarray:
-        return (np.arange(2 * self.R) // 2).astype(np.int32)
+        n_sub = int(self.class_property[:, 3].max()) + 1
+        return (np.arange(n_sub) // 2).astype(np.int32)
 
 
 def _classes(R: int, **lif) -> np.ndarray:
@@ -137,6 +139,78 @@ def whole_brain(R: int = 90, mean_size: float = 2.2e5, sigma: float = 0.5, K: in
     return NetworkSpec(name=name or f"whole_brain_R{R}", region_start=start,
                        region_n_exc=np.round(exc_frac * sizes).astype(np.int64), cum=cum.astype(np.float32), K=K,
                        class_property=_classes(R, **params), gen_seed=gen_seed, seed=seed, dt=dt)
+
+
+def ensemble(templates: list, g_scale=None, stream_id: int = 0, name: str = "ensemble") -> NetworkSpec:
+    """Members concatenated in one network (the data-assimilation ensemble layout of
+    data_assimilation/DataAssimilation.py:97, members side by side in one block).
+
+    Member m keeps its own regions, connectivity (synapses never cross members),
+    generator seed (templates[m].gen_seed) and noise stream (stream_id + m); its
+    g_ui of region r is scaled by g_scale[m][r] (4 receptor factors, or one per member).
+    Every member starts on a 128-neuron tile: a pad region of up to 127 silent
+    neurons (V_th = +inf, no noise, subblock -1) closes each member.  Subblocks are
+    2 * (global region) + {0: excitatory, 1: inhibitory}.
+    """
+    rs, ne, sb, sc, co, cf, rm, mst, mseed, cls_rows = [0], [], [], [], [], [], [], [], [], []
+    pos = 0
+    rbase = 0
+    for m, t in enumerate(templates):
+        mst.append(pos)
+        mseed.append(int(t.gen_seed))
+        Rm = t.R
+        first_off = len(cf)
+        for r in range(Rm):
+            rs.append(pos + int(t.region_start[r + 1]))
+            ne.append(int(t.region_n_exc[r]))
+            sb.append(rbase)
+            sc.append(Rm)
+            co.append(len(cf))
+            cf.extend(np.asarray(t.cum[r], np.float32).tolist())
+            rm.append(m)
+            f = np.ones(4, np.float32)
+            if g_scale is not None:
+                gs = np.asarray(g_scale[m], np.float32)
+                f = gs[r] if gs.ndim == 2 else gs
+            for k in (0, 1):
+                row = t.class_property[2 * r + k].copy()
+                row[10:14] = row[10:14] * f
+                row[3] = 2 * (rbase + r) + k
+                cls_rows.append(row)
+        pos += t.N
+        pad = (-pos) % 128
+        rs.append(pos + pad)
+        ne.append(pad)
+        sb.append(rbase)
+        sc.append(Rm)
+        co.append(first_off)
+        rm.append(m)
+        for k in (0, 1):
+            row = t.class_property[0].copy()
+            row[0] = 0.0            # no noise
+            row[8] = np.inf         # never reaches threshold
+            row[3] = -1.0           # not counted
+            cls_rows.append(row)
+        pos += pad
+        rbase += Rm + 1
+    members = dict(src_base=np.array(sb, np.int32), src_count=np.array(sc, np.int32),
+                   cum_off=np.array(co, np.int64), cum_flat=np.array(cf, np.float32),
+                   region_member=np.array(rm, np.int32), member_start=np.array(mst, np.int64),
+                   member_seed=np.array(mseed, np.uint64))
+    K = templates[0].K
+    assert all(t.K == K for t in templates), "members share one in-degree"
+    dt = templates[0].dt
+    R = len(rs) - 1
+    return NetworkSpec(name=name, region_start=np.array(rs, np.int64), region_n_exc=np.array(ne, np.int64),
+                       cum=np.ones((1, 1), np.float32), K=K, class_property=np.stack(cls_rows).astype(np.float32),
+                       gen_seed=int(templates[0].gen_seed), w_scale=templates[0].w_scale, dt=dt,
+                       seed=templates[0].seed, stream_id=stream_id, members=members,
+                       extra=dict(member_regions=[t.R for t in templates], member_sizes=[t.N for t in templates]))
+
+
+def member_region_index(spec: NetworkSpec, m: int, r: int) -> int:
+    """Global region index of region r of member m in an ensemble spec."""
+    return int(np.nonzero(spec.members["region_member"] == m)[0][0]) + r
 
 
 # Benchmark configurations (sizes and parameters of the reference's workloads).

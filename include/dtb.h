@@ -92,9 +92,9 @@ typedef struct {
  * neuron ranges [region_start[r], region_start[r+1]); the first
  * region_n_exc[r] are excitatory.  Each neuron draws K distinct presynaptic
  * neurons (never itself): source region from the cumulative row cum[r][*],
- * then a uniform neuron inside it.  Subblock of a neuron = 2r (excitatory) or
- * 2r+1 (inhibitory), parameter class = its subblock, class parameters from
- * class_property[2R][22]. */
+ * then a uniform neuron inside it.  Parameter class of a neuron = 2r
+ * (excitatory) or 2r+1 (inhibitory), class parameters from
+ * class_property[2R][22] (its column 3 is the subblock). */
 typedef struct {
     int n_regions;
     const int64_t* region_start;   /* [R+1] host */
@@ -110,6 +110,23 @@ typedef struct {
     uint32_t stream_id;
     int device;
     int build_push;
+    /* Ensembles of members (optional: all NULL / 0 for one network).  A row of
+     * region r draws its source region among src_base[r] .. src_base[r] +
+     * src_count[r] - 1 through the cumulative row cum_flat[cum_off[r] ..]
+     * (then `cum` is unused).  Region r belongs to member region_member[r];
+     * member m's neurons start at member_start[m] (a multiple of 128); its rows
+     * are drawn with key member_seed[m] and member-local row indices, and its
+     * noise with stream stream_id + m and member-local counters, so every
+     * member equals the same network generated and simulated alone.  The
+     * subblock of class c is class_property[c][3] (-1: not counted). */
+    const int32_t* src_base;
+    const int32_t* src_count;
+    const int64_t* cum_off;
+    const float* cum_flat;
+    int32_t n_members;
+    const int32_t* region_member;
+    const int64_t* member_start;
+    const uint64_t* member_seed;
 } dtb_synth_desc;
 
 typedef struct {

@@ -252,13 +252,14 @@ void oracle_bold_step_f64(int64_t R, const double* u, double* s, double* q, doub
  * Regions r = 0..R-1 own neuron ranges [region_start[r], region_start[r+1]);
  * the first region_n_exc[r] neurons of a region are excitatory.
  * Every postsynaptic neuron i (region ri) draws K distinct presynaptic
- * neurons, never itself: a source region by the cumulative row
- * cum[ri][0..R-1] (region = number of cum[ri][j] <= u for j < R-1, as
+ * neurons, never itself: a source region by its cumulative row (region =
+ * number of cum entries <= u among all but the last, as
  * numpy.searchsorted(cum[:-1], u, 'right') in generation/make_block.py:290),
  * then a neuron uniformly inside it.  Candidates come two per Philox call:
- * counter {i_lo, TAG_SRC, attempt, i_hi}, words (0,1) and (2,3).  The row is
+ * counter {l_lo, TAG_SRC, attempt, l_hi} (l = row index within its member),
+ * words (0,1) and (2,3).  The row is
  * then sorted by presynaptic index; entry j gets the weight pair from counter
- * {i_lo, TAG_W, j/2, i_hi} (words 0,1 for even j, 2,3 for odd j), each
+ * {l_lo, TAG_W, j/2, l_hi} (words 0,1 for even j, 2,3 for odd j), each
  * U[0,1) * w_scale, and kind 0 (source excitatory -> AMPA/NMDA) or 2
  * (source inhibitory -> GABAa/GABAb), as generation/make_block.py:290-291.
  */
@@ -281,31 +282,41 @@ static int region_of(int64_t n, int R, const int64_t* region_start)
     return lo;
 }
 
-/* rows [row_begin, row_end): writes K entries per row into pre/kind/w (row-local offsets). */
-int oracle_gen_rows(uint64_t gseed, int R, const int64_t* region_start, const int64_t* region_n_exc,
-                    const float* cum /*[R][R]*/, int K, float w_scale,
-                    int64_t row_begin, int64_t row_end,
+/* rows [row_begin, row_end): writes K entries per row into pre/kind/w (row-local offsets).
+ * General form: a row of region r draws its source region from the cumulative
+ * row cum_flat[cum_off[r] .. + src_count[r]) as region src_base[r] + #{k <
+ * src_count[r]-1 : cum <= u}; rows of member m = region_member[r] use the
+ * member-local index l = i - member_start[m] in the Philox counters and the
+ * key member_seed[m], so a member generated inside an ensemble equals the
+ * same member generated alone. */
+int oracle_gen_rows(int R, const int64_t* region_start, const int64_t* region_n_exc,
+                    const int32_t* src_base, const int32_t* src_count, const int64_t* cum_off, const float* cum_flat,
+                    const int32_t* region_member, const int64_t* member_start, const uint64_t* member_seed,
+                    int K, float w_scale, int64_t row_begin, int64_t row_end,
                     uint32_t* pre, uint8_t* kind, float* w)
 {
-    uint32_t key[2] = {(uint32_t)gseed, (uint32_t)(gseed >> 32)};
     int bad = 0;
     #pragma omp parallel for schedule(dynamic, 64) reduction(+:bad)
     for (int64_t i = row_begin; i < row_end; ++i) {
         uint64_t* chosen = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)K);
         int ri = region_of(i, R, region_start);
-        const float* c = cum + (size_t)ri * R;
+        const float* c = cum_flat + cum_off[ri];
+        const int cnt = src_count[ri], sbase = src_base[ri];
+        const int m = region_member[ri];
+        const uint64_t l = (uint64_t)(i - member_start[m]);
+        uint32_t key[2] = {(uint32_t)member_seed[m], (uint32_t)(member_seed[m] >> 32)};
         int have = 0;
         uint32_t attempt = 0;
         while (have < K) {
             if (attempt > (uint32_t)(64 * K + 1024)) { bad += 1; break; }
-            uint32_t ctr[4] = {(uint32_t)i, TAG_SRC, attempt, (uint32_t)((uint64_t)i >> 32)};
+            uint32_t ctr[4] = {(uint32_t)l, TAG_SRC, attempt, (uint32_t)(l >> 32)};
             uint32_t o[4];
             oracle_philox4x32_10(ctr, key, o);
             attempt++;
             for (int h = 0; h < 2 && have < K; ++h) {
                 float ur = u01_from_bits(o[2 * h]);
-                int r = 0;
-                for (int j = 0; j < R - 1; ++j) r += (c[j] <= ur);
+                int r = sbase;
+                for (int j = 0; j < cnt - 1; ++j) r += (c[j] <= ur);
                 int64_t size = region_start[r + 1] - region_start[r];
                 if (size <= 0) continue;
                 uint64_t off = ((uint64_t)o[2 * h + 1] * (uint64_t)size) >> 32;
@@ -325,7 +336,7 @@ int oracle_gen_rows(uint64_t gseed, int R, const int64_t* region_start, const in
             int rs = region_of(src, R, region_start);
             pre[base + j] = (uint32_t)src;
             kind[base + j] = (src - region_start[rs] >= region_n_exc[rs]) ? 2 : 0;
-            uint32_t ctr[4] = {(uint32_t)i, TAG_W, (uint32_t)(j >> 1), (uint32_t)((uint64_t)i >> 32)};
+            uint32_t ctr[4] = {(uint32_t)l, TAG_W, (uint32_t)(j >> 1), (uint32_t)(l >> 32)};
             uint32_t o[4];
             oracle_philox4x32_10(ctr, key, o);
             int h = j & 1;

@@ -59,7 +59,7 @@ def lib():
         L.oracle_block_step.restype = ctypes.c_int
         L.oracle_bold_step_f32.argtypes = [i64] + [vp] * 6 + [f64] * 8
         L.oracle_bold_step_f64.argtypes = [i64] + [vp] * 6 + [f64] * 8
-        L.oracle_gen_rows.argtypes = [u64, ctypes.c_int, vp, vp, vp, ctypes.c_int, f32, i64, i64, vp, vp, vp]
+        L.oracle_gen_rows.argtypes = [ctypes.c_int] + [vp] * 9 + [ctypes.c_int, f32, i64, i64, vp, vp, vp]
         L.oracle_gen_rows.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -159,6 +159,25 @@ def subblock_stats(V: np.ndarray, active: np.ndarray, sub_idx: np.ndarray):
 
 # -------------------------------------------------------------- generator
 
+def general_tables(spec: dict):
+    """Source-region tables of a network spec (single network: every region draws from all R
+    regions through its row of cum[R][R]; ensembles pass the tables explicitly)."""
+    rs = np.ascontiguousarray(spec["region_start"], dtype=np.int64)
+    R = len(rs) - 1
+    if spec.get("src_count") is not None:
+        t = dict(src_base=spec["src_base"], src_count=spec["src_count"], cum_off=spec["cum_off"],
+                 cum_flat=spec["cum_flat"], region_member=spec["region_member"],
+                 member_start=spec["member_start"], member_seed=spec["member_seed"])
+    else:
+        t = dict(src_base=np.zeros(R, np.int32), src_count=np.full(R, R, np.int32),
+                 cum_off=np.arange(R, dtype=np.int64) * R, cum_flat=np.asarray(spec["cum"], np.float32).reshape(-1),
+                 region_member=np.zeros(R, np.int32), member_start=np.zeros(1, np.int64),
+                 member_seed=np.array([int(spec["gen_seed"])], np.uint64))
+    dt = dict(src_base=np.int32, src_count=np.int32, cum_off=np.int64, cum_flat=np.float32, region_member=np.int32,
+              member_start=np.int64, member_seed=np.uint64)
+    return {k: np.ascontiguousarray(v, dtype=dt[k]) for k, v in t.items()}
+
+
 def gen_rows(spec: dict, row_begin: int, row_end: int):
     """Rows [row_begin,row_end) of the counter-based synthetic network (oracle.c)."""
     K = int(spec["K"])
@@ -168,9 +187,11 @@ def gen_rows(spec: dict, row_begin: int, row_end: int):
     w = np.zeros(n * K * 2, np.float32)
     rs = np.ascontiguousarray(spec["region_start"], dtype=np.int64)
     ne = np.ascontiguousarray(spec["region_n_exc"], dtype=np.int64)
-    cum = np.ascontiguousarray(spec["cum"], dtype=np.float32)
-    bad = lib().oracle_gen_rows(int(spec["gen_seed"]), len(rs) - 1, _p(rs), _p(ne), _p(cum), K,
-                                float(spec.get("w_scale", 1.0)), row_begin, row_end, _p(pre), _p(kind), _p(w))
+    t = general_tables(spec)
+    bad = lib().oracle_gen_rows(len(rs) - 1, _p(rs), _p(ne), _p(t["src_base"]), _p(t["src_count"]), _p(t["cum_off"]),
+                                _p(t["cum_flat"]), _p(t["region_member"]), _p(t["member_start"]),
+                                _p(t["member_seed"]), K, float(spec.get("w_scale", 1.0)), row_begin, row_end,
+                                _p(pre), _p(kind), _p(w))
     if bad:
         raise RuntimeError(f"generator could not draw {K} distinct sources for {bad} rows")
     return pre, kind, w.reshape(-1, 2)

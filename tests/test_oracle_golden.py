@@ -119,3 +119,20 @@ def test_generator_rows_are_deterministic_and_valid():
     own = region == (np.searchsorted(spec.region_start, np.arange(spec.N), side="right") - 1)[:, None]
     assert abs(own.mean() - 0.8) < 0.03                            # 80 % intra-region
     assert 0.0 <= w_a.min() and w_a.max() < 1.0
+
+
+def test_ensemble_members_equal_standalone_networks():
+    """Members of a concatenated ensemble keep their own connectivity (member-local generator counters)."""
+    t = [synthetic.single_block(500, 20, gen_seed=11, name="m0"),
+         synthetic.whole_brain(R=3, mean_size=300, sigma=0.3, K=20, gen_seed=12, name="m1"),
+         synthetic.single_block(300, 20, gen_seed=13, name="m2")]
+    e = synthetic.ensemble(t, g_scale=np.array([[1, 1, 1, 1], [1.2, 0.8, 1, 1], [0.5, 1, 1.5, 1]], np.float32))
+    assert (e.members["member_start"] % 128 == 0).all()
+    pe, ke, we = O.gen_rows(e.as_dict(), 0, e.N)
+    K = e.K
+    for m, tm in enumerate(t):
+        ps, ks, ws = O.gen_rows(tm.as_dict(), 0, tm.N)
+        ms = int(e.members["member_start"][m])
+        seg = slice(ms * K, (ms + tm.N) * K)
+        assert np.array_equal(pe[seg].astype(np.int64) - ms, ps.astype(np.int64))
+        assert np.array_equal(ke[seg], ks) and np.array_equal(we[seg], ws)
