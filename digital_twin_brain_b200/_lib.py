@@ -20,7 +20,7 @@ MODE_AUTO, MODE_PUSH, MODE_PULL = 0, 1, 2
 MODES = {"auto": MODE_AUTO, "push": MODE_PUSH, "pull": MODE_PULL}
 
 FIELD_V, FIELD_J, FIELD_I_UI, FIELD_I_SYN, FIELD_T_LAST, FIELD_ACTIVE, FIELD_NEW_ACTIVE, FIELD_T, FIELD_STEP, \
-    FIELD_SUB_COUNT, FIELD_EVENTS = range(11)
+    FIELD_SUB_COUNT, FIELD_EVENTS, FIELD_WINDOW_SPIKES = range(12)
 
 TUNE_SCATTER_WORDS, TUNE_CHUNK, TUNE_PULL_THRESHOLD_PPM, TUNE_USE_GRAPHS, TUNE_STEP_VARIANT = range(5)
 
@@ -87,11 +87,23 @@ _SIGS = {
     "dtb_bold_set_stream": [c_vp, c_vp],
     "dtb_bold_run": [c_vp, c_vp, c_vp, c_int],
     "dtb_bold_state_update": [c_vp, c_vp, c_i64, c_i64, c_i64, c_int],
+    "dtb_bold_run_steps": [c_vp, c_vp, c_int, c_f64, c_vp, c_int],
     "dtb_bold_get": [c_vp, c_int, c_vp, c_int],
     "dtb_bold_set": [c_vp, c_int, c_vp, c_int],
     "dtb_block_attach_bold": [c_vp, c_int, c_vp, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64],
     "dtb_block_get_bold": [c_vp, c_int, c_vp, c_int],
+    "dtb_block_set_bold": [c_vp, c_int, c_vp, c_int],
     "dtb_step_preallocated": [c_vp, c_f32, c_u64, c_f32, c_int, c_vp, c_vp, c_vp],
+    "dtb_mlp_create": [c_int, c_int, c_u64, c_int, ctypes.POINTER(c_vp)],
+    "dtb_mlp_destroy": [c_vp],
+    "dtb_mlp_set_stream": [c_vp, c_vp],
+    "dtb_mlp_n_params": [c_vp, ctypes.POINTER(c_i64)],
+    "dtb_mlp_get_params": [c_vp, c_vp, c_int],
+    "dtb_mlp_set_params": [c_vp, c_vp, c_int],
+    "dtb_mlp_forward": [c_vp, c_vp, c_i64, c_vp],
+    "dtb_mlp_gradient": [c_vp, c_vp, c_vp, c_i64, c_vp, c_vp],
+    "dtb_mlp_train_step": [c_vp, c_vp, c_vp, c_i64, c_f32, c_vp],
+    "dtb_mlp_last_error": [c_char_p, c_size_t],
 }
 
 _lock = threading.Lock()
@@ -127,10 +139,14 @@ def last_error() -> str:
     return buf.value.decode(errors="replace")
 
 
-def check(rc: int):
+def check(rc: int, mlp: bool = False):
     if rc != 0:
+        if mlp:
+            buf = ctypes.create_string_buffer(1024)
+            load().dtb_mlp_last_error(buf, len(buf))
+            raise DtbError(rc, buf.value.decode(errors="replace"))
         raise DtbError(rc, last_error())
 
 
 def call(name: str, *args):
-    check(getattr(load(), name)(*args))
+    check(getattr(load(), name)(*args), mlp=name.startswith("dtb_mlp_"))

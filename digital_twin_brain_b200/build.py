@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libdtb.so")
 
-SOURCES = ["dtb_api.cu", "dtb_prealloc.cu", "dtb_io.cpp"]
+SOURCES = ["dtb_api.cu", "dtb_prealloc.cu", "dtb_mlp.cu", "dtb_io.cpp"]
 HEADERS = ["dtb_device.cuh", "dtb_kernels.cuh", "dtb_io.h"]
 
 NVCC_FLAGS = [

@@ -322,6 +322,8 @@ static int upload_class_tables(dtb_block* b)
         RET(dalloc(b, &s.sub_spk, (size_t)cap));
         RET(dalloc(b, &s.sub_nact, (size_t)cap));
         RET(dalloc(b, &s.sub_vsum, (size_t)cap));
+        RET(dalloc(b, &s.win_spk, (size_t)cap));
+        CK(cudaMemsetAsync(s.win_spk, 0, sizeof(unsigned long long) * cap, b->stream));
         CK(cudaMemsetAsync(s.sub_spk, 0, sizeof(uint32_t) * cap, b->stream));
         CK(cudaMemsetAsync(s.sub_nact, 0, sizeof(uint32_t) * cap, b->stream));
         CK(cudaMemsetAsync(s.sub_vsum, 0, sizeof(double) * cap, b->stream));
@@ -429,8 +431,11 @@ static void destroy_block(dtb_block* b)
     delete b;
 }
 
+static int rebuild_groups(dtb_block* b, const int32_t* sub_to_region);
+
 static int finish_create(dtb_block* b)
 {
+    RET(rebuild_groups(b, nullptr));
     CK(cudaMallocHost((void**)&b->h_run, sizeof(RunParams)));
     RET(ensure_stats(b, 256));
     CK(cudaStreamSynchronize(b->stream));
@@ -438,6 +443,55 @@ static int finish_create(dtb_block* b)
 }
 
 // ------------------------------------------------------------ launches
+// Statistics outside the update kernel when the subblock / region count is
+// large: groups = BOLD regions with their subblocks, plus lone subblocks.
+static int rebuild_groups(dtb_block* b, const int32_t* sub_to_region)
+{
+    DevState& s = b->ds;
+    const int n_sub = b->n_sub;
+    const int R = b->bold_R;
+    s.stats_ext = (n_sub > 512 || R > 128) ? 1 : 0;
+    if (!s.stats_ext) return DTB_OK;
+    std::vector<int32_t> ptr, sub, reg;
+    if (R > 0 && sub_to_region) {
+        std::vector<std::vector<int32_t>> members((size_t)R);
+        std::vector<int32_t> lone;
+        for (int i = 0; i < n_sub; ++i) {
+            const int r = sub_to_region[i];
+            if (r >= 0 && r < R) members[(size_t)r].push_back(i); else lone.push_back(i);
+        }
+        ptr.push_back(0);
+        for (int r = 0; r < R; ++r) {
+            for (int32_t i : members[(size_t)r]) sub.push_back(i);
+            ptr.push_back((int32_t)sub.size());
+            reg.push_back(r);
+        }
+        for (int32_t i : lone) { sub.push_back(i); ptr.push_back((int32_t)sub.size()); reg.push_back(-1); }
+    } else {
+        for (int i = 0; i <= n_sub; ++i) ptr.push_back(i);
+        for (int i = 0; i < n_sub; ++i) { sub.push_back(i); reg.push_back(-1); }
+    }
+    int32_t *dp = nullptr, *ds = nullptr, *dr = nullptr;
+    RET(dalloc(b, &dp, ptr.size()));
+    RET(dalloc(b, &ds, std::max<size_t>(1, sub.size())));
+    RET(dalloc(b, &dr, std::max<size_t>(1, reg.size())));
+    CK(cudaMemcpy(dp, ptr.data(), sizeof(int32_t) * ptr.size(), cudaMemcpyHostToDevice));
+    if (!sub.empty()) CK(cudaMemcpy(ds, sub.data(), sizeof(int32_t) * sub.size(), cudaMemcpyHostToDevice));
+    if (!reg.empty()) CK(cudaMemcpy(dr, reg.data(), sizeof(int32_t) * reg.size(), cudaMemcpyHostToDevice));
+    s.grp_ptr = dp; s.grp_sub = ds; s.grp_region = dr;
+    s.n_groups = (int)reg.size();
+    return DTB_OK;
+}
+
+static int launch_stats(dtb_block* b, const DevState& s)
+{
+    if (!s.stats_ext || s.n_groups <= 0) return DTB_OK;
+    k_stats<<<grid_for(s.n_groups, 256), 256, 0, b->stream>>>(s);
+    CK(cudaGetLastError());
+    b->launches++;
+    return DTB_OK;
+}
+
 // Persistent step kernels: as many CTAs as are resident at once, each warp
 // streaming a contiguous run of tiles.
 template <bool G, bool U, bool F, int M>
@@ -491,7 +545,7 @@ static int launch_update(dtb_block* b, const DevState& s, bool gather, bool forc
     }
     CK(cudaGetLastError());
     b->launches++;
-    return DTB_OK;
+    return launch_stats(b, s);
 }
 
 static int launch_gather_only(dtb_block* b, const DevState& s)
@@ -1278,6 +1332,8 @@ int dtb_block_get(dtb_block* b, int field, void* dst, int where)
         return copy_out(b, dst, &s.ctl->steps_done, sizeof(uint64_t), where);
     }
     case DTB_FIELD_EVENTS: return copy_out(b, dst, &s.ctl->events, sizeof(unsigned long long), where);
+    case DTB_FIELD_WINDOW_SPIKES:
+        return copy_out(b, dst, s.win_spk, sizeof(unsigned long long) * (size_t)b->n_sub, where);
     case DTB_FIELD_SUB_COUNT:
         if (where == DTB_HOST) { if (b->n_sub) std::memcpy(dst, b->sub_count.data(), sizeof(uint32_t) * b->n_sub); return DTB_OK; }
         return copy_out(b, dst, s.sub_count, sizeof(uint32_t) * b->n_sub, where);
@@ -1317,6 +1373,9 @@ int dtb_block_set(dtb_block* b, int field, const void* src, int where)
         break;
     }
     case DTB_FIELD_T: CK(cudaMemcpyAsync(&s.ctl->t, src, sizeof(float), k, b->stream)); break;
+    case DTB_FIELD_WINDOW_SPIKES:
+        CK(cudaMemcpyAsync(s.win_spk, src, sizeof(unsigned long long) * (size_t)b->n_sub, k, b->stream));
+        break;
     case DTB_FIELD_STEP: {
         uint64_t v;
         if (where == DTB_HOST) std::memcpy(&v, src, 8);
@@ -1350,6 +1409,7 @@ int dtb_block_update_property(dtb_block* b, const float* property, const float* 
     RET(upload_class_tables(b));
     CK(cudaMemcpy(const_cast<uint32_t*>(s.cls), cls.data(), sizeof(uint32_t) * (size_t)b->N, cudaMemcpyHostToDevice));
     if (!s.st_spk) RET(ensure_stats(b, 256));
+    if (b->bold_R == 0) RET(rebuild_groups(b, nullptr));
     b->class_prop_base.clear();
     for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
     b->override_pending = true;
@@ -1364,19 +1424,32 @@ int dtb_block_scale_property_by_subblock(dtb_block* b, int n, const int32_t* sub
     for (int i = 0; i < n; ++i) {
         if (col[i] < 0 || col[i] >= DTB_NPROP || col[i] == 3) return fail(DTB_ERR_ARG, "column %d cannot be scaled", col[i]);
     }
+    // classes of every subblock (a subblock can span several classes)
+    std::unordered_map<int32_t, std::vector<int32_t>> by_sub;
+    for (int c = 0; c < b->n_classes; ++c) by_sub[b->classes[(size_t)c].sub].push_back(c);
+    std::vector<char> dirty((size_t)b->n_classes, 0);
     for (int i = 0; i < n; ++i) {
-        for (int c = 0; c < b->n_classes; ++c) {
-            if (b->classes[(size_t)c].sub != sub[i]) continue;
+        auto it = by_sub.find(sub[i]);
+        if (it == by_sub.end()) continue;
+        for (int32_t c : it->second) {
             auto& row = b->class_prop[(size_t)c];
             volatile float v = b->class_prop_base[(size_t)c][(size_t)col[i]] * value[i];
             row[(size_t)col[i]] = v;
-            float dc[4] = {b->class_decay[(size_t)c][0], b->class_decay[(size_t)c][1], b->class_decay[(size_t)c][2],
-                           b->class_decay[(size_t)c][3]};
-            if (col[i] >= 18) { default_decay(row.data(), b->dt, dc); b->class_decay[(size_t)c] = {dc[0], dc[1], dc[2], dc[3]}; }
-            ParamClass p = make_class(row.data(), dc, b->dt);
-            p.sub = b->classes[(size_t)c].sub;
-            b->classes[(size_t)c] = p;
+            dirty[(size_t)c] = 1;
         }
+    }
+    for (int c = 0; c < b->n_classes; ++c) {
+        if (!dirty[(size_t)c]) continue;
+        auto& row = b->class_prop[(size_t)c];
+        float dc[4] = {b->class_decay[(size_t)c][0], b->class_decay[(size_t)c][1], b->class_decay[(size_t)c][2],
+                       b->class_decay[(size_t)c][3]};
+        bool tau_changed = false;
+        for (int k = 18; k < 22; ++k) tau_changed |= row[(size_t)k] != b->class_prop_base[(size_t)c][(size_t)k];
+        if (tau_changed) { default_decay(row.data(), b->dt, dc); b->class_decay[(size_t)c] = {dc[0], dc[1], dc[2], dc[3]}; }
+        ParamClass p = make_class(row.data(), dc, b->dt);
+        p.sub = b->classes[(size_t)c].sub;
+        p.member = b->classes[(size_t)c].member;
+        b->classes[(size_t)c] = p;
     }
     CK(cudaMemcpyAsync(const_cast<ParamClass*>(b->ds.pc), b->classes.data(), sizeof(ParamClass) * b->classes.size(),
                        cudaMemcpyHostToDevice, b->stream));
@@ -1583,6 +1656,35 @@ int dtb_bold_run(dtb_bold* m, const void* u, void* out, int where)
     return DTB_OK;
 }
 
+int dtb_bold_run_steps(dtb_bold* m, const void* u, int n_steps, double u_floor, void* out, int where)
+{
+    if (!m || !u || !out || n_steps < 0) return fail(DTB_ERR_ARG, "bad argument");
+    DeviceGuard g(m->device);
+    const size_t bytes = (m->dtype ? 8 : 4) * (size_t)m->R;
+    const void* du = u;
+    void* dout = out;
+    if (where == DTB_HOST) {
+        CK(cudaMemcpyAsync(m->tmp_u, u, bytes, cudaMemcpyHostToDevice, m->stream));
+        du = m->tmp_u;
+        dout = m->tmp_o;
+    }
+    const unsigned gr = grid_for(m->R, 128);
+    if (m->dtype == 0)
+        k_bold_run_steps<float><<<gr, 128, 0, m->stream>>>(m->R, (const float*)du, n_steps, (float)u_floor,
+                                                           (float*)m->s, (float*)m->q, (float*)m->v, (float*)m->f,
+                                                           (float*)dout, bold_scalars<float>(m));
+    else
+        k_bold_run_steps<double><<<gr, 128, 0, m->stream>>>(m->R, (const double*)du, n_steps, u_floor,
+                                                            (double*)m->s, (double*)m->q, (double*)m->v,
+                                                            (double*)m->f, (double*)dout, bold_scalars<double>(m));
+    CK(cudaGetLastError());
+    if (where == DTB_HOST) {
+        CK(cudaMemcpyAsync(out, m->tmp_o, bytes, cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
+    }
+    return DTB_OK;
+}
+
 int dtb_bold_state_update(dtb_bold* m, const void* w, int64_t E, int64_t Rp, int64_t S, int where)
 {
     if (!m || !w) return fail(DTB_ERR_ARG, "null argument");
@@ -1668,7 +1770,21 @@ int dtb_block_attach_bold(dtb_block* b, int n_regions, const int32_t* sub_to_reg
     bd.epsilon = epsilon; bd.tao_s = tao_s; bd.tao_f = tao_f; bd.tao_0 = tao_0; bd.div_alpha = 1.0 / alpha;
     bd.E0 = E_0; bd.V0 = V_0; bd.delta_t = delta_t;
     b->bold_R = n_regions;
+    RET(rebuild_groups(b, sub_to_region));
     for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+    return DTB_OK;
+}
+
+int dtb_block_set_bold(dtb_block* b, int field, const double* src, int where)
+{
+    if (!b || !src || field < 0 || field > 3) return fail(DTB_ERR_ARG, "bad argument");
+    if (b->bold_R == 0) return fail(DTB_ERR_STATE, "no BOLD model attached");
+    DeviceGuard g(b->device);
+    const BoldDev& bd = b->ds.bold;
+    double* dst[4] = {bd.s, bd.q, bd.v, bd.f};
+    CK(cudaMemcpyAsync(dst[field], src, sizeof(double) * b->bold_R,
+                       where == DTB_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
     return DTB_OK;
 }
 

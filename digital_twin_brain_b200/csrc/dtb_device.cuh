@@ -102,6 +102,12 @@ struct DevState {
     double* sub_vsum;           // [n_sub]
     const uint32_t* sub_count;  // [n_sub] neurons per subblock
     uint32_t* unmapped_nact;    // new_active of neurons whose subblock is out of range
+    unsigned long long* win_spk; // [n_sub] spikes accumulated since the host last cleared them
+    int stats_ext;              // 1: statistics and BOLD in k_stats (many subblocks / regions)
+    const int32_t* grp_ptr;     // k_stats groups: [n_groups+1] into grp_sub
+    const int32_t* grp_sub;     // subblocks of every group
+    const int32_t* grp_region;  // [n_groups] BOLD region of the group or -1
+    int n_groups;
     float* st_spk;              // [stats_cap][n_sub]
     float* st_mean;             // [stats_cap][n_sub]
     uint32_t* st_nact;          // [stats_cap]

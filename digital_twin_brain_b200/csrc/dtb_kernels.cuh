@@ -112,6 +112,25 @@ __device__ __forceinline__ float4 gather_row(const DevState& s, const uint32_t* 
     return make_float4(a0, a1, a2, a3);
 }
 
+// ------------------------------------------------------------ BOLD step
+// models/bold_model_pytorch.py:43-78 in float64 for region r with input u
+// (q before v before f_in before s, f_in clamped at 0).
+__device__ __forceinline__ void bold_region_step(const BoldDev& b, int r, double u)
+{
+    double fi = b.f[r], si = b.s[r], qi = b.q[r], vi = b.v[r];
+    const double ds = ((b.epsilon * u) - si / b.tao_s) - (fi - 1.0) / b.tao_f;
+    const double qpart = fi > 0.0 ? (1.0 - pow(1.0 - b.E0, 1.0 / fi)) : 1.0;
+    const double dq = (((fi * qpart) / b.E0) - qi * pow(vi, b.div_alpha - 1.0)) / b.tao_0;
+    qi = qi + dq * b.delta_t;
+    const double dv = (fi - pow(vi, b.div_alpha)) / b.tao_0;
+    vi = vi + dv * b.delta_t;
+    fi = fi + si * b.delta_t;
+    fi = fi > 0.0 ? fi : 0.0;
+    si = si + ds * b.delta_t;
+    b.s[r] = si; b.q[r] = qi; b.v[r] = vi; b.f[r] = fi;
+    b.out[r] = b.V0 * ((7.0 * b.E0 * (1.0 - qi) + 2.0 * (1.0 - qi / vi)) + (2.0 * b.E0 - 0.2) * (1.0 - vi));
+}
+
 // ------------------------------------------------------------ epilogue
 // Runs in the last CTA of an update kernel: per-subblock statistics of step
 // `steps_done` (models/block.py:144-150), BOLD (simulation/simulation.py:
@@ -121,6 +140,17 @@ __device__ void step_epilogue(const DevState& s, unsigned long long steps_done, 
     Ctl* ctl = s.ctl;
     const unsigned long long row = steps_done - ctl->run_base;
     const bool write = row < (unsigned long long)ctl->stats_cap;
+    if (s.stats_ext) {   // k_stats folds the statistics right after this kernel
+        if (threadIdx.x == 0) {
+            if (write) s.st_nact[row] = atomicExch(s.unmapped_nact, 0u);
+            ctl->t = t;
+            ctl->use_isyn_override = 0u;
+            ctl->done = 0u;
+            ctl->steps_done = steps_done + 1ull;
+            __threadfence();
+        }
+        return;
+    }
     __shared__ unsigned long long sh_nact;
     if (threadIdx.x == 0) sh_nact = atomicExch(s.unmapped_nact, 0u);
     if (s.bold.n_regions > 0)
@@ -133,6 +163,7 @@ __device__ void step_epilogue(const DevState& s, unsigned long long steps_done, 
             atomicExch(reinterpret_cast<unsigned long long*>(s.sub_vsum + i), 0ull);
         const double vsum = __longlong_as_double((long long)vb);
         const uint32_t cnt = s.sub_count[i];
+        if (s.win_spk) s.win_spk[i] += spk;
         if (write) {
             s.st_spk[row * s.n_sub + i] = (float)spk;
             s.st_mean[row * s.n_sub + i] = cnt ? (float)(vsum / (double)cnt) : __int_as_float(0x7fc00000);
@@ -149,19 +180,7 @@ __device__ void step_epilogue(const DevState& s, unsigned long long steps_done, 
         for (int r = threadIdx.x; r < b.n_regions; r += blockDim.x) {
             const double act = b.region_n[r] > 0.0 ? b.act[r] / b.region_n[r] : 0.0;
             b.act[r] = act;
-            const double u = act > 1e-5 ? act : 1e-5;
-            double fi = b.f[r], si = b.s[r], qi = b.q[r], vi = b.v[r];
-            const double ds = ((b.epsilon * u) - si / b.tao_s) - (fi - 1.0) / b.tao_f;
-            const double qpart = fi > 0.0 ? (1.0 - pow(1.0 - b.E0, 1.0 / fi)) : 1.0;
-            const double dq = (((fi * qpart) / b.E0) - qi * pow(vi, b.div_alpha - 1.0)) / b.tao_0;
-            qi = qi + dq * b.delta_t;
-            const double dv = (fi - pow(vi, b.div_alpha)) / b.tao_0;
-            vi = vi + dv * b.delta_t;
-            fi = fi + si * b.delta_t;
-            fi = fi > 0.0 ? fi : 0.0;
-            si = si + ds * b.delta_t;
-            b.s[r] = si; b.q[r] = qi; b.v[r] = vi; b.f[r] = fi;
-            b.out[r] = b.V0 * ((7.0 * b.E0 * (1.0 - qi) + 2.0 * (1.0 - qi / vi)) + (2.0 * b.E0 - 0.2) * (1.0 - vi));
+            bold_region_step(b, r, act > 1e-5 ? act : 1e-5);
         }
     }
     if (threadIdx.x == 0) {
@@ -172,6 +191,46 @@ __device__ void step_epilogue(const DevState& s, unsigned long long steps_done, 
         ctl->steps_done = steps_done + 1ull;
         __threadfence();
     }
+}
+
+// ------------------------------------------------------------ statistics kernel
+// For networks with many subblocks or regions (ensembles): one thread per
+// group (a BOLD region with its subblocks, or a lone subblock) folds the
+// accumulators of the step just taken into the per-step rows and the window
+// totals, and runs the region's BOLD step.  Launched right after each update.
+__global__ void __launch_bounds__(256) k_stats(DevState s)
+{
+    const Ctl* ctl = s.ctl;
+    const unsigned long long row = ctl->steps_done - 1ull - ctl->run_base;   // clock already advanced
+    const bool write = row < (unsigned long long)ctl->stats_cap;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t nact_sum = 0;
+    if (g < s.n_groups) {
+        double spk_sum = 0.0;
+        for (int k = s.grp_ptr[g]; k < s.grp_ptr[g + 1]; ++k) {
+            const int i = s.grp_sub[k];
+            const uint32_t spk = atomicExch(s.sub_spk + i, 0u);
+            nact_sum += atomicExch(s.sub_nact + i, 0u);
+            const double vsum = __longlong_as_double(
+                (long long)atomicExch(reinterpret_cast<unsigned long long*>(s.sub_vsum + i), 0ull));
+            const uint32_t cnt = s.sub_count[i];
+            if (s.win_spk) s.win_spk[i] += spk;
+            if (write) {
+                s.st_spk[row * s.n_sub + i] = (float)spk;
+                s.st_mean[row * s.n_sub + i] = cnt ? (float)(vsum / (double)cnt) : __int_as_float(0x7fc00000);
+            }
+            spk_sum += (double)spk;
+        }
+        const int r = s.grp_region[g];
+        if (r >= 0 && s.bold.n_regions > 0) {
+            const BoldDev& b = s.bold;
+            const double act = b.region_n[r] > 0.0 ? spk_sum / b.region_n[r] : 0.0;
+            b.act[r] = act;
+            bold_region_step(b, r, act > 1e-5 ? act : 1e-5);
+        }
+    }
+    const uint32_t w = __reduce_add_sync(0xffffffffu, nact_sum);
+    if ((threadIdx.x & 31) == 0 && w && write) atomicAdd(s.st_nact + row, w);
 }
 
 // ------------------------------------------------------------ step kernel
@@ -635,6 +694,32 @@ __global__ void k_bold_run(int64_t R, const T* __restrict__ u, T* s, T* q, T* v,
     fi = fi + si * c.dt;
     fi = fi > (T)0 ? fi : (T)0;
     si = si + ds * c.dt;
+    s[i] = si; q[i] = qi; v[i] = vi; f[i] = fi;
+    out[i] = ((c.k7 * (one - qi) + (one - qi / vi) * (T)2) + c.k2 * (one - vi)) * c.V0;
+}
+
+// n_steps Euler steps of BOLD.run with a constant input per region
+// (u_r = max(u[r], floor)), outputs the last step's signal.
+template <typename T>
+__global__ void k_bold_run_steps(int64_t R, const T* __restrict__ u, int n_steps, T floor_u, T* s, T* q, T* v, T* f,
+                                 T* __restrict__ out, BoldScalars<T> c)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R) return;
+    T fi = f[i], si = s[i], qi = q[i], vi = v[i];
+    const T one = (T)1;
+    const T ui = u[i] > floor_u ? u[i] : floor_u;
+    for (int k = 0; k < n_steps; ++k) {
+        const T ds = ((ui * c.eps) - si / c.ts) - (fi - one) / c.tf;
+        const T qpart = fi > (T)0 ? (one - dpow(c.base, (one / fi) * one)) : one;
+        const T dq = (((fi * qpart) / c.E0) - qi * dpow(vi, c.exq)) / c.t0;
+        qi = qi + dq * c.dt;
+        const T dv = (fi - dpow(vi, c.exv)) / c.t0;
+        vi = vi + dv * c.dt;
+        fi = fi + si * c.dt;
+        fi = fi > (T)0 ? fi : (T)0;
+        si = si + ds * c.dt;
+    }
     s[i] = si; q[i] = qi; v[i] = vi; f[i] = fi;
     out[i] = ((c.k7 * (one - qi) + (one - qi / vi) * (T)2) + c.k2 * (one - vi)) * c.V0;
 }

@@ -1,0 +1,130 @@
+"""Data-assimilation window benchmark: surrogate-served vs all-simulator ensemble.
+
+    python -m digital_twin_brain_b200.da_bench [--members 128] [--judges 16] [--regions 90]
+        [--region-size 2000] [--windows 50] [--steps-per-window 8000] [--train-windows 18] [--out FILE]
+
+1. Truth: one network with hidden true g_ui factors (per region, 4 receptors)
+   runs `windows` windows; its BOLD at the end of every window plus Gaussian
+   noise (sigma = 0.1 x the per-region std over windows) is the observation.
+2. Plain: EnsembleDA with every member on the simulator
+   (data_assimilation/DataAssimilation.py:402-453 restated).
+3. Surrogate: training windows from a random-walk ensemble, RateSurrogate
+   trained on them, then SurrogateDA (judges on the simulator, the rest
+   forecast by the network, fallback on judge error).
+Reports mean window time of both, their ratio, the BOLD-fit RMSE of the
+ensemble-mean forecast against the observation, and the g_ui recovery error.
+The reference's 2e5 neurons per region do not fit 128 members on one GPU
+(~3 TB of synapses); --region-size scales every region (stated in the output).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+import torch
+
+from . import synthetic
+from .assimilation import DAConfig, EnsembleDA, SurrogateDA, collect_windows, log_torch
+from .surrogate import RateSurrogate
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--members", type=int, default=128)
+    ap.add_argument("--judges", type=int, default=16)
+    ap.add_argument("--regions", type=int, default=90)
+    ap.add_argument("--region-size", type=float, default=2000)
+    ap.add_argument("--K", type=int, default=100)
+    ap.add_argument("--windows", type=int, default=50)
+    ap.add_argument("--steps-per-window", type=int, default=8000)
+    ap.add_argument("--train-windows", type=int, default=18)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--threshold", type=float, default=0.5)
+    ap.add_argument("--skip", type=int, default=5, help="windows excluded from the RMSE (spin-up)")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    dev = torch.device("cuda", 0)
+    t_all = time.perf_counter()
+    template = synthetic.whole_brain(R=a.regions, mean_size=a.region_size, sigma=0.5, K=a.K, gen_seed=a.seed,
+                                     name=f"da_template_{a.regions}x{int(a.region_size)}")
+    base = dict(steps_per_window=a.steps_per_window, seed=a.seed)
+    rng = np.random.default_rng(a.seed + 99)
+
+    # ---- truth and observations
+    truth = EnsembleDA(template, DAConfig(n_members=1, **base))
+    hp_true = torch.from_numpy(rng.uniform(0.6, 1.4, (template.R, 4)).astype(np.float32)).to(dev)
+    truth.hp_log = log_torch(hp_true.reshape(1, -1), truth.low, truth.high)
+    truth.apply_hp()
+    bold_true = []
+    for _ in range(a.windows):
+        bold_true.append(truth.evolve()[0, :, -1].double())
+    bold_true = torch.stack(bold_true)                                  # [W, R]
+    sd = bold_true.std(0, keepdim=True).clamp_min(1e-9)
+    obs = (bold_true + 0.1 * sd * torch.randn(bold_true.shape, device=dev, dtype=torch.float64,
+                                               generator=torch.Generator(device=dev).manual_seed(a.seed + 5)))
+    obs = obs.float()
+    del truth
+
+    def summarize(res, label):
+        bp = res["bold_pred"][a.skip:]
+        ob = obs.cpu().numpy()[a.skip:len(res["bold_pred"])]
+        rmse = float(np.sqrt(np.mean((bp - ob) ** 2)))
+        hp_fin = res["hp_mean"][-min(10, len(res["hp_mean"])):].mean(0)
+        gerr = float(np.mean(np.abs(hp_fin - hp_true.cpu().numpy()) / hp_true.cpu().numpy()))
+        ws = res["window_s"]
+        return {f"{label}_window_s": float(np.mean(ws[1:] if len(ws) > 1 else ws)), f"{label}_rmse": rmse,
+                f"{label}_gui_rel_err": gerr}
+
+    out = dict(members=a.members, judges=a.judges, regions=a.regions, region_size=a.region_size, K=a.K,
+               windows=a.windows, steps_per_window=a.steps_per_window,
+               neurons_per_member=template.N, synapses_per_member=template.S)
+
+    # ---- plain: every member on the simulator
+    plain = EnsembleDA(template, DAConfig(n_members=a.members, **base))
+    res_p = plain.run(obs)
+    out.update(summarize(res_p, "plain"))
+    del plain
+    torch.cuda.empty_cache()
+
+    # ---- surrogate training windows (a separate random-walk ensemble)
+    t0 = time.perf_counter()
+    g, h, tgt = collect_windows(template, DAConfig(n_members=a.members, **{**base, "seed": a.seed + 7}),
+                                windows=a.train_windows)
+    t_collect = time.perf_counter() - t0
+    n = g.shape[0]
+    perm = torch.from_numpy(np.random.default_rng(a.seed).permutation(n))
+    ntr = int(0.9 * n)
+    tr, te = perm[:ntr], perm[ntr:]
+    sur = RateSurrogate(seed=a.seed)
+    t0 = time.perf_counter()
+    hist = sur.fit(g[tr], h[tr], tgt[tr], epochs=a.epochs)
+    t_train = time.perf_counter() - t0
+    pred = sur.predict(g[te], h[te]).cpu()
+    eps = 1e-6
+    lerr_net = float(torch.sqrt(torch.mean((torch.log(pred + eps) - torch.log(tgt[te] + eps)) ** 2)))
+    lerr_persist = float(torch.sqrt(torch.mean((torch.log(h[te][:, -1] + eps) - torch.log(tgt[te] + eps)) ** 2)))
+    out.update(train_samples=int(n), train_windows=a.train_windows, train_collect_s=t_collect, train_s=t_train,
+               train_loss_first=hist[0], train_loss_last=hist[-1], heldout_logrmse_net=lerr_net,
+               heldout_logrmse_persistence=lerr_persist)
+
+    # ---- surrogate-served DA
+    sda = SurrogateDA(template, DAConfig(n_members=a.members, **base), sur, n_judge=a.judges,
+                      threshold=a.threshold)
+    res_s = sda.run(obs)
+    out.update(summarize(res_s, "surrogate"))
+    out.update(fallbacks=int(res_s["fallbacks"]), judge_logrmse_mean=float(np.mean(res_s["errors"])))
+    out["speedup"] = out["plain_window_s"] / out["surrogate_window_s"]
+    out["rmse_ratio"] = out["surrogate_rmse"] / out["plain_rmse"]
+    out["total_s"] = time.perf_counter() - t_all
+    line = json.dumps(out)
+    print(line)
+    if a.out:
+        with open(a.out, "w") as f:
+            f.write(line + "\n")
+
+
+if __name__ == "__main__":
+    main()

@@ -13,7 +13,8 @@ import torch
 
 from . import _lib
 from ._lib import (DTB_DEVICE, DTB_HOST, FIELD_ACTIVE, FIELD_EVENTS, FIELD_I_SYN, FIELD_I_UI, FIELD_J,
-                   FIELD_NEW_ACTIVE, FIELD_STEP, FIELD_SUB_COUNT, FIELD_T, FIELD_T_LAST, FIELD_V, MODES)
+                   FIELD_NEW_ACTIVE, FIELD_STEP, FIELD_SUB_COUNT, FIELD_T, FIELD_T_LAST, FIELD_V, FIELD_WINDOW_SPIKES,
+                   MODES)
 from .synthetic import NetworkSpec
 
 _FIELD_SHAPE = {FIELD_V: (1, np.float32), FIELD_J: (4, np.float32), FIELD_I_UI: (4, np.float32),
@@ -270,11 +271,37 @@ class Network:
                   float(tao_f), float(tao_0), float(alpha), float(E_0), float(V_0), dts)
         self.n_regions = int(n_regions)
 
-    def get_bold(self, field: str = "bold") -> np.ndarray:
+    def get_bold(self, field: str = "bold", device: bool = False):
         idx = {"s": 0, "q": 1, "v": 2, "f_in": 3, "bold": 4, "act": 5}[field]
+        if device:
+            out = torch.empty(self.n_regions, dtype=torch.float64, device=torch.device("cuda", self.device))
+            _lib.call("dtb_block_get_bold", self._h, idx, _ptr(out), DTB_DEVICE)
+            self.synchronize()
+            return out
         out = np.empty(self.n_regions, np.float64)
         _lib.call("dtb_block_get_bold", self._h, idx, _ptr(out), DTB_HOST)
         return out
+
+    def set_bold(self, field: str, value):
+        """Overwrite the BOLD state s, q, v or f_in (host array or CUDA tensor of n_regions doubles)."""
+        idx = {"s": 0, "q": 1, "v": 2, "f_in": 3}[field]
+        if isinstance(value, torch.Tensor) and value.is_cuda:
+            v = value.to(torch.float64).contiguous()
+            torch.cuda.current_stream(self.device).synchronize()
+            _lib.call("dtb_block_set_bold", self._h, idx, _ptr(v), DTB_DEVICE)
+        else:
+            v = np.ascontiguousarray(value, np.float64)
+            _lib.call("dtb_block_set_bold", self._h, idx, _ptr(v), DTB_HOST)
+
+    def window_spikes(self) -> np.ndarray:
+        """Spikes per subblock since the last clear_window_spikes() (uint64 [n_sub])."""
+        out = np.empty(self.n_sub, np.uint64)
+        _lib.call("dtb_block_get", self._h, FIELD_WINDOW_SPIKES, _ptr(out), DTB_HOST)
+        return out
+
+    def clear_window_spikes(self):
+        z = np.zeros(self.n_sub, np.uint64)
+        _lib.call("dtb_block_set", self._h, FIELD_WINDOW_SPIKES, _ptr(z), DTB_HOST)
 
 
 class BoldModel:
@@ -315,6 +342,14 @@ class BoldModel:
         out = torch.empty_like(du)
         self._on_torch_stream()
         _lib.call("dtb_bold_run", self._h, _ptr(du), _ptr(out), DTB_DEVICE)
+        return out
+
+    def run_steps(self, u: torch.Tensor, n_steps: int, u_floor: float = 1e-5) -> torch.Tensor:
+        """n_steps BOLD steps with constant input max(u, u_floor); returns the last signal."""
+        du = self._dev(u)
+        out = torch.empty_like(du)
+        self._on_torch_stream()
+        _lib.call("dtb_bold_run_steps", self._h, _ptr(du), int(n_steps), float(u_floor), _ptr(out), DTB_DEVICE)
         return out
 
     def state_update(self, w: torch.Tensor):

@@ -58,7 +58,9 @@ typedef enum {
     DTB_FIELD_T = 7,          /* float[1]      block.t            models/block.py:58  */
     DTB_FIELD_STEP = 8,       /* uint64[1]     steps taken (Philox step counter) */
     DTB_FIELD_SUB_COUNT = 9,  /* uint32[n_sub] neurons per subblock */
-    DTB_FIELD_EVENTS = 10     /* uint64[1]     synaptic events propagated since creation */
+    DTB_FIELD_EVENTS = 10,    /* uint64[1]     synaptic events propagated since creation */
+    DTB_FIELD_WINDOW_SPIKES = 11 /* uint64[n_sub] spikes per subblock since last set (window totals,
+                                    simulation/simulation.py:269-279 freqs summed over a TR) */
 } dtb_field;
 
 typedef struct dtb_block dtb_block;
@@ -275,6 +277,11 @@ int dtb_bold_destroy(dtb_bold* m);
 int dtb_bold_set_stream(dtb_bold* m, void* stream);
 /* BOLD.run (bold_model_pytorch.py:43-78): one Euler step, u -> out, both [R] of the model's dtype. */
 int dtb_bold_run(dtb_bold* m, const void* u, void* out, int where);
+/* n_steps x BOLD.run with a constant input u[r] (floored at u_floor, as
+ * simulation/simulation.py:279 floors at 1e-5); out = the last step's
+ * signal.  Integrates the hemodynamics of a window whose rate is forecast
+ * instead of simulated. */
+int dtb_bold_run_steps(dtb_bold* m, const void* u, int n_steps, double u_floor, void* out, int where);
 /* BOLD.state_update (bold_model_pytorch.py:34-41): w is [E][Rp][S] of the
  * model's dtype with E*Rp == R; s = w[..,0], q = max(w[..,1],1e-5),
  * v = max(w[..,2],1e-5), f_in = max(w[..,3],1e-5). */
@@ -293,6 +300,35 @@ int dtb_block_attach_bold(dtb_block* b, int n_regions, const int32_t* sub_to_reg
                           double E_0, double V_0, double delta_t);
 /* field: 0 s, 1 q, 2 v, 3 f_in, 4 bold output of the last step, 5 act of the last step; double[R]. */
 int dtb_block_get_bold(dtb_block* b, int field, double* dst, int where);
+/* Overwrite the attached BOLD state (field 0 s, 1 q, 2 v, 3 f_in; double[R]): the
+ * bold.state_update after an ensemble Kalman filter step
+ * (data_assimilation/DataAssimilation.py:400). */
+int dtb_block_set_bold(dtb_block* b, int field, const double* src, int where);
+
+/* ---- surrogate forecast network ------------------------------------------- */
+
+/* No counterpart in the reference (its EnKF forecast always runs the
+ * simulator, data_assimilation/DataAssimilation.py:353-370).  A multilayer
+ * perceptron in_dim -> hidden -> hidden -> 1 with GELU: BF16 weights for
+ * compute, FP32 master weights, FP32 activations and accumulation; forward,
+ * MSE backward and Adam are CUDA kernels.  Flat parameter order (FP32):
+ * W1[hidden][in_dim], b1[hidden], W2[hidden][hidden], b2[hidden], W3[hidden], b3.
+ * x / target / y / grad pointers are device memory; calls are asynchronous on
+ * the handle's stream (dtb_mlp_set_stream). */
+typedef struct dtb_mlp dtb_mlp;
+int dtb_mlp_create(int in_dim, int hidden, uint64_t seed, int device, dtb_mlp** out);
+int dtb_mlp_destroy(dtb_mlp* m);
+int dtb_mlp_set_stream(dtb_mlp* m, void* stream);
+int dtb_mlp_n_params(const dtb_mlp* m, int64_t* n);
+int dtb_mlp_get_params(dtb_mlp* m, float* dst, int where);
+int dtb_mlp_set_params(dtb_mlp* m, const float* src, int where);
+/* y[B] = MLP(x[B][in_dim]) */
+int dtb_mlp_forward(dtb_mlp* m, const float* x, int64_t B, float* y);
+/* gradient of mean((MLP(x) - target)^2) into grad[n_params] and the loss into *loss (both nullable) */
+int dtb_mlp_gradient(dtb_mlp* m, const float* x, const float* target, int64_t B, float* grad, float* loss);
+/* one Adam step (beta 0.9 / 0.999, eps 1e-8) on that loss */
+int dtb_mlp_train_step(dtb_mlp* m, const float* x, const float* target, int64_t B, float lr, float* loss);
+int dtb_mlp_last_error(char* buf, size_t len);
 
 /* ---- one step without any allocation ------------------------------------ */
 

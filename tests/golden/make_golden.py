@@ -186,8 +186,42 @@ def case_bold(steps: int = 300, R: int = 16, seed: int = 3):
     print("bold: ok")
 
 
+def case_enkf(seed: int = 5):
+    """data_assimilation/DataAssimilation.py:40-60 diffusion_enkf with torch.normal fixed."""
+    sys.path.insert(0, os.path.join(REF, "data_assimilation"))
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("ref_da_enkf", os.path.join(REF, "data_assimilation",
+                                                                              "DataAssimilation.py"))
+    src = open(spec.origin).read()
+    # only the filter function: the module imports matplotlib and the gRPC simulation at top level
+    start = src.index("def diffusion_enkf(")
+    end = src.index("class DataAssimilation(")
+    ns = {"torch": torch, "np": np}
+    exec(compile(src[start:end], spec.origin, "exec"), ns)
+    rng = np.random.default_rng(seed)
+    out = {}
+    for name, (E, R, S) in {"small": (8, 5, 10), "da": (128, 90, 10)}.items():
+        w_hat = torch.from_numpy(rng.normal(0.0, 1.0, (E, R, S)).astype(np.float32))
+        w_hat[:, :, -1] = torch.from_numpy(rng.uniform(0.01, 0.05, (E, R)).astype(np.float32))
+        bold_t = torch.from_numpy(rng.uniform(0.01, 0.05, (1, R)).astype(np.float32))
+        noise = torch.from_numpy(rng.normal(0.0, 1.0, (E, R)).astype(np.float32))
+        orig = torch.normal
+        torch.normal = lambda *a, **k: noise.clone()
+        try:
+            w = ns["diffusion_enkf"](w_hat, 1e-4, bold_t, 0.8)
+        finally:
+            torch.normal = orig
+        out.update({f"{name}_w_hat": w_hat.numpy(), f"{name}_bold_t": bold_t.numpy(), f"{name}_noise": noise.numpy(),
+                    f"{name}_w": w.numpy()})
+    np.savez_compressed(os.path.join(HERE, "enkf_ref.npz"), bold_sigma=1e-4, solo_rate=0.8, **out)
+    print("enkf: ok")
+
+
 if __name__ == "__main__":
     torch.set_num_threads(8)
+    if "--enkf" in sys.argv:
+        case_enkf()
+        sys.exit(0)
     case_bold()
     case_small_unsorted()
     case_single_block()

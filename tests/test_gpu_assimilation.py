@@ -1,0 +1,56 @@
+"""Data assimilation on the device: ensemble windows, EnKF analysis, surrogate-served windows."""
+import numpy as np
+import pytest
+import torch
+
+from digital_twin_brain_b200 import synthetic
+from digital_twin_brain_b200.assimilation import DAConfig, EnsembleDA, SurrogateDA, collect_windows, log_torch
+from digital_twin_brain_b200.surrogate import RateSurrogate
+
+pytestmark = pytest.mark.gpu
+
+TEMPLATE = synthetic.whole_brain(R=6, mean_size=400, sigma=0.3, K=40, gen_seed=3, name="da_small")
+
+
+def test_ensemble_da_window_and_filter():
+    cfg = DAConfig(n_members=12, steps_per_window=400, seed=1)
+    da = EnsembleDA(TEMPLATE, cfg)
+    da.hp_random_initialize()
+    h = da.da_evolve()
+    assert h.shape == (12, TEMPLATE.R, 4 + 6) and torch.isfinite(h).all()
+    rates = da.window_rates()
+    assert rates.shape == (12, TEMPLATE.R) and (rates > 0).all()
+    obs = h[:, :, -1].mean(0)
+    before = da.hp_log.clone()
+    da.da_filter(obs)
+    assert not torch.equal(before, da.hp_log)
+    np.testing.assert_allclose(da.net.get_bold("s")[da.region_idx.reshape(-1)],
+                               da.hidden[:, :, -5].reshape(-1).double().cpu().numpy(), rtol=1e-6)
+
+
+def test_member_hp_changes_its_own_rate():
+    cfg = DAConfig(n_members=2, steps_per_window=1500, seed=2)
+    da = EnsembleDA(TEMPLATE, cfg)
+    hp = torch.ones(2, TEMPLATE.R * 4, device=da.dev)
+    hp[1, 0::4] = 1.45      # more AMPA in member 1
+    hp[1, 2::4] = 0.55      # less GABAa
+    da.hp_log = log_torch(hp.clamp(0.51, 1.49), da.low, da.high)
+    da.apply_hp()
+    da.evolve()
+    r = da.window_rates()
+    assert (r[1] > r[0]).mean() >= 0.8
+
+
+def test_surrogate_da_runs_with_judges_and_fallback():
+    cfg = DAConfig(n_members=12, steps_per_window=300, seed=3)
+    g, h, t = collect_windows(TEMPLATE, cfg, windows=10)
+    assert g.shape[0] == h.shape[0] == t.shape[0] == 2 * 12 * TEMPLATE.R and h.shape[1] == 8
+    sur = RateSurrogate(seed=0)
+    sur.fit(g, h, t, epochs=5)
+    sda = SurrogateDA(TEMPLATE, cfg, sur, n_judge=4, threshold=0.0)     # always falls back
+    obs = torch.full((3, TEMPLATE.R), 0.02, device=sda.dev)
+    res = sda.run(obs)
+    assert res["fallbacks"] == 3 and np.isfinite(res["bold_pred"]).all()
+    sda2 = SurrogateDA(TEMPLATE, cfg, sur, n_judge=4, threshold=1e9)    # never falls back
+    res2 = sda2.run(obs)
+    assert res2["fallbacks"] == 0 and np.isfinite(res2["bold_pred"]).all()

@@ -70,3 +70,39 @@ def test_pad_neurons_stay_silent():
     cls = e.neuron_class()
     pad = e.class_property[cls, 3] < 0
     assert pad.any() and not na[pad].any()
+
+
+def test_many_subblocks_stats_and_bold_match_standalone():
+    """300 members: statistics and per-region BOLD run in the multi-CTA k_stats kernel;
+    each member still equals the same network simulated alone (in-kernel epilogue)."""
+    M = 300
+    t = [synthetic.single_block(300, 10, gen_seed=100 + m, name=f"s{m}") for m in range(M)]
+    e = synthetic.ensemble(t)
+    ens = Network.from_spec(e, device=0, build_push=False)
+    ens.attach_bold(e.sub_to_region(), e.R)
+    ens.clear_window_spikes()
+    s_e, m_e, na_e = ens.run(120, mode="pull")
+    win = ens.window_spikes()
+    assert np.array_equal(win.astype(np.float64), s_e.sum(0).astype(np.float64))
+    bold_e = ens.get_bold("bold")
+    for m in (0, 137, M - 1):
+        alone = synthetic.single_block(300, 10, gen_seed=100 + m, name="alone")
+        alone.stream_id = m
+        net = Network.from_spec(alone, device=0, build_push=False)
+        net.attach_bold(alone.sub_to_region(), alone.R)
+        s_a, m_a, _ = net.run(120, mode="pull")
+        r = synthetic.member_region_index(e, m, 0)
+        assert np.array_equal(s_e[:, 2 * r:2 * r + 2], s_a)
+        assert np.array_equal(m_e[:, 2 * r:2 * r + 2], m_a)
+        assert np.array_equal(bold_e[r:r + 1], net.get_bold("bold"))
+
+
+def test_set_bold_state_roundtrip():
+    e = synthetic.ensemble([synthetic.single_block(400, 10, gen_seed=5 + m) for m in range(3)])
+    net = Network.from_spec(e, device=0, build_push=False)
+    net.attach_bold(e.sub_to_region(), e.R)
+    net.run(10, mode="pull")
+    for f in ("s", "q", "v", "f_in"):
+        v = np.linspace(0.5, 1.5, e.R)
+        net.set_bold(f, v)
+        assert np.array_equal(net.get_bold(f), v)
