@@ -93,6 +93,8 @@ _SIGS = {
     "dtb_block_attach_bold": [c_vp, c_int, c_vp, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_f64],
     "dtb_block_get_bold": [c_vp, c_int, c_vp, c_int],
     "dtb_block_set_bold": [c_vp, c_int, c_vp, c_int],
+    "dtb_block_set_samples": [c_vp, c_int, c_vp, c_i64],
+    "dtb_block_get_samples": [c_vp, c_vp, c_vp, ctypes.POINTER(c_i64), c_int],
     "dtb_step_preallocated": [c_vp, c_f32, c_u64, c_f32, c_int, c_vp, c_vp, c_vp],
     "dtb_mlp_create": [c_int, c_int, c_u64, c_int, ctypes.POINTER(c_vp)],
     "dtb_mlp_destroy": [c_vp],

@@ -220,7 +220,7 @@ class SurrogateDA:
     """
 
     def __init__(self, template: synthetic.NetworkSpec, cfg: DAConfig, surrogate, n_judge: int = 16,
-                 threshold: float = 0.5, device: int = 0):
+                 threshold: float = 0.3, device: int = 0):
         from .network import BoldModel
         from .surrogate import HISTORY
         self.cfg = cfg
@@ -295,8 +295,8 @@ class SurrogateDA:
         # surrogate forecast of every member's window rate
         gui = hp.reshape(-1, self.n_hp)
         pred = self.sur.predict(gui, self.hist.reshape(-1, self.H)).reshape(self.M, self.R)
-        eps = 1e-6
-        err = torch.sqrt(torch.mean((torch.log(pred[:self.J] + eps) - torch.log(rates_j + eps)) ** 2)).item()
+        # judge score: symmetric relative error of the window rates (floor 1e-5 spikes/step ~ 0.1 Hz)
+        err = torch.mean(torch.abs(pred[:self.J] - rates_j) / (0.5 * (pred[:self.J] + rates_j) + 1e-5)).item()
         self.errors.append(err)
         sqvf = torch.stack([self.bold.get(k) for k in range(4)], dim=-1).reshape(self.M - self.J, self.R, 4)
         if err > self.threshold:

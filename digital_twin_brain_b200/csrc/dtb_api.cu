@@ -155,6 +155,8 @@ struct dtb_block {
     RunParams* h_run = nullptr;   // pinned
     // auto mode
     int64_t launches = 0;
+    uint64_t samples_from = 0;    // step at which sampling started
+    int64_t samples_written = 0;
     double last_frac = -1.0;
     double pull_threshold = 0.05;
     int chunk = 32;
@@ -485,10 +487,16 @@ static int rebuild_groups(dtb_block* b, const int32_t* sub_to_region)
 
 static int launch_stats(dtb_block* b, const DevState& s)
 {
-    if (!s.stats_ext || s.n_groups <= 0) return DTB_OK;
-    k_stats<<<grid_for(s.n_groups, 256), 256, 0, b->stream>>>(s);
-    CK(cudaGetLastError());
-    b->launches++;
+    if (s.stats_ext && s.n_groups > 0) {
+        k_stats<<<grid_for(s.n_groups, 256), 256, 0, b->stream>>>(s);
+        CK(cudaGetLastError());
+        b->launches++;
+    }
+    if (s.n_samples > 0) {
+        k_samples<<<grid_for(s.n_samples, 256), 256, 0, b->stream>>>(s);
+        CK(cudaGetLastError());
+        b->launches++;
+    }
     return DTB_OK;
 }
 
@@ -1772,6 +1780,55 @@ int dtb_block_attach_bold(dtb_block* b, int n_regions, const int32_t* sub_to_reg
     b->bold_R = n_regions;
     RET(rebuild_groups(b, sub_to_region));
     for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+    return DTB_OK;
+}
+
+int dtb_block_set_samples(dtb_block* b, int n, const uint32_t* idx, int64_t capacity_steps)
+{
+    if (!b || n < 0 || (n > 0 && (!idx || capacity_steps < 1))) return fail(DTB_ERR_ARG, "bad argument");
+    DeviceGuard g(b->device);
+    DevState& s = b->ds;
+    s.n_samples = 0;
+    b->samples_written = 0;
+    if (n == 0) { drop_graphs(b); return DTB_OK; }
+    for (int i = 0; i < n; ++i)
+        if (idx[i] >= (uint64_t)b->N) return fail(DTB_ERR_ARG, "sample %d: neuron %u out of range", i, idx[i]);
+    uint32_t* di = nullptr; uint8_t* sp = nullptr; float* sv = nullptr;
+    RET(dalloc(b, &di, (size_t)n));
+    RET(dalloc(b, &sp, (size_t)n * (size_t)capacity_steps));
+    RET(dalloc(b, &sv, (size_t)n * (size_t)capacity_steps));
+    CK(cudaMemcpy(di, idx, sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    s.samples = di; s.samp_spk = sp; s.samp_v = sv; s.samp_cap = capacity_steps; s.n_samples = n;
+    b->samples_from = b->steps;
+    drop_graphs(b);
+    return DTB_OK;
+}
+
+int dtb_block_get_samples(dtb_block* b, uint8_t* spikes, float* v, int64_t* rows, int where)
+{
+    if (!b || !rows) return fail(DTB_ERR_ARG, "null argument");
+    const DevState& s = b->ds;
+    if (s.n_samples <= 0) { *rows = 0; return DTB_OK; }
+    DeviceGuard g(b->device);
+    const int64_t total = (int64_t)(b->steps - b->samples_from);
+    const int64_t nr = std::min<int64_t>(total, s.samp_cap);
+    *rows = nr;
+    if (nr <= 0) return DTB_OK;
+    // chronological order: the oldest kept row first
+    const int64_t first_step = (int64_t)b->steps - nr;
+    const int64_t r0 = first_step % s.samp_cap;
+    const int64_t n1 = std::min<int64_t>(nr, s.samp_cap - r0);
+    const cudaMemcpyKind k = where == DTB_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    const size_t ns = (size_t)s.n_samples;
+    if (spikes) {
+        CK(cudaMemcpyAsync(spikes, s.samp_spk + r0 * ns, n1 * ns, k, b->stream));
+        if (nr > n1) CK(cudaMemcpyAsync(spikes + n1 * ns, s.samp_spk, (nr - n1) * ns, k, b->stream));
+    }
+    if (v) {
+        CK(cudaMemcpyAsync(v, s.samp_v + r0 * ns, n1 * ns * 4, k, b->stream));
+        if (nr > n1) CK(cudaMemcpyAsync(v + n1 * ns, s.samp_v, (nr - n1) * ns * 4, k, b->stream));
+    }
+    CK(cudaStreamSynchronize(b->stream));
     return DTB_OK;
 }
 

@@ -108,6 +108,11 @@ struct DevState {
     const int32_t* grp_sub;     // subblocks of every group
     const int32_t* grp_region;  // [n_groups] BOLD region of the group or -1
     int n_groups;
+    const uint32_t* samples;    // sampled neurons (cuda/src/stage/sample.cpp:8)
+    int n_samples;
+    int64_t samp_cap;           // ring rows
+    uint8_t* samp_spk;          // [samp_cap][n_samples] spike (threshold crossing) of the step
+    float* samp_v;              // [samp_cap][n_samples] V after the step
     float* st_spk;              // [stats_cap][n_sub]
     float* st_mean;             // [stats_cap][n_sub]
     uint32_t* st_nact;          // [stats_cap]

@@ -233,6 +233,20 @@ __global__ void __launch_bounds__(256) k_stats(DevState s)
     if ((threadIdx.x & 31) == 0 && w && write) atomicAdd(s.st_nact + row, w);
 }
 
+// ------------------------------------------------------------ samples
+// cuda/src/stage/sample.cpp:8-26 / stat_result.cpp:283-305: spike and V of the
+// sampled neurons after the step just taken, into a ring of steps.
+__global__ void k_samples(DevState s)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n_samples) return;
+    const unsigned long long step = s.ctl->steps_done - 1ull;   // clock already advanced
+    const int64_t row = (int64_t)(step % (unsigned long long)s.samp_cap);
+    const uint32_t n = s.samples[i];
+    s.samp_spk[row * s.n_samples + i] = (uint8_t)((s.abits[n >> 5] >> (n & 31)) & 1u);
+    s.samp_v[row * s.n_samples + i] = s.V[n];
+}
+
 // ------------------------------------------------------------ step kernel
 // Persistent: the grid is sized to the resident CTAs, and every warp streams a
 // contiguous run of 128-neuron tiles (tiles_per_warp of them).  In a tile a

@@ -293,6 +293,22 @@ class Network:
             v = np.ascontiguousarray(value, np.float64)
             _lib.call("dtb_block_set_bold", self._h, idx, _ptr(v), DTB_HOST)
 
+    def set_samples(self, idx, capacity_steps: int):
+        """Record spike and V of neurons idx after every step (ring of capacity_steps rows)."""
+        idx = np.ascontiguousarray(idx, np.uint32)
+        self.n_samples = len(idx)
+        _lib.call("dtb_block_set_samples", self._h, len(idx), _ptr(idx) if len(idx) else None, int(capacity_steps))
+
+    def get_samples(self):
+        """(spikes [rows, n] uint8, V [rows, n] float32), oldest step first."""
+        n = getattr(self, "n_samples", 0)
+        rows = ctypes.c_int64()
+        _lib.call("dtb_block_get_samples", self._h, None, None, ctypes.byref(rows), DTB_HOST)
+        sp = np.empty((rows.value, n), np.uint8)
+        v = np.empty((rows.value, n), np.float32)
+        _lib.call("dtb_block_get_samples", self._h, _ptr(sp), _ptr(v), ctypes.byref(rows), DTB_HOST)
+        return sp, v
+
     def window_spikes(self) -> np.ndarray:
         """Spikes per subblock since the last clear_window_spikes() (uint64 [n_sub])."""
         out = np.empty(self.n_sub, np.uint64)

@@ -267,6 +267,15 @@ int dtb_block_update_conn_weight(dtb_block* b, int64_t n, const uint8_t* channel
 int dtb_block_save(dtb_block* b, const char* path);
 int dtb_block_load(dtb_block* b, const char* path);
 
+/* Sampled neurons (cuda/python/dist_blockwrapper_pytorch.py set_samples,
+ * cuda/src/stage/sample.cpp:8): after every step the spike (threshold
+ * crossing, noise excluded) and V of the n neurons idx[] are recorded in a
+ * device ring of capacity_steps rows.  n = 0 stops sampling. */
+int dtb_block_set_samples(dtb_block* b, int n, const uint32_t* idx, int64_t capacity_steps);
+/* The recorded rows in step order, oldest first (at most capacity_steps):
+ * spikes[rows][n] uint8, v[rows][n] float (either nullable), *rows = count. */
+int dtb_block_get_samples(dtb_block* b, uint8_t* spikes, float* v, int64_t* rows, int where);
+
 /* ---- BOLD (models/bold_model_pytorch.py) --------------------------------- */
 
 /* BOLD.__init__ (bold_model_pytorch.py:12-25). dtype: 0 float32, 1 float64.

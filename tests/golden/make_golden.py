@@ -217,8 +217,34 @@ def case_enkf(seed: int = 5):
     print("enkf: ok")
 
 
+def case_statistics(seed: int = 9):
+    """analysis/spike_statistics.py and analysis/getpsd.py on a random raster (matplotlib stubbed:
+    the module imports it at top level and it is not installed here)."""
+    import types
+    sys.modules.setdefault("matplotlib", types.ModuleType("matplotlib"))
+    sys.modules.setdefault("matplotlib.pyplot", types.ModuleType("matplotlib.pyplot"))
+    import numpy as _np
+    if not hasattr(_np, "int"):
+        _np.int = int      # analysis/getpsd.py:10 uses np.int, removed from numpy
+    from analysis import spike_statistics as S
+    from analysis import getpsd as G
+    rng = np.random.default_rng(seed)
+    p = rng.uniform(0.0005, 0.02, 60)
+    raster = (rng.random((5000, 60)) < p).astype(np.uint8)
+    f, pw = S.spike_psd(raster)
+    sig = rng.normal(0, 1, 6000)
+    gf, gp = G.get_psd(sig, fs=1000, resolution=0.5)
+    np.savez_compressed(os.path.join(HERE, "statistics_ref.npz"), raster=raster, rate=S.mean_firing_rate(raster),
+                        inst=S.instantaneous_rate(raster), cv=S.coefficient_of_variation(raster), psd_f=f, psd=pw,
+                        sig=sig, welch_f=gf, welch=gp)
+    print("statistics: ok")
+
+
 if __name__ == "__main__":
     torch.set_num_threads(8)
+    if "--statistics" in sys.argv:
+        case_statistics()
+        sys.exit(0)
     if "--enkf" in sys.argv:
         case_enkf()
         sys.exit(0)
