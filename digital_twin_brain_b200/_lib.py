@@ -20,7 +20,7 @@ MODE_AUTO, MODE_PUSH, MODE_PULL = 0, 1, 2
 MODES = {"auto": MODE_AUTO, "push": MODE_PUSH, "pull": MODE_PULL}
 
 FIELD_V, FIELD_J, FIELD_I_UI, FIELD_I_SYN, FIELD_T_LAST, FIELD_ACTIVE, FIELD_NEW_ACTIVE, FIELD_T, FIELD_STEP, \
-    FIELD_SUB_COUNT, FIELD_EVENTS, FIELD_WINDOW_SPIKES = range(12)
+    FIELD_SUB_COUNT, FIELD_EVENTS, FIELD_WINDOW_SPIKES, FIELD_G_FACTOR = range(13)
 
 TUNE_SCATTER_WORDS, TUNE_CHUNK, TUNE_PULL_THRESHOLD_PPM, TUNE_USE_GRAPHS, TUNE_STEP_VARIANT = range(5)
 
@@ -78,6 +78,8 @@ _SIGS = {
     "dtb_block_get_csr": [c_vp, c_int, c_vp, c_vp, c_vp, c_int],
     "dtb_block_update_property": [c_vp, c_vp, c_vp],
     "dtb_block_scale_property_by_subblock": [c_vp, c_int, c_vp, c_vp, c_vp],
+    "dtb_block_gamma_property_by_subblock": [c_vp, c_int, c_vp, c_vp, c_vp, c_vp],
+    "dtb_block_set_input_spikes": [c_vp, c_i64, c_vp, c_i64, c_vp],
     "dtb_block_update_conn_weight": [c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
     "dtb_block_save": [c_vp, c_char_p],
     "dtb_block_load": [c_vp, c_char_p],

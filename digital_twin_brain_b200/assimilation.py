@@ -207,6 +207,11 @@ class EnsembleDA:
         return dict(bold_pred=np.stack(bold_pred), hp_mean=np.stack(hp_mean), window_s=np.array(times))
 
 
+def judge_error(pred: torch.Tensor, rates: torch.Tensor) -> float:
+    """Symmetric relative error of window rates (floor 1e-5 spikes/step, ~0.1 Hz), the judges' score."""
+    return torch.mean(torch.abs(pred - rates) / (0.5 * (pred + rates) + 1e-5)).item()
+
+
 class SurrogateDA:
     """EnKF data assimilation whose forecast comes from the surrogate for most members.
 
@@ -214,7 +219,8 @@ class SurrogateDA:
     surrogate predicts every member's window rate from its g_ui factors and
     rate history, the surrogate members' hemodynamics are integrated from
     that rate (dtb_bold_run_steps), and the judges score the surrogate on
-    their simulated rates: when the log-rate RMS error exceeds `threshold`,
+    their simulated rates: when their symmetric relative error exceeds `threshold`
+    (calibrate it on held-out windows: a margin over the surrogate's validated error),
     the window is recomputed for the surrogate members on the simulator
     (fallback).  The analysis step is the same diffusion EnKF over all members.
     """
@@ -296,7 +302,7 @@ class SurrogateDA:
         gui = hp.reshape(-1, self.n_hp)
         pred = self.sur.predict(gui, self.hist.reshape(-1, self.H)).reshape(self.M, self.R)
         # judge score: symmetric relative error of the window rates (floor 1e-5 spikes/step ~ 0.1 Hz)
-        err = torch.mean(torch.abs(pred[:self.J] - rates_j) / (0.5 * (pred[:self.J] + rates_j) + 1e-5)).item()
+        err = judge_error(pred[:self.J], rates_j)
         self.errors.append(err)
         sqvf = torch.stack([self.bold.get(k) for k in range(4)], dim=-1).reshape(self.M - self.J, self.R, 4)
         if err > self.threshold:

@@ -168,6 +168,9 @@ struct dtb_block {
     bool use_graphs = true;
     // attached BOLD
     int bold_R = 0;
+    // gamma-distributed g_ui (per-neuron factors; ds.gnrn points here while active)
+    float4* d_gnrn = nullptr;
+    uint32_t gamma_calls = 0;
 };
 
 struct dtb_bold {
@@ -541,9 +544,34 @@ static void launch_step(dtb_block* b, const DevState& s)
     else launch_step_m<G, U, F, 2>(b, s);
 }
 
+// models/block.py:104-109 reads column iter + 1 of src after replaying column
+// iter, so a raster of T columns serves T - 1 steps (an IndexError after that).
+static int check_src_steps(dtb_block* b, int64_t n)
+{
+    const DevState& s = b->ds;
+    if (s.n_src <= 0) return DTB_OK;
+    if ((int64_t)(b->steps - s.src_from) + n > s.src_T - 1)
+        return fail(DTB_ERR_ARG, "input spike raster exhausted: %lld columns serve %lld steps, %lld taken, %lld asked",
+                    (long long)s.src_T, (long long)(s.src_T - 1), (long long)(b->steps - s.src_from), (long long)n);
+    return DTB_OK;
+}
+
+static int launch_src(dtb_block* b, const DevState& s)
+{
+    CK(cudaMemsetAsync(s.src_val, 0, sizeof(uint32_t) * (size_t)s.n_words, b->stream));
+    k_src_bits<<<grid_for(s.n_src, 256), 256, 0, b->stream>>>(s);
+    CK(cudaGetLastError());
+    b->launches++;
+    return DTB_OK;
+}
+
 static int launch_update(dtb_block* b, const DevState& s, bool gather, bool forced)
 {
     if (s.N <= 0) return DTB_OK;
+    if (s.n_src > 0 && s.forced_active == s.src_val) {   // input neurons replay their raster
+        RET(launch_src(b, s));
+        forced = true;
+    }
     if (forced) {
         if (gather) launch_step<true, true, true>(b, s);
         else launch_step<false, true, true>(b, s);
@@ -1089,6 +1117,7 @@ int dtb_block_run(dtb_block* b, int n_steps, float noise_rate, int isolated, int
     if (mode < DTB_MODE_AUTO || mode > DTB_MODE_PULL) return fail(DTB_ERR_ARG, "bad mode %d", mode);
     if (where != DTB_HOST && where != DTB_DEVICE) return fail(DTB_ERR_ARG, "bad where");
     if (!b->has_pull && !b->has_push) return fail(DTB_ERR_STATE, "network has no synapse tables");
+    RET(check_src_steps(b, n_steps));
     DeviceGuard g(b->device);
     b->override_pending = false;
     int64_t done = 0;
@@ -1115,6 +1144,7 @@ int dtb_block_run(dtb_block* b, int n_steps, float noise_rate, int isolated, int
 int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isolated, int mode, float* out_ms)
 {
     if (!b || !out_ms || n_steps <= 0) return fail(DTB_ERR_ARG, "bad argument");
+    RET(check_src_steps(b, n_steps));
     DeviceGuard g(b->device);
     const int m = choose_mode(b, mode);
     RET(ensure_stats(b, (uint32_t)n_steps));
@@ -1276,8 +1306,10 @@ int dtb_block_step_forced(dtb_block* b, float noise_rate, int isolated, int mode
         k_u8_to_bits<<<grid_for(s.n_words, 256), 256, 0, b->stream>>>(b->d_u8, b->N, b->d_forced[k], s.n_words);
         CK(cudaGetLastError());
     }
-    s.forced_active = forced_active ? b->d_forced[0] : nullptr;
+    s.forced_active = forced_active ? b->d_forced[0] : b->ds.forced_active;   // input neurons stay forced
+    s.forced_mask = forced_active ? nullptr : b->ds.forced_mask;
     s.forced_new = forced_new_active ? b->d_forced[1] : nullptr;
+    RET(check_src_steps(b, 1));
     RET(set_run_params(b, noise_rate, isolated));
     const int m = choose_mode(b, mode);
     RET(launch_update(b, s, false, true));
@@ -1342,6 +1374,9 @@ int dtb_block_get(dtb_block* b, int field, void* dst, int where)
     case DTB_FIELD_EVENTS: return copy_out(b, dst, &s.ctl->events, sizeof(unsigned long long), where);
     case DTB_FIELD_WINDOW_SPIKES:
         return copy_out(b, dst, s.win_spk, sizeof(unsigned long long) * (size_t)b->n_sub, where);
+    case DTB_FIELD_G_FACTOR:
+        if (!s.gnrn) return fail(DTB_ERR_STATE, "no gamma-distributed g_ui");
+        return copy_out(b, dst, s.gnrn, sizeof(float4) * N, where);
     case DTB_FIELD_SUB_COUNT:
         if (where == DTB_HOST) { if (b->n_sub) std::memcpy(dst, b->sub_count.data(), sizeof(uint32_t) * b->n_sub); return DTB_OK; }
         return copy_out(b, dst, s.sub_count, sizeof(uint32_t) * b->n_sub, where);
@@ -1419,8 +1454,34 @@ int dtb_block_update_property(dtb_block* b, const float* property, const float* 
     if (!s.st_spk) RET(ensure_stats(b, 256));
     if (b->bold_R == 0) RET(rebuild_groups(b, nullptr));
     b->class_prop_base.clear();
+    s.gnrn = nullptr;   // the new matrix holds every neuron's g_ui: gamma factors no longer apply
     for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
     b->override_pending = true;
+    return DTB_OK;
+}
+
+// Re-derives the device parameters of every dirty class from its current row
+// (decay again from tau when a tau column moved) and uploads the table.
+static int rebuild_dirty_classes(dtb_block* b, const std::vector<char>& dirty,
+                                 const std::vector<char>* tau_set = nullptr)
+{
+    for (int c = 0; c < b->n_classes; ++c) {
+        if (!dirty[(size_t)c]) continue;
+        auto& row = b->class_prop[(size_t)c];
+        float dc[4] = {b->class_decay[(size_t)c][0], b->class_decay[(size_t)c][1], b->class_decay[(size_t)c][2],
+                       b->class_decay[(size_t)c][3]};
+        bool tau_changed = false;
+        for (int k = 18; k < 22; ++k) tau_changed |= row[(size_t)k] != b->class_prop_base[(size_t)c][(size_t)k];
+        if (tau_set) tau_changed |= (*tau_set)[(size_t)c] != 0;
+        if (tau_changed) { default_decay(row.data(), b->dt, dc); b->class_decay[(size_t)c] = {dc[0], dc[1], dc[2], dc[3]}; }
+        ParamClass p = make_class(row.data(), dc, b->dt);
+        p.sub = b->classes[(size_t)c].sub;
+        p.member = b->classes[(size_t)c].member;
+        b->classes[(size_t)c] = p;
+    }
+    CK(cudaMemcpyAsync(const_cast<ParamClass*>(b->ds.pc), b->classes.data(), sizeof(ParamClass) * b->classes.size(),
+                       cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
     return DTB_OK;
 }
 
@@ -1446,22 +1507,120 @@ int dtb_block_scale_property_by_subblock(dtb_block* b, int n, const int32_t* sub
             dirty[(size_t)c] = 1;
         }
     }
-    for (int c = 0; c < b->n_classes; ++c) {
-        if (!dirty[(size_t)c]) continue;
-        auto& row = b->class_prop[(size_t)c];
-        float dc[4] = {b->class_decay[(size_t)c][0], b->class_decay[(size_t)c][1], b->class_decay[(size_t)c][2],
-                       b->class_decay[(size_t)c][3]};
-        bool tau_changed = false;
-        for (int k = 18; k < 22; ++k) tau_changed |= row[(size_t)k] != b->class_prop_base[(size_t)c][(size_t)k];
-        if (tau_changed) { default_decay(row.data(), b->dt, dc); b->class_decay[(size_t)c] = {dc[0], dc[1], dc[2], dc[3]}; }
-        ParamClass p = make_class(row.data(), dc, b->dt);
-        p.sub = b->classes[(size_t)c].sub;
-        p.member = b->classes[(size_t)c].member;
-        b->classes[(size_t)c] = p;
+    return rebuild_dirty_classes(b, dirty);
+}
+
+int dtb_block_gamma_property_by_subblock(dtb_block* b, int n, const int32_t* sub, const int32_t* col,
+                                         const float* alpha, const float* beta)
+{
+    if (!b || n < 0 || (n > 0 && (!sub || !col || !alpha || !beta))) return fail(DTB_ERR_ARG, "bad argument");
+    if (n == 0) return DTB_OK;
+    for (int i = 0; i < n; ++i) {
+        if (!(alpha[i] >= 0.0f) || !(beta[i] > 0.0f)) return fail(DTB_ERR_ARG, "request %d: need alpha >= 0, beta > 0", i);
+        const bool g_col = col[i] >= 10 && col[i] < 14;
+        const bool delta = alpha[i] >= 1e6f;   // relative spread 1/sqrt(alpha) <= 1e-3
+        if (col[i] < 0 || col[i] >= DTB_NPROP || col[i] == 1 || col[i] == 3)
+            return fail(DTB_ERR_ARG, "column %d cannot be gamma-distributed", col[i]);
+        if (!g_col && !delta)
+            return fail(DTB_ERR_ARG, "column %d: per-neuron values are kept for g_ui (columns 10-13) only; "
+                        "other columns take the delta limit (alpha >= 1e6)", col[i]);
     }
-    CK(cudaMemcpyAsync(const_cast<ParamClass*>(b->ds.pc), b->classes.data(), sizeof(ParamClass) * b->classes.size(),
-                       cudaMemcpyHostToDevice, b->stream));
-    CK(cudaStreamSynchronize(b->stream));
+    DeviceGuard g(b->device);
+    if (b->class_prop_base.empty()) b->class_prop_base = b->class_prop;
+    std::unordered_map<int32_t, std::vector<int32_t>> by_sub;
+    for (int c = 0; c < b->n_classes; ++c) by_sub[b->classes[(size_t)c].sub].push_back(c);
+    std::vector<char> dirty((size_t)b->n_classes, 0), tau_set((size_t)b->n_classes, 0);
+    std::vector<int32_t> req((size_t)std::max(1, b->n_sub) * 4, -1);
+    std::vector<double> ha, hb;
+    bool any_g = false;
+    for (int i = 0; i < n; ++i) {
+        auto it = by_sub.find(sub[i]);
+        if (it == by_sub.end()) continue;
+        const bool g_col = col[i] >= 10 && col[i] < 14;
+        // the sampled values become the base that later subblock scalings multiply
+        const float v = g_col ? 1.0f : (float)((double)alpha[i] / (double)beta[i]);
+        for (int32_t c : it->second) {
+            b->class_prop[(size_t)c][(size_t)col[i]] = v;
+            b->class_prop_base[(size_t)c][(size_t)col[i]] = v;
+            dirty[(size_t)c] = 1;
+            if (col[i] >= 18) tau_set[(size_t)c] = 1;
+        }
+        if (g_col && sub[i] >= 0 && sub[i] < b->n_sub) {
+            req[(size_t)sub[i] * 4 + (size_t)(col[i] - 10)] = (int32_t)ha.size();
+            ha.push_back(alpha[i]);
+            hb.push_back(beta[i]);
+            any_g = true;
+        }
+    }
+    if (any_g) {
+        if (!b->d_gnrn) {
+            RET(dalloc(b, &b->d_gnrn, (size_t)std::max<int64_t>(b->N, 1)));
+            k_fill4<<<grid_for(b->N, 256), 256, 0, b->stream>>>(b->d_gnrn, b->N, make_float4(1.f, 1.f, 1.f, 1.f));
+            CK(cudaGetLastError());
+        }
+        if (!b->ds.gnrn) {   // re-activated after update_property: start again from factor 1
+            k_fill4<<<grid_for(b->N, 256), 256, 0, b->stream>>>(b->d_gnrn, b->N, make_float4(1.f, 1.f, 1.f, 1.f));
+            CK(cudaGetLastError());
+        }
+        int32_t* dreq = nullptr; double* da = nullptr; double* db = nullptr;
+        cudaError_t e = cudaMalloc(&dreq, sizeof(int32_t) * req.size());
+        if (e == cudaSuccess) e = cudaMalloc(&da, sizeof(double) * ha.size());
+        if (e == cudaSuccess) e = cudaMalloc(&db, sizeof(double) * hb.size());
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dreq, req.data(), sizeof(int32_t) * req.size(), cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(da, ha.data(), sizeof(double) * ha.size(), cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(db, hb.data(), sizeof(double) * hb.size(), cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess) {
+            b->ds.gnrn = b->d_gnrn;
+            k_gamma<<<grid_for(b->N, 256), 256, 0, b->stream>>>(b->ds, dreq, da, db, b->gamma_calls, b->d_gnrn);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        cudaFree(dreq); cudaFree(da); cudaFree(db);
+        if (e != cudaSuccess) return fail(DTB_ERR_CUDA, "gamma sampling: %s", cudaGetErrorString(e));
+        b->gamma_calls++;
+        drop_graphs(b);   // graphs hold the state by value
+    }
+    return rebuild_dirty_classes(b, dirty, &tau_set);
+}
+
+int dtb_block_set_input_spikes(dtb_block* b, int64_t n_src, const uint32_t* neurons, int64_t T, const uint8_t* spikes)
+{
+    if (!b || n_src < 0 || (n_src > 0 && (!neurons || !spikes || T < 1))) return fail(DTB_ERR_ARG, "bad argument");
+    DeviceGuard g(b->device);
+    DevState& s = b->ds;
+    if (n_src == 0) {
+        s.n_src = 0;
+        s.forced_active = nullptr;
+        s.forced_mask = nullptr;
+        drop_graphs(b);
+        return DTB_OK;
+    }
+    std::vector<uint32_t> mask((size_t)s.n_words, 0u);
+    for (int64_t i = 0; i < n_src; ++i) {
+        if (neurons[i] >= (uint64_t)b->N) return fail(DTB_ERR_ARG, "input %lld: neuron %u out of range", (long long)i, neurons[i]);
+        uint32_t& w = mask[neurons[i] >> 5];
+        if (w & (1u << (neurons[i] & 31))) return fail(DTB_ERR_ARG, "input neuron %u given twice", neurons[i]);
+        w |= 1u << (neurons[i] & 31);
+    }
+    const int64_t words = (n_src + 31) / 32;
+    std::vector<uint32_t> raster((size_t)(T * words), 0u);   // [T][words], from [n_src][T] bytes
+    for (int64_t i = 0; i < n_src; ++i)
+        for (int64_t t = 0; t < T; ++t)
+            if (spikes[i * T + t]) raster[(size_t)(t * words + (i >> 5))] |= 1u << (i & 31);
+    uint32_t *dn = nullptr, *dr = nullptr, *dm = nullptr, *dv = nullptr;
+    RET(dalloc(b, &dn, (size_t)n_src));
+    RET(dalloc(b, &dr, raster.size()));
+    RET(dalloc(b, &dm, (size_t)s.n_words));
+    RET(dalloc(b, &dv, (size_t)s.n_words));
+    CK(cudaMemcpy(dn, neurons, sizeof(uint32_t) * (size_t)n_src, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dr, raster.data(), sizeof(uint32_t) * raster.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dm, mask.data(), sizeof(uint32_t) * mask.size(), cudaMemcpyHostToDevice));
+    s.n_src = n_src; s.src_neuron = dn; s.src_raster = dr; s.src_words = words; s.src_T = T;
+    s.src_from = b->steps;
+    s.src_val = dv;
+    s.forced_active = dv;
+    s.forced_mask = dm;
+    drop_graphs(b);
     return DTB_OK;
 }
 

@@ -86,11 +86,21 @@ struct DevState {
     float* isyn_override;       // [N] used once after update_property
     const uint32_t* cls;
     const ParamClass* pc;
+    const float4* gnrn;         // [N] per-neuron factors of g_ui (gamma-distributed properties; nullable)
     const int64_t* member_start;  // [M] first neuron of every ensemble member (nullable)
     uint32_t* bits[2];          // new_active bitmask by step parity
     uint32_t* abits;            // active bitmask of the latest update
     const uint32_t* forced_active;   // teacher forcing bitmasks (nullable)
     const uint32_t* forced_new;
+    const uint32_t* forced_mask;     // neurons forced_active applies to (nullable: every neuron)
+    // input neurons (models/block.py:37-50, :104-109): their spikes replay a raster
+    int64_t n_src;
+    const uint32_t* src_neuron;      // [n_src]
+    const uint32_t* src_raster;      // [T][src_words] bits by input ordinal
+    int64_t src_words;
+    int64_t src_T;
+    unsigned long long src_from;     // step at which column 0 is replayed
+    uint32_t* src_val;               // [n_words] this step's input spikes (forced_active while inputs are set)
     // pull CSR
     const int64_t* prow; const uint32_t* pcol; const float2* pw;
     // push CSR

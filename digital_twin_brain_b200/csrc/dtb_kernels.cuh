@@ -24,22 +24,24 @@ namespace dtb {
 // Operation order of models/block.py:83-111 with round-to-nearest float32
 // intrinsics so that no multiply-add is contracted.
 
-__device__ __forceinline__ float isyn_of(const ParamClass& p, float v, float4 J)
+__device__ __forceinline__ float isyn_g(float4 g, float4 Vu, float v, float4 J)
 {
-    const float i0 = __fmul_rn(__fmul_rn(p.g.x, __fsub_rn(p.Vu.x, v)), J.x);
-    const float i1 = __fmul_rn(__fmul_rn(p.g.y, __fsub_rn(p.Vu.y, v)), J.y);
-    const float i2 = __fmul_rn(__fmul_rn(p.g.z, __fsub_rn(p.Vu.z, v)), J.z);
-    const float i3 = __fmul_rn(__fmul_rn(p.g.w, __fsub_rn(p.Vu.w, v)), J.w);
+    const float i0 = __fmul_rn(__fmul_rn(g.x, __fsub_rn(Vu.x, v)), J.x);
+    const float i1 = __fmul_rn(__fmul_rn(g.y, __fsub_rn(Vu.y, v)), J.y);
+    const float i2 = __fmul_rn(__fmul_rn(g.z, __fsub_rn(Vu.z, v)), J.z);
+    const float i3 = __fmul_rn(__fmul_rn(g.w, __fsub_rn(Vu.w, v)), J.w);
     return __fadd_rn(__fadd_rn(__fadd_rn(i0, i1), i2), i3);
 }
 
-__device__ __forceinline__ float4 iui_of(const ParamClass& p, float v, float4 J)
+__device__ __forceinline__ float4 iui_g(float4 g, float4 Vu, float v, float4 J)
 {
-    return make_float4(__fmul_rn(__fmul_rn(p.g.x, __fsub_rn(p.Vu.x, v)), J.x),
-                       __fmul_rn(__fmul_rn(p.g.y, __fsub_rn(p.Vu.y, v)), J.y),
-                       __fmul_rn(__fmul_rn(p.g.z, __fsub_rn(p.Vu.z, v)), J.z),
-                       __fmul_rn(__fmul_rn(p.g.w, __fsub_rn(p.Vu.w, v)), J.w));
+    return make_float4(__fmul_rn(__fmul_rn(g.x, __fsub_rn(Vu.x, v)), J.x),
+                       __fmul_rn(__fmul_rn(g.y, __fsub_rn(Vu.y, v)), J.y),
+                       __fmul_rn(__fmul_rn(g.z, __fsub_rn(Vu.z, v)), J.z),
+                       __fmul_rn(__fmul_rn(g.w, __fsub_rn(Vu.w, v)), J.w));
 }
+
+__device__ __forceinline__ float isyn_of(const ParamClass& p, float v, float4 J) { return isyn_g(p.g, p.Vu, v, J); }
 
 __device__ __forceinline__ ParamClass load_class(const ParamClass* __restrict__ pc, uint32_t c)
 {
@@ -374,7 +376,10 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             const int64_t n = base + j * 32 + lane;
             const float v = v_in[j];
             const float4 J = GATHER ? Jn[j] : J_in[j];
-            const float isyn = use_override ? s.isyn_override[n] : isyn_of(p, v, J);
+            float isyn;
+            if (use_override) isyn = s.isyn_override[n];
+            else if (s.gnrn) isyn = isyn_g(mul4(p.g, __ldcs(s.gnrn + n)), p.Vu, v, J);   // gamma-distributed g_ui
+            else isyn = isyn_of(p, v, J);
             const float mainp = __fmul_rn(-p.gL, __fsub_rn(v, p.VL));
             const float cd = __fadd_rn(__fadd_rn(mainp, isyn), p.Iext);
             const float vn = __fadd_rn(v, __fmul_rn(p.rCdt, cd));
@@ -382,7 +387,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             const float vs = notsat ? vn : p.Vreset;
             bool a = vs >= p.Vth;
             const float vmin = isnan(vs) ? vs : (isnan(p.Vth) ? p.Vth : (vs < p.Vth ? vs : p.Vth));
-            if (FORCED && s.forced_active) a = (__ldg(s.forced_active + (n >> 5)) >> (n & 31)) & 1u;
+            if (FORCED && s.forced_active && (!s.forced_mask || ((__ldg(s.forced_mask + (n >> 5)) >> (n & 31)) & 1u)))
+                a = (__ldg(s.forced_active + (n >> 5)) >> (n & 31)) & 1u;
             const float rate = noise_rate >= 0.0f ? noise_rate : p.noise;
             const bool nz = u01(words[j]) < rate;
             bool na = isolated ? nz : (nz || a);
@@ -610,11 +616,12 @@ __global__ void k_export_current(const DevState s, float* __restrict__ iui, floa
     const ParamClass p = load_class(s.pc, s.cls[n]);
     const float v = s.V[n];
     const float4 J = load_J(s, n);
+    const float4 g = s.gnrn ? mul4(p.g, s.gnrn[n]) : p.g;
     if (iui) {
-        const float4 i = iui_of(p, v, J);
+        const float4 i = iui_g(g, p.Vu, v, J);
         iui[n] = i.x; iui[s.N + n] = i.y; iui[2 * s.N + n] = i.z; iui[3 * s.N + n] = i.w;
     }
-    if (isyn) isyn[n] = isyn_of(p, v, J);
+    if (isyn) isyn[n] = isyn_g(g, p.Vu, v, J);
 }
 
 __global__ void k_bits_to_u8(const uint32_t* __restrict__ bits, int64_t N, uint8_t* __restrict__ out)
@@ -634,6 +641,21 @@ __global__ void k_u8_to_bits(const uint8_t* __restrict__ in, int64_t N, uint32_t
         if (n < N && in[n]) w |= (1u << b);
     }
     bits[wi] = w;
+}
+
+// This step's input spikes: column (steps_done - src_from) of the raster, as
+// bits of the input neurons in src_val (cleared beforehand).
+__global__ void k_src_bits(const DevState s)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.n_src) return;
+    const unsigned long long col = s.ctl->steps_done - s.src_from;
+    if (col >= (unsigned long long)s.src_T) return;   // the host refuses runs past the raster
+    const uint32_t w = __ldg(s.src_raster + (int64_t)col * s.src_words + (i >> 5));
+    if ((w >> (i & 31)) & 1u) {
+        const uint32_t n = s.src_neuron[i];
+        atomicOr(s.src_val + (n >> 5), 1u << (n & 31));
+    }
 }
 
 __global__ void k_J_from_planar(DevState s, const float* __restrict__ in)
@@ -1025,6 +1047,77 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_push_rows(int64_t N, c
         qcol[e0 + k] = (uint32_t)(kk >> 32) | (uint32_t)(kk & kKindBit);
         qw[e0 + k] = wtmp[(int)(kk & 0x7fffffffull)];
     }
+}
+
+// ------------------------------------------------------------ gamma-distributed properties
+// cuda/src/stage/property.cpp:313-471 (gamma_kernel / sample_gamma): every
+// neuron of a subblock draws its own value Gamma(alpha, 1) / beta.  Method of
+// Marsaglia & Tsang, "A simple method for generating gamma variables", ACM
+// TOMS 26(3), 2000 (squeeze test, then the log test; alpha < 1 through
+// G(alpha) = G(alpha + 1) U^(1/alpha)).  Normals by the Box-Muller transform
+// (Box & Muller 1958).  All arithmetic in double; uniforms from Philox4x32-10
+// with counter {n_lo, n_hi, attempt, tag} and key {seed_lo, seed_hi ^ 'GAMM'}
+// (tag = 0x80000000 | receptor << 24 | call number), 64 attempts at most (the
+// acceptance rate is above 95 % per attempt), after which the mode d is used.
+constexpr uint32_t kGammaKeyXor = 0x47414D4Du;
+
+__host__ __device__ inline double gamma_u24(uint32_t x, int open_zero)
+{
+    return ((double)(x >> 8) + (open_zero ? 1.0 : 0.0)) * (1.0 / 16777216.0);
+}
+
+__device__ inline double gamma_unit(double alpha, uint64_t seed, uint64_t n, uint32_t tag)
+{
+    if (!(alpha > 0.0)) return 0.0;
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kGammaKeyXor;
+    double scale = 1.0;
+    if (alpha < 1.0) {
+        const U4 r = philox4x32_10(U4{(uint32_t)n, (uint32_t)(n >> 32), 0xffffffffu, tag}, k0, k1);
+        scale = pow(gamma_u24(r.x, 1), 1.0 / alpha);
+        alpha += 1.0;
+    }
+    const double d = alpha - 1.0 / 3.0;
+    const double c = 1.0 / sqrt(9.0 * d);
+    for (uint32_t it = 0; it < 64u; ++it) {
+        const U4 r = philox4x32_10(U4{(uint32_t)n, (uint32_t)(n >> 32), it, tag}, k0, k1);
+        const double u1 = gamma_u24(r.x, 1), u2 = gamma_u24(r.y, 0);
+        const double x = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+        const double y = 1.0 + c * x;
+        if (y <= 0.0) continue;
+        const double v = y * y * y;
+        const double u = gamma_u24(r.z, 1);
+        const double xx = x * x;
+        if (u < 1.0 - 0.0331 * xx * xx) return scale * d * v;
+        if (log(u) < 0.5 * xx + d * (1.0 - v + log(v))) return scale * d * v;
+    }
+    return scale * d;
+}
+
+// req[sub * 4 + u] = request index for receptor u of subblock sub, or -1.
+__global__ void k_gamma(const DevState s, const int32_t* __restrict__ req, const double* __restrict__ alpha,
+                        const double* __restrict__ beta, uint32_t call, float4* __restrict__ g)
+{
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= s.N) return;
+    const int sub = s.pc[s.cls[n]].sub;
+    if (sub < 0 || sub >= s.n_sub) return;
+    float4 v = g[n];
+    float* vp = reinterpret_cast<float*>(&v);
+    bool any = false;
+    for (int u = 0; u < 4; ++u) {
+        const int r = req[(int64_t)sub * 4 + u];
+        if (r < 0) continue;
+        const uint32_t tag = 0x80000000u | ((uint32_t)u << 24) | (call & 0x00ffffffu);
+        vp[u] = (float)(gamma_unit(alpha[r], s.seed, (uint64_t)n, tag) / beta[r]);
+        any = true;
+    }
+    if (any) g[n] = v;
+}
+
+__global__ void k_fill4(float4* p, int64_t n, float4 val)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = val;
 }
 
 }  // namespace dtb

@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from . import synthetic
-from .assimilation import DAConfig, EnsembleDA, SurrogateDA, collect_windows, log_torch
+from .assimilation import DAConfig, EnsembleDA, SurrogateDA, collect_windows, judge_error, log_torch
 from .surrogate import RateSurrogate
 
 
@@ -43,7 +43,9 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--train-sigma", type=float, default=1.0,
                     help="random-walk variance of the training ensemble (wider than the DA walk for coverage)")
-    ap.add_argument("--threshold", type=float, default=0.3)
+    ap.add_argument("--threshold", type=float, default=None,
+                    help="judge fallback threshold (default: --margin x the held-out judge error of the surrogate)")
+    ap.add_argument("--margin", type=float, default=1.5)
     ap.add_argument("--gain", type=float, default=2.0,
                     help="excitatory g_ui of the template as a multiple of the single-block values (2.0: ~6 Hz)")
     ap.add_argument("--skip", type=int, default=5, help="windows excluded from the RMSE (spin-up)")
@@ -112,13 +114,16 @@ def main(argv=None):
     eps = 1e-6
     lerr_net = float(torch.sqrt(torch.mean((torch.log(pred + eps) - torch.log(tgt[te] + eps)) ** 2)))
     lerr_persist = float(torch.sqrt(torch.mean((torch.log(h[te][:, -1] + eps) - torch.log(tgt[te] + eps)) ** 2)))
+    val_err = judge_error(pred, tgt[te])
+    threshold = a.threshold if a.threshold is not None else a.margin * val_err
+    out.update(heldout_judge_err=val_err, threshold=threshold)
     out.update(train_samples=int(n), train_windows=a.train_windows, train_sigma=a.train_sigma, train_collect_s=t_collect, train_s=t_train,
                train_loss_first=hist[0], train_loss_last=hist[-1], heldout_logrmse_net=lerr_net,
                heldout_logrmse_persistence=lerr_persist)
 
     # ---- surrogate-served DA
     sda = SurrogateDA(template, DAConfig(n_members=a.members, **base), sur, n_judge=a.judges,
-                      threshold=a.threshold)
+                      threshold=threshold)
     res_s = sda.run(obs)
     out.update(summarize(res_s, "surrogate"))
     out.update(fallbacks=int(res_s["fallbacks"]), judge_rel_err_mean=float(np.mean(res_s["errors"])))

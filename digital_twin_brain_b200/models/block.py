@@ -17,8 +17,10 @@ Differences from the reference, by design:
   and agree to float32 rounding.
 * A dense ``w_uij`` is accepted and converted to its nonzero entries; dense
   ``torch.matmul`` summation order is not reproduced (rounding-level match).
-* ``src`` (replayed input spike trains, models/block.py:37-50,104-109) is not
-  supported yet and raises NotImplementedError.
+* ``src`` (input neurons replaying a spike raster, models/block.py:37-50,
+  104-109) is held on the device; as in the reference, the input neurons are
+  those without incoming synapses, a raster of T columns serves T - 1 steps
+  and the step after that raises IndexError.
 """
 from __future__ import annotations
 
@@ -86,9 +88,7 @@ class block:
         K = w_uij.shape[0]
         assert K == 4, "w_uij must have 4 channels (AMPA, NMDA, GABAa, GABAb)"
         assert node_property.shape[0] == N and node_property.shape[1] == 22
-        if src is not None:
-            raise NotImplementedError("input (src) neurons are not supported by the GPU block yet")
-        self.src = None
+        self.src = src
         self.src_neuron = None
         self.iter = None
         self.delta_t = delta_t
@@ -101,6 +101,13 @@ class block:
         self._net = Network.from_arrays(prop, post, pre, kind, w, dt=float(delta_t), seed=seed,
                                         decay=decay_of(node_property, delta_t), device=device,
                                         build_push=build_push)
+        if src is not None:
+            # neurons without any incoming entry (models/block.py:41-47)
+            idx = np.setdiff1d(np.arange(N, dtype=np.int64), np.unique(post))
+            self.src_neuron = torch.from_numpy(idx)
+            assert self.src_neuron.shape[0] == src.shape[0]
+            self.iter = 0
+            self._net.set_input_spikes(idx, torch.as_tensor(src).cpu().numpy().astype(np.uint8))
         self._set_property_views(node_property)
 
     def _set_property_views(self, node_property):
@@ -121,13 +128,24 @@ class block:
         return torch.from_numpy(a).to(self._out_device)
 
     # ---------------------------------------------------------------- step
+    def _take_src(self, n: int):
+        if self.src is None:
+            return
+        if self.iter + n >= self.src.shape[1]:
+            # models/block.py:107 reads src[:, iter + 1] after replaying column iter
+            raise IndexError(f"index {self.src.shape[1]} is out of bounds for dimension 1 with size "
+                             f"{self.src.shape[1]}")
+        self.iter += n
+
     def run(self, noise_rate=0.01, isolated=False):
         """One time step (models/block.py:116-150): (spike sum, mean V) per subblock."""
+        self._take_src(1)
         s, m, _ = self._net.run(1, noise_rate=noise_rate, isolated=isolated, mode=self.mode, out="host")
         return self._out(s[0]), self._out(m[0])
 
     def run_steps(self, n_steps: int, noise_rate=0.01, isolated=False):
         """n_steps calls of run() in one native call; per-step results stacked."""
+        self._take_src(n_steps)
         s, m, _ = self._net.run(n_steps, noise_rate=noise_rate, isolated=isolated, mode=self.mode, out="host")
         return self._out(s), self._out(m)
 

@@ -13,7 +13,8 @@ import torch
 
 from . import _lib
 from ._lib import (DTB_DEVICE, DTB_HOST, FIELD_ACTIVE, FIELD_EVENTS, FIELD_I_SYN, FIELD_I_UI, FIELD_J,
-                   FIELD_NEW_ACTIVE, FIELD_STEP, FIELD_SUB_COUNT, FIELD_T, FIELD_T_LAST, FIELD_V, FIELD_WINDOW_SPIKES,
+                   FIELD_G_FACTOR, FIELD_NEW_ACTIVE, FIELD_STEP, FIELD_SUB_COUNT, FIELD_T, FIELD_T_LAST, FIELD_V,
+                   FIELD_WINDOW_SPIKES,
                    MODES)
 from .synthetic import NetworkSpec
 
@@ -248,6 +249,32 @@ class Network:
         value = np.ascontiguousarray(value, np.float32)
         _lib.call("dtb_block_scale_property_by_subblock", self._h, len(sub), _ptr(sub), _ptr(col), _ptr(value))
 
+    def set_input_spikes(self, neurons, spikes):
+        """Input neurons replaying a raster spikes[i, t] (models/block.py:37-50, :104-109); T columns serve
+        T - 1 steps.  neurons=[] removes them."""
+        idx = np.ascontiguousarray(neurons, np.uint32)
+        if len(idx) == 0:
+            _lib.call("dtb_block_set_input_spikes", self._h, 0, None, 0, None)
+            return
+        sp = np.ascontiguousarray(spikes, np.uint8)
+        assert sp.ndim == 2 and sp.shape[0] == len(idx)
+        _lib.call("dtb_block_set_input_spikes", self._h, len(idx), _ptr(idx), sp.shape[1], _ptr(sp))
+
+    def gamma_property_by_subblock(self, sub, col, alpha, beta):
+        """Column col[i] of every neuron of subblock sub[i] <- Gamma(alpha[i], 1) / beta[i] per neuron
+        (cuda/src/stage/property.cpp:313-471); g_ui columns per neuron, others in the delta limit."""
+        sub = np.ascontiguousarray(sub, np.int32)
+        col = np.ascontiguousarray(col, np.int32)
+        a = np.ascontiguousarray(alpha, np.float32)
+        b = np.ascontiguousarray(beta, np.float32)
+        _lib.call("dtb_block_gamma_property_by_subblock", self._h, len(sub), _ptr(sub), _ptr(col), _ptr(a), _ptr(b))
+
+    def g_factors(self) -> np.ndarray:
+        """Per-neuron g_ui factors [N, 4] set by gamma_property_by_subblock."""
+        out = np.empty((self.N, 4), np.float32)
+        _lib.call("dtb_block_get", self._h, FIELD_G_FACTOR, _ptr(out), DTB_HOST)
+        return out
+
     def update_conn_weight(self, channel, post, pre, value):
         ch = np.ascontiguousarray(channel, np.uint8)
         po = np.ascontiguousarray(post, np.uint32)
@@ -299,14 +326,23 @@ class Network:
         self.n_samples = len(idx)
         _lib.call("dtb_block_set_samples", self._h, len(idx), _ptr(idx) if len(idx) else None, int(capacity_steps))
 
-    def get_samples(self):
-        """(spikes [rows, n] uint8, V [rows, n] float32), oldest step first."""
+    def get_samples(self, out: str = "host"):
+        """(spikes [rows, n] uint8, V [rows, n] float32), oldest step first; out 'host' (numpy) or 'device'
+        (torch CUDA tensors)."""
         n = getattr(self, "n_samples", 0)
         rows = ctypes.c_int64()
         _lib.call("dtb_block_get_samples", self._h, None, None, ctypes.byref(rows), DTB_HOST)
+        if out == "device":
+            dev = torch.device("cuda", self.device)
+            sp = torch.empty((rows.value, n), dtype=torch.uint8, device=dev)
+            v = torch.empty((rows.value, n), dtype=torch.float32, device=dev)
+            if rows.value and n:
+                _lib.call("dtb_block_get_samples", self._h, _ptr(sp), _ptr(v), ctypes.byref(rows), DTB_DEVICE)
+            return sp, v
         sp = np.empty((rows.value, n), np.uint8)
         v = np.empty((rows.value, n), np.float32)
-        _lib.call("dtb_block_get_samples", self._h, _ptr(sp), _ptr(v), ctypes.byref(rows), DTB_HOST)
+        if rows.value and n:
+            _lib.call("dtb_block_get_samples", self._h, _ptr(sp), _ptr(v), ctypes.byref(rows), DTB_HOST)
         return sp, v
 
     def window_spikes(self) -> np.ndarray:

@@ -59,8 +59,9 @@ typedef enum {
     DTB_FIELD_STEP = 8,       /* uint64[1]     steps taken (Philox step counter) */
     DTB_FIELD_SUB_COUNT = 9,  /* uint32[n_sub] neurons per subblock */
     DTB_FIELD_EVENTS = 10,    /* uint64[1]     synaptic events propagated since creation */
-    DTB_FIELD_WINDOW_SPIKES = 11 /* uint64[n_sub] spikes per subblock since last set (window totals,
+    DTB_FIELD_WINDOW_SPIKES = 11, /* uint64[n_sub] spikes per subblock since last set (window totals,
                                     simulation/simulation.py:269-279 freqs summed over a TR) */
+    DTB_FIELD_G_FACTOR = 12   /* float[N][4]  per-neuron g_ui factors after dtb_block_gamma_property_by_subblock */
 } dtb_field;
 
 typedef struct dtb_block dtb_block;
@@ -254,6 +255,29 @@ int dtb_block_update_property(dtb_block* b, const float* property, const float* 
  * sub[i] becomes base_value * value[i], base = the value at creation. */
 int dtb_block_scale_property_by_subblock(dtb_block* b, int n, const int32_t* sub, const int32_t* col,
                                          const float* value);
+
+/* cuda/src/stage/property.cpp:313-471 (gamma_kernel), cuda/src/block.cpp:815-855
+ * update_Gamma_Prop_Cols_gpu, client cuda/python/dist_blockwrapper_pytorch.py:460
+ * gamma_property_by_subblk: property column col[i] of every neuron of
+ * subblock sub[i] becomes its own draw of Gamma(alpha[i], 1) / beta[i].
+ * g_ui columns (10-13) keep one value per neuron (a per-neuron factor on the
+ * class value, which becomes 1); any other column takes the delta limit
+ * alpha/beta and needs alpha >= 1e6 (the reference's near-delta use,
+ * simulation/simulation.py:120-144).  The drawn values become the base of
+ * later dtb_block_scale_property_by_subblock calls.  Sampler: Marsaglia &
+ * Tsang (2000) on Philox4x32-10 in double precision; the stream is keyed by
+ * the block seed, the neuron and a per-block call counter. */
+int dtb_block_gamma_property_by_subblock(dtb_block* b, int n, const int32_t* sub, const int32_t* col,
+                                         const float* alpha, const float* beta);
+
+/* models/block.py:37-50, :104-109 (block with src): the n_src input neurons
+ * `neurons` replay a spike raster, spikes[i][t] (uint8, [n_src][T]) being the
+ * spike of input i at the t-th step from now; their other state evolves as
+ * usual (noise still ORs into what they propagate).  As in the reference, a
+ * raster of T columns serves T - 1 steps: running further fails.  n_src = 0
+ * removes the inputs. */
+int dtb_block_set_input_spikes(dtb_block* b, int64_t n_src, const uint32_t* neurons, int64_t T,
+                               const uint8_t* spikes);
 
 /* models/block.py:172-177 block.update_conn_weight: set the channel weight
  * of existing synapses (channel[i], post[i], pre[i]) to value[i]. */

@@ -109,7 +109,9 @@ void oracle_noise_uniforms(uint64_t seed, uint32_t stream, uint64_t step, int64_
  *
  * State in/out: V[N], J[4][N], tlast[N], Isyn[N], *t.
  * noise_rate >= 0: scalar rate (block.py:136); < 0: per-neuron rates.
- * forced_* (nullable): teacher forcing of this step's active / new_active.
+ * forced_* (nullable): teacher forcing of this step's active / new_active;
+ * a forced_active value of 2 keeps the computed spike of that neuron (input
+ * neurons replay their raster, the others run free: models/block.py:104-106).
  */
 int oracle_block_step(int64_t N,
                       const float* Iext, const float* C, const float* Tref,
@@ -148,7 +150,7 @@ int oracle_block_step(int64_t N,
         float vth = Vth[i];
         float vmin = isnan(vsel) ? vsel : (isnan(vth) ? vth : (vsel < vth ? vsel : vth));
         V[i] = vmin;
-        if (forced_active) act = forced_active[i] != 0;
+        if (forced_active && forced_active[i] != 2) act = forced_active[i] != 0;
         float rate = noise_rate >= 0.0f ? noise_rate : noise_per_neuron[i];
         int noise = u[i] < rate;
         int na = isolated ? noise : (noise | act);
@@ -346,4 +348,55 @@ int oracle_gen_rows(int R, const int64_t* region_start, const int64_t* region_n_
         free(chosen);
     }
     return bad;
+}
+
+/* --------------------------------------------------------- gamma properties */
+/* Per-neuron Gamma(alpha, 1) / beta draws of gamma-distributed properties
+ * (cuda/src/stage/property.cpp:313-344 sample_gamma uses the same method):
+ * Marsaglia & Tsang, ACM TOMS 26(3) 2000, with the alpha < 1 boost
+ * G(alpha) = G(alpha + 1) U^(1/alpha) and Box-Muller normals, in double, on
+ * Philox4x32-10 with counter {n_lo, n_hi, attempt, tag} and key
+ * {seed_lo, seed_hi ^ 0x47414D4D}; tag = 0x80000000 | receptor << 24 | call;
+ * at most 64 attempts, then the mode d. */
+static double gamma_u24(uint32_t x, int open_zero)
+{
+    return ((double)(x >> 8) + (open_zero ? 1.0 : 0.0)) * (1.0 / 16777216.0);
+}
+
+double oracle_gamma_unit(double alpha, uint64_t seed, uint64_t n, uint32_t tag)
+{
+    if (!(alpha > 0.0)) return 0.0;
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32) ^ 0x47414D4Du};
+    uint32_t o[4];
+    double scale = 1.0;
+    if (alpha < 1.0) {
+        const uint32_t ctr[4] = {(uint32_t)n, (uint32_t)(n >> 32), 0xffffffffu, tag};
+        oracle_philox4x32_10(ctr, key, o);
+        scale = pow(gamma_u24(o[0], 1), 1.0 / alpha);
+        alpha += 1.0;
+    }
+    const double d = alpha - 1.0 / 3.0;
+    const double c = 1.0 / sqrt(9.0 * d);
+    for (uint32_t it = 0; it < 64u; ++it) {
+        const uint32_t ctr[4] = {(uint32_t)n, (uint32_t)(n >> 32), it, tag};
+        oracle_philox4x32_10(ctr, key, o);
+        const double u1 = gamma_u24(o[0], 1), u2 = gamma_u24(o[1], 0);
+        const double x = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+        const double y = 1.0 + c * x;
+        if (y <= 0.0) continue;
+        const double v = y * y * y;
+        const double u = gamma_u24(o[2], 1);
+        const double xx = x * x;
+        if (u < 1.0 - 0.0331 * xx * xx) return scale * d * v;
+        if (log(u) < 0.5 * xx + d * (1.0 - v + log(v))) return scale * d * v;
+    }
+    return scale * d;
+}
+
+void oracle_gamma(int64_t count, const int64_t* neuron, double alpha, double beta, int receptor, uint32_t call,
+                  uint64_t seed, float* out)
+{
+    const uint32_t tag = 0x80000000u | ((uint32_t)receptor << 24) | (call & 0x00ffffffu);
+    for (int64_t i = 0; i < count; ++i)
+        out[i] = (float)(oracle_gamma_unit(alpha, seed, (uint64_t)neuron[i], tag) / beta);
 }

@@ -60,6 +60,8 @@ def lib():
         L.oracle_bold_step_f32.argtypes = [i64] + [vp] * 6 + [f64] * 8
         L.oracle_bold_step_f64.argtypes = [i64] + [vp] * 6 + [f64] * 8
         L.oracle_gen_rows.argtypes = [ctypes.c_int] + [vp] * 9 + [ctypes.c_int, f32, i64, i64, vp, vp, vp]
+        L.oracle_gamma.argtypes = [i64, vp, f64, f64, ctypes.c_int, u32, u64, vp]
+        L.oracle_gamma.restype = None
         L.oracle_gen_rows.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -277,6 +279,14 @@ class OracleBlock:
             raise MemoryError("oracle_block_step failed")
         self.step_index += 1
         return subblock_stats(self.V, self.active, P.sub_idx)
+
+
+def gamma(neurons, alpha: float, beta: float, receptor: int, call: int, seed: int) -> np.ndarray:
+    """Per-neuron Gamma(alpha, 1) / beta draws of the product's gamma-distributed g_ui (float32)."""
+    idx = np.ascontiguousarray(neurons, np.int64)
+    out = np.empty(len(idx), np.float32)
+    lib().oracle_gamma(len(idx), _p(idx), float(alpha), float(beta), int(receptor), int(call), int(seed), _p(out))
+    return out
 
 
 def bold_step(u, s, q, v, f, params: dict, delta_t: float):

@@ -161,6 +161,52 @@ def case_small_unsorted(seed: int = 7):
     print("small_blocks: mean spikes/step", res["sums"].sum(1).mean())
 
 
+def case_src(seed: int = 13, steps: int = 150):
+    """Input neurons (models/block.py:37-50, :104-109): N=200, neurons 0..39 have no incoming
+    synapse and replay a raster of steps + 1 columns."""
+    rng = np.random.default_rng(seed)
+    N, n_src, K = 200, 40, 20
+    post = np.repeat(np.arange(n_src, N), K)
+    pre = np.concatenate([rng.choice(N, K, replace=False) for _ in range(n_src, N)])
+    kind = np.where(pre >= 160, 2, 0).astype(np.uint8)
+    w = (rng.random((len(post), 2)) * 2.0).astype(np.float32)
+    spec = synthetic.config_single_block()
+    prop = np.repeat(spec.class_property[:1], N, axis=0).copy()
+    prop[160:] = spec.class_property[1]
+    prop[:, 3] = np.where(np.arange(N) < n_src, 0, np.where(np.arange(N) < 160, 1, 2))
+    prop[:, 2] = rng.uniform(0.0, 0.6, N)
+    prop[:, 10:14] *= np.float32(3.0)
+    prop = prop.astype(np.float32)
+    src = rng.random((n_src, steps + 1)) < 0.08
+    idx = np.stack([kind.astype(np.int64), post, pre])
+    idx = np.stack([idx, idx], axis=-1)
+    idx[0, :, 1] += 1
+    W = torch.sparse_coo_tensor(torch.from_numpy(idx.reshape(3, -1)), torch.from_numpy(w.reshape(-1).copy()),
+                                (4, N, N))
+    b = RefBlock(torch.from_numpy(prop), W, delta_t=0.1, src=torch.from_numpy(src))
+    assert np.array_equal(b.src_neuron.numpy(), np.arange(n_src))
+    out = {k: [] for k in ("active", "sums", "means", "V")}
+    with PhiloxRand(0) as rnd:
+        for _ in range(steps):
+            sm, m = b.run(noise_rate=0.01)
+            out["active"].append(packbits(b.active.numpy()))
+            out["sums"].append(sm.numpy().astype(np.float32))
+            out["means"].append(m.numpy().astype(np.float32))
+            out["V"].append(b.V_i.numpy().copy())
+        try:
+            b.run(noise_rate=0.01)
+            raise AssertionError("the reference accepted a step past its raster")
+        except IndexError:
+            pass
+        assert rnd.step == steps     # the failing step raises before drawing its noise
+    res = {key: np.stack(v) for key, v in out.items()}
+    np.savez_compressed(os.path.join(HERE, "src_block_ref.npz"), prop=prop, post=post, pre=pre, kind=kind, w=w,
+                        src=src, seed=0, dt=0.1, steps=steps, J_final=b.J_ui.numpy(), I_syn_final=b.I_syn.numpy(),
+                        t_last_final=b.t_ik_last.numpy(), **res)
+    act = np.unpackbits(res["active"], axis=-1, bitorder="little")[:, :N]
+    print("src_block: input spikes/step", act[:, :n_src].sum(1).mean(), "others", act[:, n_src:].sum(1).mean())
+
+
 def case_bold(steps: int = 300, R: int = 16, seed: int = 3):
     rng = np.random.default_rng(seed)
     out = {}
@@ -242,6 +288,9 @@ def case_statistics(seed: int = 9):
 
 if __name__ == "__main__":
     torch.set_num_threads(8)
+    if "--src" in sys.argv:
+        case_src()
+        sys.exit(0)
     if "--statistics" in sys.argv:
         case_statistics()
         sys.exit(0)

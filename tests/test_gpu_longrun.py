@@ -83,12 +83,12 @@ def test_longrun_push_statistics(oracle_run):
 
 def test_samples_subset_and_ring():
     """A subset of neurons; the ring keeps the last capacity steps, oldest first."""
-    spec = synthetic.config_single_block()
+    spec = _spec()
     rp, pre, kind, w = O.gen_network(spec.as_dict())
     prop = spec.property()
     ob = O.OracleBlock(prop, decay_like_reference(prop, spec.dt), rp, pre, kind, w, spec.dt, spec.seed)
-    idx = np.array([0, 5, 17, 1599, 1600, 1999, 1234], np.uint32)
-    n, cap = 300, 128
+    idx = np.concatenate([[999, 0, 5, 17, 799, 800, 17], np.arange(100, 900, 8)]).astype(np.uint32)
+    n, cap = 600, 128
     ref_sp = np.zeros((n, len(idx)), np.uint8)
     ref_v = np.zeros((n, len(idx)), np.float32)
     for i in range(n):

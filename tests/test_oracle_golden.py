@@ -136,3 +136,25 @@ def test_ensemble_members_equal_standalone_networks():
         seg = slice(ms * K, (ms + tm.N) * K)
         assert np.array_equal(pe[seg].astype(np.int64) - ms, ps.astype(np.int64))
         assert np.array_equal(ke[seg], ks) and np.array_equal(we[seg], ws)
+
+
+def test_oracle_input_neurons_vs_reference():
+    """models/block.py with src (input neurons replaying a raster), run by the reference itself."""
+    g = np.load(os.path.join(GOLDEN, "src_block_ref.npz"))
+    prop, src = g["prop"], g["src"]
+    N = prop.shape[0]
+    n_src = src.shape[0]
+    rp, pre, kind, w = O.pull_csr(N, g["post"], g["pre"], g["kind"], g["w"])
+    ob = O.OracleBlock(prop, decay_like_reference(prop, float(g["dt"])), rp, pre, kind, w, float(g["dt"]),
+                       int(g["seed"]))
+    act = unpack(g["active"], N)
+    for k in range(int(g["steps"])):
+        fa = np.full(N, 2, np.uint8)
+        fa[:n_src] = src[:, k]
+        s, m = ob.run(0.01, forced_active=fa)
+        assert np.array_equal(ob.active.astype(bool), act[k]), k
+        assert np.array_equal(ob.V, g["V"][k]), k
+        assert np.array_equal(s, g["sums"][k])
+    assert np.array_equal(ob.J, g["J_final"])
+    assert np.array_equal(ob.Isyn, g["I_syn_final"])
+    assert np.array_equal(ob.tlast, g["t_last_final"])
