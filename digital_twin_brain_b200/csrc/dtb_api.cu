@@ -162,9 +162,13 @@ struct dtb_block {
     int chunk = 32;
     int scatter_wpw = 32;         // bitmask words per warp in the push scatter
     int step_variant = 0;         // 0: 2 resident CTAs/SM register budget, 1: 3
-    // graphs: [mode][isolated-agnostic] chunk graphs
-    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
-    int graph_len[3] = {0, 0, 0};
+    // ordered push (bit-exact pull through per-neuron slots)
+    bool has_qpos = false;
+    int pull_method = 0;          // 0: ordered push while activity <= slot_threshold, 1: row gather, 2: ordered push
+    double slot_threshold = 0.1;
+    // graphs: one chunk graph per propagation method (push, pull rows, pull slots)
+    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+    int graph_len[4] = {0, 0, 0, 0};
     bool use_graphs = true;
     // attached BOLD
     int bold_R = 0;
@@ -385,9 +389,12 @@ static int ensure_stats(dtb_block* b, uint32_t rows)
 // Host CSR builders: stable counting sorts keep the given entry order
 // inside every row (pull: by post, torch.sparse.mm order; push: by pre,
 // cuda/src/configuration.cpp:228 stable_sort_by_key).
+// rel_out[e]: position of entry e inside its row; carried[d] = carry[e] for
+// the entry e placed at d (the pull-row positions travel into the push CSR).
 static int build_csr_host(int64_t N, int64_t S, const uint32_t* key, const uint32_t* other, const uint8_t* kind,
                           const float* w, std::vector<int64_t>& rowptr, std::vector<uint32_t>& col,
-                          std::vector<float2>& val, int64_t& max_row)
+                          std::vector<float2>& val, int64_t& max_row, std::vector<uint16_t>* rel_out = nullptr,
+                          const std::vector<uint16_t>* carry = nullptr, std::vector<uint16_t>* carried = nullptr)
 {
     rowptr.assign((size_t)N + 1, 0);
     for (int64_t e = 0; e < S; ++e) rowptr[(size_t)key[e] + 1]++;
@@ -399,10 +406,14 @@ static int build_csr_host(int64_t N, int64_t S, const uint32_t* key, const uint3
     col.resize((size_t)S);
     val.resize((size_t)S);
     std::vector<int64_t> cur(rowptr.begin(), rowptr.end() - 1);
+    if (rel_out) rel_out->resize((size_t)S);
+    if (carried) carried->resize((size_t)S);
     for (int64_t e = 0; e < S; ++e) {
         const int64_t d = cur[(size_t)key[e]]++;
         col[(size_t)d] = other[e] | (kind[e] ? kKindBit : 0u);
         val[(size_t)d] = make_float2(w[2 * e], w[2 * e + 1]);
+        if (rel_out) (*rel_out)[(size_t)e] = (uint16_t)(d - rowptr[(size_t)key[e]]);
+        if (carried) (*carried)[(size_t)d] = (*carry)[(size_t)e];
     }
     return DTB_OK;
 }
@@ -505,7 +516,7 @@ static int launch_stats(dtb_block* b, const DevState& s)
 
 // Persistent step kernels: as many CTAs as are resident at once, each warp
 // streaming a contiguous run of tiles.
-template <bool G, bool U, bool F, int M>
+template <int G, bool U, bool F, int M>
 static int step_blocks_per_sm()
 {
     static int v = 0;
@@ -528,7 +539,7 @@ static void step_grid(const dtb_block* b, int per_sm, unsigned& grid, int& tiles
     grid = (unsigned)((ntiles + (int64_t)tiles_per_warp * warps - 1) / ((int64_t)tiles_per_warp * warps));
 }
 
-template <bool G, bool U, bool F, int M>
+template <int G, bool U, bool F, int M>
 static void launch_step_m(dtb_block* b, const DevState& s)
 {
     unsigned grid;
@@ -537,7 +548,7 @@ static void launch_step_m(dtb_block* b, const DevState& s)
     k_step<G, U, F, M><<<grid, kStepThreads, 0, b->stream>>>(s, tpw);
 }
 
-template <bool G, bool U, bool F>
+template <int G, bool U, bool F>
 static void launch_step(dtb_block* b, const DevState& s)
 {
     if (b->step_variant == 1) launch_step_m<G, U, F, 3>(b, s);
@@ -565,7 +576,8 @@ static int launch_src(dtb_block* b, const DevState& s)
     return DTB_OK;
 }
 
-static int launch_update(dtb_block* b, const DevState& s, bool gather, bool forced)
+// gather: 0 none, kGatherRows (fused pull gather), kGatherSlots (ordered-push slots)
+static int launch_update(dtb_block* b, const DevState& s, int gather, bool forced)
 {
     if (s.N <= 0) return DTB_OK;
     if (s.n_src > 0 && s.forced_active == s.src_val) {   // input neurons replay their raster
@@ -573,35 +585,63 @@ static int launch_update(dtb_block* b, const DevState& s, bool gather, bool forc
         forced = true;
     }
     if (forced) {
-        if (gather) launch_step<true, true, true>(b, s);
-        else launch_step<false, true, true>(b, s);
+        if (gather == kGatherRows) launch_step<kGatherRows, true, true>(b, s);
+        else if (gather == kGatherSlots) launch_step<kGatherSlots, true, true>(b, s);
+        else launch_step<0, true, true>(b, s);
     } else {
-        if (gather) launch_step<true, true, false>(b, s);
-        else launch_step<false, true, false>(b, s);
+        if (gather == kGatherRows) launch_step<kGatherRows, true, false>(b, s);
+        else if (gather == kGatherSlots) launch_step<kGatherSlots, true, false>(b, s);
+        else launch_step<0, true, false>(b, s);
     }
     CK(cudaGetLastError());
     b->launches++;
     return launch_stats(b, s);
 }
 
-static int launch_gather_only(dtb_block* b, const DevState& s)
+// Folds the propagation of the last step into J (end of a pull run).
+static int launch_gather_only(dtb_block* b, const DevState& s, int gather = kGatherRows)
 {
     if (s.N <= 0) return DTB_OK;
-    launch_step<true, false, false>(b, s);
+    if (gather == kGatherSlots) launch_step<kGatherSlots, false, false>(b, s);
+    else launch_step<kGatherRows, false, false>(b, s);
     CK(cudaGetLastError());
     b->launches++;
     return DTB_OK;
 }
 
-static int launch_scatter(dtb_block* b, const DevState& s)
+static int launch_scatter(dtb_block* b, const DevState& s, bool ordered = false)
 {
     const int wpw = b->scatter_wpw;
     const int64_t warps = (s.n_words + wpw - 1) / wpw;
     const unsigned grid = grid_for(warps * 32, kScatterThreads);
     if (grid == 0) return DTB_OK;
-    k_scatter<<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
+    if (ordered) k_scatter<true><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
+    else k_scatter<false><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
     CK(cudaGetLastError());
     b->launches++;
+    return DTB_OK;
+}
+
+static void drop_graphs(dtb_block* b)
+{
+    for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+}
+
+// Internal propagation methods: DTB_MODE_PUSH, DTB_MODE_PULL (row gather) and
+// the ordered push that DTB_MODE_PULL resolves to while activity is low.
+constexpr int kModeSlots = 3;
+
+static int ensure_slots(dtb_block* b)
+{
+    DevState& s = b->ds;
+    if (s.slots) return DTB_OK;
+    uint32_t* cnt = nullptr; uint4* sl = nullptr;
+    RET(dalloc(b, &cnt, (size_t)std::max<int64_t>(b->N, 1)));
+    RET(dalloc(b, &sl, (size_t)std::max<int64_t>(b->N, 1) * kSlotCap));
+    CK(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (size_t)std::max<int64_t>(b->N, 1), b->stream));
+    s.slot_cnt = cnt;
+    s.slots = sl;
+    drop_graphs(b);
     return DTB_OK;
 }
 
@@ -612,12 +652,20 @@ static int enqueue_steps(dtb_block* b, int n, int mode)
     const DevState& s = b->ds;
     if (mode == DTB_MODE_PUSH) {
         for (int k = 0; k < n; ++k) {
-            RET(launch_update(b, s, false, false));
+            RET(launch_update(b, s, 0, false));
             RET(launch_scatter(b, s));
         }
+    } else if (mode == kModeSlots) {
+        RET(launch_update(b, s, 0, false));
+        RET(launch_scatter(b, s, true));
+        for (int k = 1; k < n; ++k) {
+            RET(launch_update(b, s, kGatherSlots, false));
+            RET(launch_scatter(b, s, true));
+        }
+        RET(launch_gather_only(b, s, kGatherSlots));
     } else {
-        RET(launch_update(b, s, false, false));
-        for (int k = 1; k < n; ++k) RET(launch_update(b, s, true, false));
+        RET(launch_update(b, s, 0, false));
+        for (int k = 1; k < n; ++k) RET(launch_update(b, s, kGatherRows, false));
         RET(launch_gather_only(b, s));
     }
     return DTB_OK;
@@ -655,6 +703,16 @@ static int choose_mode(dtb_block* b, int mode)
     if (!b->has_pull) return DTB_MODE_PUSH;
     const double f = b->last_frac < 0.0 ? 0.0 : b->last_frac;
     return f > b->pull_threshold ? DTB_MODE_PULL : DTB_MODE_PUSH;
+}
+
+// DTB_MODE_PULL runs as ordered push when the push CSR carries pull-row
+// positions and activity is low enough that rows rarely overflow their slots.
+static int resolve_method(dtb_block* b, int m)
+{
+    if (m != DTB_MODE_PULL || !b->has_qpos || !b->has_push || b->pull_method == 1) return m;
+    if (b->pull_method == 2) return kModeSlots;
+    const double f = b->last_frac < 0.0 ? 0.0 : b->last_frac;
+    return f <= b->slot_threshold ? kModeSlots : m;
 }
 
 static int set_run_params(dtb_block* b, float noise_rate, int isolated)
@@ -741,6 +799,81 @@ static int create_common(dtb_block* b, int device, float dt, uint64_t seed, uint
     return DTB_OK;
 }
 
+// Host sort of push rows longer than the device sort holds (same key).
+static int sort_long_push_rows(dtb_block* b, const std::vector<int64_t>& qrow, uint32_t* qcol, float2* qw,
+                               uint16_t* qpos)
+{
+    for (int64_t r = 0; r < b->N; ++r) {
+        const int64_t e0 = qrow[(size_t)r], len = qrow[(size_t)r + 1] - e0;
+        if (len <= kSortCap) continue;
+        std::vector<uint32_t> c((size_t)len), c2((size_t)len);
+        std::vector<float2> w((size_t)len), w2((size_t)len);
+        std::vector<uint16_t> p(qpos ? (size_t)len : 0), p2(qpos ? (size_t)len : 0);
+        CK(cudaMemcpy(c.data(), qcol + e0, 4 * (size_t)len, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(w.data(), qw + e0, 8 * (size_t)len, cudaMemcpyDeviceToHost));
+        if (qpos) CK(cudaMemcpy(p.data(), qpos + e0, 2 * (size_t)len, cudaMemcpyDeviceToHost));
+        std::vector<int64_t> ord((size_t)len);
+        for (int64_t k = 0; k < len; ++k) ord[(size_t)k] = k;
+        auto key = [&](int64_t k) {
+            return ((uint64_t)(c[(size_t)k] & kIndexMask) << 32) | (uint64_t)(c[(size_t)k] & kKindBit) |
+                   (qpos ? (uint64_t)p[(size_t)k] : 0ull);
+        };
+        std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t z) { return key(a) < key(z); });
+        for (int64_t k = 0; k < len; ++k) {
+            c2[(size_t)k] = c[(size_t)ord[(size_t)k]];
+            w2[(size_t)k] = w[(size_t)ord[(size_t)k]];
+            if (qpos) p2[(size_t)k] = p[(size_t)ord[(size_t)k]];
+        }
+        CK(cudaMemcpy(qcol + e0, c2.data(), 4 * (size_t)len, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(qw + e0, w2.data(), 8 * (size_t)len, cudaMemcpyHostToDevice));
+        if (qpos) CK(cudaMemcpy(qpos + e0, p2.data(), 2 * (size_t)len, cudaMemcpyHostToDevice));
+    }
+    return DTB_OK;
+}
+
+// Push CSR (rows = presynaptic neurons) by transposing the pull CSR on the
+// device: rows ordered by (postsynaptic neuron, kind, pull-row position), with
+// every entry's pull-row position (qpos, for the ordered push) when in-degrees
+// fit 16 bits.  counts: device [N+1] out-degrees, reused as fill cursors.
+static int build_push_device(dtb_block* b, uint32_t* counts, bool with_qpos)
+{
+    const int64_t N = b->N, S = b->S;
+    int64_t* qrow = nullptr; uint32_t* qcol = nullptr; float2* qw = nullptr; uint16_t* qpos = nullptr;
+    RET(dalloc(b, &qrow, (size_t)N + 1));
+    RET(dalloc(b, &qcol, (size_t)S));
+    RET(dalloc(b, &qw, (size_t)S));
+    if (with_qpos) RET(dalloc(b, &qpos, (size_t)S));
+    long long* tiles = nullptr;
+    const int64_t ntiles = (N + kScanTile - 1) / kScanTile;
+    CK(cudaMalloc(&tiles, sizeof(long long) * (size_t)(ntiles + 1)));
+    k_scan_tiles<<<(unsigned)ntiles, kScanThreads, 0, b->stream>>>(counts, N, qrow, tiles);
+    k_scan_tile_sums<<<1, kScanThreads, 0, b->stream>>>(tiles, ntiles);
+    k_scan_add<<<grid_for(N, 256), 256, 0, b->stream>>>(qrow, N, tiles, ntiles);
+    cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)(N + 1), b->stream);
+    k_fill_push<<<grid_for(N * 32, 256), 256, 0, b->stream>>>(N, b->ds.prow, b->ds.pcol, b->ds.pw, qrow, counts,
+                                                               qcol, qw, qpos);
+    cudaMemsetAsync(b->d_err, 0, 16, b->stream);
+    const size_t smem = (sizeof(unsigned long long) + sizeof(float2) + sizeof(uint16_t)) * (size_t)kSortCap * kSortWarps;
+    cudaFuncSetAttribute(k_sort_push_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_sort_push_rows<<<grid_for(N, kSortWarps), kSortWarps * 32, smem, b->stream>>>(N, qrow, qcol, qw, qpos, b->d_err);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    cudaFree(tiles);
+    unsigned herr[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(herr, b->d_err, 16, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(DTB_ERR_CUDA, "push CSR build: %s", cudaGetErrorString(e));
+    std::vector<int64_t> hq((size_t)N + 1);
+    CK(cudaMemcpy(hq.data(), qrow, sizeof(int64_t) * hq.size(), cudaMemcpyDeviceToHost));
+    if (herr[0]) RET(sort_long_push_rows(b, hq, qcol, qw, qpos));
+    int64_t mx = 0;
+    for (int64_t i = 0; i < N; ++i) mx = std::max(mx, hq[(size_t)i + 1] - hq[(size_t)i]);
+    b->max_out = mx;
+    b->ds.qrow = qrow; b->ds.qcol = qcol; b->ds.qw = qw; b->ds.qpos = qpos;
+    b->has_push = true;
+    b->has_qpos = qpos != nullptr;
+    return DTB_OK;
+}
+
 int dtb_block_create(const dtb_block_desc* d, dtb_block** out)
 {
     if (!d || !out) return fail(DTB_ERR_ARG, "null argument");
@@ -768,13 +901,27 @@ int dtb_block_create(const dtb_block_desc* d, dtb_block** out)
         if (rc == DTB_OK) rc = upload_classes(b, cls, true);
         if (rc == DTB_OK) {
             std::vector<int64_t> rp; std::vector<uint32_t> col; std::vector<float2> val;
-            rc = build_csr_host(N, S, d->post, d->pre, d->kind, d->weight, rp, col, val, b->max_in);
+            std::vector<uint16_t> rel, qpos;
+            rc = build_csr_host(N, S, d->post, d->pre, d->kind, d->weight, rp, col, val, b->max_in,
+                                d->build_push ? &rel : nullptr);
             if (rc == DTB_OK) rc = upload_csr(b, rp, col, val, &b->ds.prow, &b->ds.pcol, &b->ds.pw);
             b->has_pull = (rc == DTB_OK);
             if (rc == DTB_OK && d->build_push) {
-                rc = build_csr_host(N, S, d->pre, d->post, d->kind, d->weight, rp, col, val, b->max_out);
+                const bool pos16 = b->max_in <= 65535;   // pull-row positions fit 16 bits
+                rc = build_csr_host(N, S, d->pre, d->post, d->kind, d->weight, rp, col, val, b->max_out, nullptr,
+                                    pos16 ? &rel : nullptr, pos16 ? &qpos : nullptr);
                 if (rc == DTB_OK) rc = upload_csr(b, rp, col, val, &b->ds.qrow, &b->ds.qcol, &b->ds.qw);
                 b->has_push = (rc == DTB_OK);
+                if (rc == DTB_OK && pos16) {
+                    uint16_t* dq = nullptr;
+                    rc = dalloc(b, &dq, (size_t)S);
+                    if (rc == DTB_OK && S > 0) {
+                        cudaError_t e = cudaMemcpy(dq, qpos.data(), sizeof(uint16_t) * (size_t)S, cudaMemcpyHostToDevice);
+                        if (e != cudaSuccess) rc = fail(DTB_ERR_CUDA, "qpos upload: %s", cudaGetErrorString(e));
+                    }
+                    b->ds.qpos = dq;
+                    b->has_qpos = (rc == DTB_OK);
+                }
             }
         }
         if (rc == DTB_OK) rc = finish_create(b);
@@ -948,46 +1095,7 @@ int dtb_block_create_synthetic(const dtb_synth_desc* d, dtb_block** out)
             b->max_in = d->K;
         }
         // push CSR by transposition on the device
-        if (rc == DTB_OK && d->build_push) {
-            int64_t* qrow = nullptr; uint32_t* qcol = nullptr; float2* qw = nullptr;
-            rc = dalloc(b, &qrow, (size_t)N + 1);
-            if (rc == DTB_OK) rc = dalloc(b, &qcol, (size_t)S);
-            if (rc == DTB_OK) rc = dalloc(b, &qw, (size_t)S);
-            long long* tiles = nullptr;
-            const int64_t ntiles = (N + kScanTile - 1) / kScanTile;
-            if (rc == DTB_OK) {
-                cudaError_t e = cudaMalloc(&tiles, sizeof(long long) * (size_t)(ntiles + 1));
-                if (e != cudaSuccess) { cudaGetLastError(); rc = fail(DTB_ERR_NOMEM, "scan temporaries"); }
-            }
-            if (rc == DTB_OK) {
-                k_scan_tiles<<<(unsigned)ntiles, kScanThreads, 0, b->stream>>>(outdeg, N, qrow, tiles);
-                k_scan_tile_sums<<<1, kScanThreads, 0, b->stream>>>(tiles, ntiles);
-                k_scan_add<<<grid_for(N, 256), 256, 0, b->stream>>>(qrow, N, tiles, ntiles);
-                cudaMemsetAsync(outdeg, 0, sizeof(uint32_t) * (size_t)(N + 1), b->stream);
-                k_fill_push<<<grid_for(N * 32, 256), 256, 0, b->stream>>>(N, prow, pcol, pw, qrow, outdeg, qcol, qw);
-                cudaMemsetAsync(b->d_err, 0, 16, b->stream);
-                const size_t smem = (sizeof(unsigned long long) + sizeof(float2)) * (size_t)kSortCap * kSortWarps;
-                cudaFuncSetAttribute(k_sort_push_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                k_sort_push_rows<<<grid_for(N, kSortWarps), kSortWarps * 32, smem, b->stream>>>(N, qrow, qcol, qw, b->d_err);
-                cudaError_t e = cudaGetLastError();
-                if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-                unsigned herr[4] = {0, 0, 0, 0};
-                if (e == cudaSuccess) e = cudaMemcpy(herr, b->d_err, 16, cudaMemcpyDeviceToHost);
-                if (e != cudaSuccess) rc = fail(DTB_ERR_CUDA, "push CSR build: %s", cudaGetErrorString(e));
-                else if (herr[0]) rc = fail(DTB_ERR_LIMIT, "push CSR build: %u rows longer than %d", herr[0], kSortCap);
-                // max out-degree
-                if (rc == DTB_OK) {
-                    std::vector<int64_t> hq((size_t)N + 1);
-                    cudaMemcpy(hq.data(), qrow, sizeof(int64_t) * hq.size(), cudaMemcpyDeviceToHost);
-                    int64_t mx = 0;
-                    for (int64_t i = 0; i < N; ++i) mx = std::max(mx, hq[(size_t)i + 1] - hq[(size_t)i]);
-                    b->max_out = mx;
-                }
-            }
-            if (tiles) cudaFree(tiles);
-            b->ds.qrow = qrow; b->ds.qcol = qcol; b->ds.qw = qw;
-            b->has_push = (rc == DTB_OK);
-        }
+        if (rc == DTB_OK && d->build_push) rc = build_push_device(b, outdeg, d->K <= 65535);
         cudaFree(t_rs); cudaFree(t_ne); cudaFree(t_cum); cudaFree(t_out); cudaFree(t_tab);
     }
     if (rc == DTB_OK) rc = finish_create(b);
@@ -1001,71 +1109,140 @@ int dtb_block_create_from_npz(const char* dir, float dt, uint64_t seed, uint32_t
 {
     if (!dir || !out) return fail(DTB_ERR_ARG, "null argument");
     *out = nullptr;
-    // generation/read_block.py:31-40: block_0.npz, block_1.npz, ... and their bases
-    std::vector<std::map<std::string, NpyArray>> files;
+    // generation/read_block.py:31-40: block_0.npz, block_1.npz, ... and their bases.
+    // Two passes over the files keep host memory at one file's synapses: the first
+    // reads the properties and counts the synapses, the second sorts every file's
+    // synapses into its own pull rows (a file holds every row of its population)
+    // and copies them to the device.
+    std::vector<std::string> paths;
     for (int i = 0;; ++i) {
         std::string path = std::string(dir) + "/block_" + std::to_string(i) + ".npz";
         FILE* f = std::fopen(path.c_str(), "rb");
         if (!f) break;
         std::fclose(f);
+        paths.push_back(path);
+    }
+    if (paths.empty()) return fail(DTB_ERR_IO, "no block_0.npz in %s", dir);
+    const size_t F = paths.size();
+    std::vector<int64_t> bases(F + 1, 0), syn(F + 1, 0);
+    std::vector<float> prop;
+    {
+        const std::vector<std::string> only = {"property", "output_neuron_idx"};
+        for (size_t i = 0; i < F; ++i) {
+            std::map<std::string, NpyArray> m;
+            std::vector<std::string> names;
+            std::string err;
+            if (!npz_read(paths[i], m, err, &only, &names)) return fail(DTB_ERR_FORMAT, "%s", err.c_str());
+            auto it = m.find("property");
+            if (it == m.end() || it->second.shape.size() != 2 || it->second.shape[1] != DTB_NPROP ||
+                it->second.descr != "<f4")
+                return fail(DTB_ERR_FORMAT, "block_%zu.npz: property must be float32 [N,22]", i);
+            for (auto& nm : names)
+                if (nm == "src_timestamp" || nm == "src_neuron_idx")
+                    return fail(DTB_ERR_FORMAT, "block_%zu.npz: input (src) blocks are not supported", i);
+            if (!m.count("output_neuron_idx")) return fail(DTB_ERR_FORMAT, "block_%zu.npz: missing output_neuron_idx", i);
+            bases[i + 1] = bases[i] + it->second.shape[0];
+            syn[i + 1] = syn[i] + m["output_neuron_idx"].count();
+            const size_t at = prop.size();
+            prop.resize(at + it->second.data.size() / sizeof(float));
+            std::memcpy(prop.data() + at, it->second.data.data(), it->second.data.size());
+        }
+    }
+    const int64_t N = bases.back(), S = syn.back();
+    if (N <= 0 || N > (int64_t)kIndexMask) return fail(DTB_ERR_LIMIT, "n_neurons must be in [1, 2^31-1]");
+    dtb_block* b = new dtb_block();
+    DeviceGuard guard(device < 0 ? 0 : device);
+    int rc = create_common(b, device, dt, seed, stream_id);
+    std::vector<uint32_t> cls;
+    if (rc == DTB_OK) {
+        b->N = N;
+        b->S = S;
+        rc = build_classes(b, N, prop.data(), nullptr, cls);
+    }
+    if (rc == DTB_OK) rc = alloc_state(b);
+    if (rc == DTB_OK) rc = upload_classes(b, cls, true);
+    int64_t* prow = nullptr; uint32_t* pcol = nullptr; float2* pw = nullptr; uint32_t* counts = nullptr;
+    if (rc == DTB_OK) rc = dalloc(b, &prow, (size_t)N + 1);
+    if (rc == DTB_OK) rc = dalloc(b, &pcol, (size_t)S);
+    if (rc == DTB_OK) rc = dalloc(b, &pw, (size_t)S);
+    std::vector<int64_t> rp((size_t)N + 1, 0);
+    std::vector<uint32_t> outdeg(build_push ? (size_t)N + 1 : 0, 0u);
+    const std::vector<std::string> syn_names = {"output_neuron_idx", "input_block_idx", "input_neuron_idx",
+                                                "input_channel_offset", "weight"};
+    for (size_t i = 0; i < F && rc == DTB_OK; ++i) {
         std::map<std::string, NpyArray> m;
         std::string err;
-        if (!npz_read(path, m, err)) return fail(DTB_ERR_FORMAT, "%s", err.c_str());
-        files.push_back(std::move(m));
-    }
-    if (files.empty()) return fail(DTB_ERR_IO, "no block_0.npz in %s", dir);
-    std::vector<int64_t> bases(files.size() + 1, 0);
-    for (size_t i = 0; i < files.size(); ++i) {
-        auto it = files[i].find("property");
-        if (it == files[i].end() || it->second.shape.size() != 2 || it->second.shape[1] != DTB_NPROP ||
-            it->second.descr != "<f4")
-            return fail(DTB_ERR_FORMAT, "block_%zu.npz: property must be float32 [N,22]", i);
-        if (files[i].count("src_timestamp") || files[i].count("src_neuron_idx"))
-            return fail(DTB_ERR_FORMAT, "block_%zu.npz: input (src) blocks are not supported", i);
-        bases[i + 1] = bases[i] + it->second.shape[0];
-    }
-    const int64_t N = bases.back();
-    std::vector<float> prop((size_t)N * DTB_NPROP);
-    std::vector<uint32_t> post, pre;
-    std::vector<uint8_t> kind;
-    std::vector<float> w;
-    for (size_t i = 0; i < files.size(); ++i) {
-        auto& m = files[i];
-        const NpyArray& p = m["property"];
-        std::memcpy(prop.data() + bases[i] * DTB_NPROP, p.data.data(), p.data.size());
-        const char* names[5] = {"output_neuron_idx", "input_block_idx", "input_neuron_idx", "input_channel_offset", "weight"};
-        for (auto nm : names)
-            if (!m.count(nm)) return fail(DTB_ERR_FORMAT, "block_%zu.npz: missing %s", i, nm);
+        if (!npz_read(paths[i], m, err, &syn_names)) { rc = fail(DTB_ERR_FORMAT, "%s", err.c_str()); break; }
+        for (auto& nm : syn_names)
+            if (!m.count(nm)) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: missing %s", i, nm.c_str()); break; }
+        if (rc != DTB_OK) break;
         const NpyArray &on = m["output_neuron_idx"], &ib = m["input_block_idx"], &in = m["input_neuron_idx"],
                        &ic = m["input_channel_offset"], &wt = m["weight"];
         const int64_t E = on.count();
-        if (ib.count() != E || in.count() != E || ic.count() != E || wt.count() != 2 * E)
-            return fail(DTB_ERR_FORMAT, "block_%zu.npz: inconsistent synapse array lengths", i);
-        if (on.descr != "<u4" || in.descr != "<u4" || ib.descr != "<i2" || ic.descr != "|u1" || wt.descr != "<f4")
-            return fail(DTB_ERR_FORMAT, "block_%zu.npz: unexpected synapse dtypes", i);
+        if (E != syn[i + 1] - syn[i] || ib.count() != E || in.count() != E || ic.count() != E || wt.count() != 2 * E) {
+            rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: inconsistent synapse array lengths", i);
+            break;
+        }
+        if (on.descr != "<u4" || in.descr != "<u4" || ib.descr != "<i2" || ic.descr != "|u1" || wt.descr != "<f4") {
+            rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: unexpected synapse dtypes", i);
+            break;
+        }
         const uint32_t* onp = reinterpret_cast<const uint32_t*>(on.data.data());
         const int16_t* ibp = reinterpret_cast<const int16_t*>(ib.data.data());
         const uint32_t* inp = reinterpret_cast<const uint32_t*>(in.data.data());
         const uint8_t* icp = reinterpret_cast<const uint8_t*>(ic.data.data());
         const float* wtp = reinterpret_cast<const float*>(wt.data.data());
+        // stable counting sort of this file's entries into its rows (file order inside a row)
+        const int64_t n_i = bases[i + 1] - bases[i];
+        std::vector<int64_t> cur((size_t)n_i + 1, 0);
+        for (int64_t e = 0; e < E; ++e) {
+            if ((int64_t)onp[e] >= n_i) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: neuron index out of range", i); break; }
+            cur[(size_t)onp[e] + 1]++;
+        }
+        if (rc != DTB_OK) break;
+        for (int64_t r = 0; r < n_i; ++r) {
+            b->max_in = std::max<int64_t>(b->max_in, cur[(size_t)r + 1]);
+            cur[(size_t)r + 1] += cur[(size_t)r];
+            rp[(size_t)(bases[i] + r + 1)] = syn[i] + cur[(size_t)r + 1];
+        }
+        std::vector<uint32_t> col((size_t)E);
+        std::vector<float2> val((size_t)E);
         for (int64_t e = 0; e < E; ++e) {
             const int64_t sb = (int64_t)i + ibp[e];
-            if (sb < 0 || sb >= (int64_t)files.size()) return fail(DTB_ERR_FORMAT, "block_%zu.npz: input_block_idx out of range", i);
-            const int64_t po = bases[i] + onp[e], pr = bases[(size_t)sb] + inp[e];
-            if (po >= bases[i + 1] || pr >= bases[(size_t)sb + 1]) return fail(DTB_ERR_FORMAT, "block_%zu.npz: neuron index out of range", i);
-            post.push_back((uint32_t)po);
-            pre.push_back((uint32_t)pr);
-            kind.push_back(icp[e]);
-            w.push_back(wtp[2 * e]);
-            w.push_back(wtp[2 * e + 1]);
+            if (sb < 0 || sb >= (int64_t)F) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: input_block_idx out of range", i); break; }
+            const int64_t pr = bases[(size_t)sb] + inp[e];
+            if (pr >= bases[(size_t)sb + 1]) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: neuron index out of range", i); break; }
+            if (icp[e] != 0 && icp[e] != 2) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: input_channel_offset must be 0 or 2", i); break; }
+            const int64_t d = cur[onp[e]]++;
+            col[(size_t)d] = (uint32_t)pr | (icp[e] ? kKindBit : 0u);
+            val[(size_t)d] = make_float2(wtp[2 * e], wtp[2 * e + 1]);
+            if (build_push) outdeg[(size_t)pr]++;
+        }
+        if (rc != DTB_OK) break;
+        if (E > 0) {
+            cudaError_t e1 = cudaMemcpy(pcol + syn[i], col.data(), 4 * (size_t)E, cudaMemcpyHostToDevice);
+            if (e1 == cudaSuccess) e1 = cudaMemcpy(pw + syn[i], val.data(), 8 * (size_t)E, cudaMemcpyHostToDevice);
+            if (e1 != cudaSuccess) rc = fail(DTB_ERR_CUDA, "synapse upload: %s", cudaGetErrorString(e1));
         }
     }
-    dtb_block_desc d;
-    std::memset(&d, 0, sizeof(d));
-    d.n_neurons = N; d.property = prop.data(); d.decay = nullptr;
-    d.n_synapses = (int64_t)post.size(); d.post = post.data(); d.pre = pre.data(); d.kind = kind.data(); d.weight = w.data();
-    d.dt = dt; d.seed = seed; d.stream_id = stream_id; d.device = device; d.build_push = build_push;
-    return dtb_block_create(&d, out);
+    if (rc == DTB_OK) {
+        cudaError_t e1 = cudaMemcpy(prow, rp.data(), sizeof(int64_t) * rp.size(), cudaMemcpyHostToDevice);
+        if (e1 != cudaSuccess) rc = fail(DTB_ERR_CUDA, "row pointer upload: %s", cudaGetErrorString(e1));
+        b->ds.prow = prow; b->ds.pcol = pcol; b->ds.pw = pw;
+        b->has_pull = (rc == DTB_OK);
+    }
+    if (rc == DTB_OK && build_push) {
+        rc = dalloc(b, &counts, (size_t)N + 1);
+        if (rc == DTB_OK) {
+            cudaError_t e1 = cudaMemcpy(counts, outdeg.data(), sizeof(uint32_t) * outdeg.size(), cudaMemcpyHostToDevice);
+            if (e1 != cudaSuccess) rc = fail(DTB_ERR_CUDA, "out-degree upload: %s", cudaGetErrorString(e1));
+        }
+        if (rc == DTB_OK) rc = build_push_device(b, counts, b->max_in <= 65535);
+    }
+    if (rc == DTB_OK) rc = finish_create(b);
+    if (rc != DTB_OK) { destroy_block(b); return rc; }
+    *out = b;
+    return DTB_OK;
 }
 
 int dtb_block_destroy(dtb_block* b)
@@ -1123,13 +1300,15 @@ int dtb_block_run(dtb_block* b, int n_steps, float noise_rate, int isolated, int
     int64_t done = 0;
     while (done < n_steps) {
         const int m = choose_mode(b, mode);
+        const int mm = resolve_method(b, m);
+        if (mm == kModeSlots) RET(ensure_slots(b));
         const uint32_t cap = b->stats_cap;
         int n = (int)std::min<int64_t>(n_steps - done, (int64_t)std::min<uint32_t>(cap, (uint32_t)b->chunk));
         RET(set_run_params(b, noise_rate, isolated));
-        RET(enqueue_chunk(b, n, m));
+        RET(enqueue_chunk(b, n, mm));
         b->steps += (uint64_t)n;
         std::vector<uint32_t> nact;
-        const bool want_nact = (mode == DTB_MODE_AUTO);
+        const bool want_nact = (mode == DTB_MODE_AUTO) || (m == DTB_MODE_PULL && b->has_qpos && b->pull_method == 0);
         RET(emit_stats(b, n, done, sum_out, mean_out, nact_out, where, want_nact ? &nact : nullptr));
         if (want_nact && n > 0) {
             double tot = 0.0;
@@ -1146,7 +1325,8 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
     if (!b || !out_ms || n_steps <= 0) return fail(DTB_ERR_ARG, "bad argument");
     RET(check_src_steps(b, n_steps));
     DeviceGuard g(b->device);
-    const int m = choose_mode(b, mode);
+    const int m = resolve_method(b, choose_mode(b, mode));
+    if (m == kModeSlots) RET(ensure_slots(b));
     RET(ensure_stats(b, (uint32_t)n_steps));
     RET(set_run_params(b, noise_rate, isolated));
     unsigned long long ev0 = 0, ev1 = 0;
@@ -1155,29 +1335,35 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
     const int n_ev = 4 * n_steps + 4;
     std::vector<cudaEvent_t> ev((size_t)n_ev);
     for (auto& e : ev) CK(cudaEventCreate(&e));
-    std::vector<int> kind;  // 0 update kernel, 1 propagation-only kernel
+    std::vector<int> kind;  // 0 update kernel, 1 propagation kernel, 2 closing fold (not averaged)
     int k = 0;
     auto rec = [&](int i) { return cudaEventRecord(ev[(size_t)i], b->stream); };
     int rc = DTB_OK;
-    if (m == DTB_MODE_PUSH) {
-        for (int st = 0; st < n_steps && rc == DTB_OK; ++st) {
-            rec(k); rc = launch_update(b, b->ds, false, false); rec(k + 1); kind.push_back(0); k += 2;
+    int done_steps = 0;
+    if (m == DTB_MODE_PUSH || m == kModeSlots) {
+        const bool ord = m == kModeSlots;
+        for (int st = 0; st < n_steps && rc == DTB_OK && k + 6 <= n_ev; ++st) {
+            rec(k); rc = launch_update(b, b->ds, (ord && st > 0) ? kGatherSlots : 0, false); rec(k + 1);
+            kind.push_back(0); k += 2;
             if (rc != DTB_OK) break;
-            rec(k); rc = launch_scatter(b, b->ds); rec(k + 1); kind.push_back(1); k += 2;
-            if (k + 2 > n_ev) break;
+            rec(k); rc = launch_scatter(b, b->ds, ord); rec(k + 1); kind.push_back(1); k += 2;
+            done_steps++;
+        }
+        if (ord && rc == DTB_OK) {
+            rec(k); rc = launch_gather_only(b, b->ds, kGatherSlots); rec(k + 1); kind.push_back(2); k += 2;
         }
     } else {
-        rec(k); rc = launch_update(b, b->ds, false, false); rec(k + 1); kind.push_back(0); k += 2;
+        rec(k); rc = launch_update(b, b->ds, 0, false); rec(k + 1); kind.push_back(0); k += 2;
         for (int st = 1; st < n_steps && rc == DTB_OK && k + 4 <= n_ev; ++st) {
-            rec(k); rc = launch_update(b, b->ds, true, false); rec(k + 1); kind.push_back(0); k += 2;
+            rec(k); rc = launch_update(b, b->ds, kGatherRows, false); rec(k + 1); kind.push_back(0); k += 2;
         }
         if (rc == DTB_OK) { rec(k); rc = launch_gather_only(b, b->ds); rec(k + 1); kind.push_back(1); k += 2; }
+        done_steps = (int)kind.size() - 1;
     }
-    const int done_steps = (m == DTB_MODE_PUSH) ? (int)(kind.size() / 2) : (int)kind.size() - 1;
     b->steps += (uint64_t)done_steps;
     cudaError_t e = cudaStreamSynchronize(b->stream);
-    double sum[2] = {0.0, 0.0};
-    int cnt[2] = {0, 0};
+    double sum[3] = {0.0, 0.0, 0.0};
+    int cnt[3] = {0, 0, 0};
     for (size_t i = 0; i < kind.size() && e == cudaSuccess; ++i) {
         float ms = 0.0f;
         e = cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
@@ -1197,10 +1383,6 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
     return DTB_OK;
 }
 
-static void drop_graphs(dtb_block* b)
-{
-    for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
-}
 
 int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
 {
@@ -1209,6 +1391,11 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
     case DTB_TUNE_SCATTER_WORDS:
         if (value < 1 || value > 32) return fail(DTB_ERR_ARG, "scatter words per warp must be 1..32");
         b->scatter_wpw = (int)value;
+        break;
+    case DTB_TUNE_PULL_METHOD:
+        if (value < 0 || value > 2) return fail(DTB_ERR_ARG, "pull method must be 0 (auto), 1 (rows) or 2 (ordered push)");
+        if (value == 2 && !b->has_qpos) return fail(DTB_ERR_STATE, "ordered push needs the push CSR with pull-row positions");
+        b->pull_method = (int)value;
         break;
     case DTB_TUNE_CHUNK:
         if (value < 1 || value > 4096) return fail(DTB_ERR_ARG, "chunk must be 1..4096");
@@ -1238,6 +1425,7 @@ int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value)
     case DTB_TUNE_PULL_THRESHOLD_PPM: *value = (int64_t)std::llround(b->pull_threshold * 1e6); break;
     case DTB_TUNE_USE_GRAPHS: *value = b->use_graphs ? 1 : 0; break;
     case DTB_TUNE_STEP_VARIANT: *value = b->step_variant; break;
+    case DTB_TUNE_PULL_METHOD: *value = b->pull_method; break;
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
     }
     return DTB_OK;
@@ -1312,7 +1500,7 @@ int dtb_block_step_forced(dtb_block* b, float noise_rate, int isolated, int mode
     RET(check_src_steps(b, 1));
     RET(set_run_params(b, noise_rate, isolated));
     const int m = choose_mode(b, mode);
-    RET(launch_update(b, s, false, true));
+    RET(launch_update(b, s, 0, true));
     if (m == DTB_MODE_PUSH) RET(launch_scatter(b, s));
     else RET(launch_gather_only(b, s));
     b->steps += 1;

@@ -19,6 +19,9 @@ namespace dtb {
 constexpr uint32_t kKindBit = 0x80000000u;
 constexpr uint32_t kIndexMask = 0x7fffffffu;
 constexpr int kWarpNeurons = 128;      // neurons owned by one warp in the step kernels
+constexpr uint32_t kSlotCap = 8;       // ordered-push contributions kept per neuron and step
+constexpr int kGatherRows = 1;         // k_step gathers whole pull rows
+constexpr int kGatherSlots = 2;        // k_step sums its ordered-push slots
 constexpr int kStepThreads = 256;      // 8 warps, 1024 neurons per CTA
 
 // One deduplicated row of the 22-column property matrix
@@ -105,6 +108,10 @@ struct DevState {
     const int64_t* prow; const uint32_t* pcol; const float2* pw;
     // push CSR
     const int64_t* qrow; const uint32_t* qcol; const float2* qw;
+    const uint16_t* qpos;       // [S] position of every push entry inside its pull row (nullable)
+    // ordered push (bit-exact pull order at push cost): pending contributions per neuron
+    uint32_t* slot_cnt;         // [N] contributions written since the neuron last consumed them
+    uint4* slots;               // [N][kSlotCap] {pull-row position | kind bit, 0, w.x bits, w.y bits}
     // statistics
     int n_sub;
     uint32_t* sub_spk;          // [n_sub] accumulators (active)

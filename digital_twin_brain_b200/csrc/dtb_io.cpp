@@ -2,6 +2,8 @@
 // ZIP container with ZIP64 extensions; deflate through zlib).
 #include "dtb_io.h"
 
+#include <algorithm>
+
 #include <zlib.h>
 
 #include <cstdio>
@@ -104,7 +106,8 @@ static bool inflate_raw(const unsigned char* src, size_t n, std::vector<char>& d
     return true;
 }
 
-bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std::string& err)
+bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std::string& err,
+              const std::vector<std::string>* only, std::vector<std::string>* names)
 {
     FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) { err = "cannot open " + path; return false; }
@@ -151,6 +154,12 @@ bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std
             q += 4 + sz;
         }
         p += 46 + (uint64_t)nlen + xlen + clen;
+        {
+            std::string key = name;
+            if (key.size() > 4 && key.compare(key.size() - 4, 4, ".npy") == 0) key = key.substr(0, key.size() - 4);
+            if (names) names->push_back(key);
+            if (only && std::find(only->begin(), only->end(), key) == only->end()) continue;
+        }
         if (loff + 30 > (uint64_t)fsize || rd32(b + loff) != 0x04034b50u) { err = "bad local header: " + name; return false; }
         const uint64_t data = loff + 30 + rd16(b + loff + 26) + rd16(b + loff + 28);
         if (data + csize > (uint64_t)fsize) { err = "truncated member: " + name; return false; }

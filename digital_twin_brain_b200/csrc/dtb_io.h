@@ -27,7 +27,10 @@ struct NpyArray {
 // Parses one .npy buffer. Returns false and sets err on failure.
 bool npy_parse(const char* buf, size_t len, NpyArray& out, std::string& err);
 
-// Reads every member of a .npz (ZIP; stored or deflate; ZIP64 aware).
-bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std::string& err);
+// Reads the members of a .npz (ZIP; stored or deflate; ZIP64 aware): all of
+// them, or those named in `only` (names without ".npy").  `names` (nullable)
+// receives every member name.
+bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std::string& err,
+              const std::vector<std::string>* only = nullptr, std::vector<std::string>* names = nullptr);
 
 }  // namespace dtb

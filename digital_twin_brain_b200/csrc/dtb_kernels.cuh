@@ -114,6 +114,37 @@ __device__ __forceinline__ float4 gather_row(const DevState& s, const uint32_t* 
     return make_float4(a0, a1, a2, a3);
 }
 
+// Sum of one neuron's c <= kSlotCap ordered-push contributions in ascending
+// pull-row position (the order gather_row adds them).  Two terms added to +0
+// give the same float in either order, so only c >= 3 needs the ordering.
+__device__ __forceinline__ float4 slot_sum(const uint4* __restrict__ sl, uint32_t c)
+{
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+    auto add = [&](uint4 v) {
+        const float wx = __uint_as_float(v.z), wy = __uint_as_float(v.w);
+        if (v.x & kKindBit) { a2 = __fadd_rn(a2, wx); a3 = __fadd_rn(a3, wy); }
+        else { a0 = __fadd_rn(a0, wx); a1 = __fadd_rn(a1, wy); }
+    };
+    if (c <= 2u) {
+        add(__ldcs(sl));
+        if (c == 2u) add(__ldcs(sl + 1));
+    } else {
+        uint32_t last = 0u;
+        for (uint32_t r = 0; r < c; ++r) {
+            uint4 best = make_uint4(0u, 0u, 0u, 0u);
+            uint32_t bp = 0xffffffffu;
+            for (uint32_t k = 0; k < c; ++k) {
+                const uint4 v = sl[k];
+                const uint32_t p = v.x & kIndexMask;
+                if ((r == 0u || p > last) && p < bp) { bp = p; best = v; }
+            }
+            add(best);
+            last = bp;
+        }
+    }
+    return make_float4(a0, a1, a2, a3);
+}
+
 // ------------------------------------------------------------ BOLD step
 // models/bold_model_pytorch.py:43-78 in float64 for region r with input u
 // (q before v before f_in before s, f_in clamped at 0).
@@ -258,7 +289,7 @@ __global__ void k_samples(DevState s)
 // subblock, so the CTA-wide barrier and the done-count happen once per CTA.
 // MINB = resident CTAs per SM the register budget is sized for (2: no spills,
 // 3: more warps, a few spills); the autotuner picks per network.
-template <bool GATHER, bool UPDATE, bool FORCED, int MINB = 2>
+template <int GATHER, bool UPDATE, bool FORCED, int MINB = 2>
 __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int tiles_per_warp)
 {
     constexpr int kWarps = kStepThreads / 32;
@@ -296,7 +327,48 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     for (int64_t tile = tile0; tile < tile1; ++tile) {
         const int64_t base = tile * kWarpNeurons;
         float4 Jn[4];
-        if (GATHER) {
+        if (GATHER == kGatherSlots) {
+            float4 sum[4];
+            uint32_t ovf = 0u;   // bit j: neuron j of this lane got more contributions than slots
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                sum[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (n < s.N) {
+                    const uint32_t c = __ldcs(s.slot_cnt + n);
+                    if (c) {
+                        s.slot_cnt[n] = 0u;
+                        if (c > kSlotCap) ovf |= 1u << j;
+                        else sum[j] = slot_sum(s.slots + n * kSlotCap, c);
+                    }
+                }
+            }
+            // overflowing rows: the warp gathers them whole, in row order
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                unsigned m = __ballot_sync(0xffffffffu, (ovf >> j) & 1u);
+                while (m) {
+                    const int l = __ffs(m) - 1;
+                    m &= m - 1;
+                    uint32_t ev = 0;
+                    const float4 a = gather_row(s, gbits, base + j * 32 + l, lane, ev);
+                    if (lane == l) sum[j] = a;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                if (n < s.N) Jn[j] = add4(load_J(s, n), sum[j]);   // models/block.py:71-73
+            }
+            if (!UPDATE) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t n = base + j * 32 + lane;
+                    if (n < s.N) store_J(s, n, Jn[j]);
+                }
+                continue;
+            }
+        } else if (GATHER == kGatherRows) {
             float4 sum[4];
             uint32_t events = 0;
 #pragma unroll
@@ -519,6 +591,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
 constexpr int kScatterThreads = 256;
 constexpr int kScatterMaxWords = 32;
 
+template <bool ORDERED>
 __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw)
 {
     __shared__ uint32_t sh_rows[kScatterThreads / 32][kScatterMaxWords * 32];
@@ -566,6 +639,7 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
         for (int64_t v0 = 0; v0 < T; v0 += 128) {
             uint32_t c[4];
             float2 w[4];
+            uint32_t ppos[4];
             bool ok[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -585,13 +659,21 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
                     const int64_t e = re0 + (v - rs);
                     c[u] = __ldcs(s.qcol + e);
                     w[u] = __ldcs(s.qw + e);
+                    if (ORDERED) ppos[u] = __ldcs(s.qpos + e);
                 }
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                if (ok[u]) {
-                    float2* dst = s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + (int64_t)(c[u] & kIndexMask) * s.j_es;
-                    atomicAdd(dst, w[u]);
+                if (!ok[u]) continue;
+                const int64_t post = (int64_t)(c[u] & kIndexMask);
+                if (ORDERED) {
+                    const uint32_t k = atomicAdd(s.slot_cnt + post, 1u);
+                    if (k < kSlotCap)
+                        __stcg(s.slots + post * kSlotCap + k, make_uint4(ppos[u] | (c[u] & kKindBit), 0u,
+                                                                         __float_as_uint(w[u].x),
+                                                                         __float_as_uint(w[u].y)));
+                } else {
+                    atomicAdd(s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + post * s.j_es, w[u]);
                 }
             }
         }
@@ -979,9 +1061,16 @@ __global__ void k_scan_add(int64_t* out, int64_t n, const long long* __restrict_
 }
 
 // Fill the push CSR from the pull CSR (unordered within a row; sorted next).
+// Out-degree of every presynaptic neuron from the pull CSR (counts[N] zeroed).
+__global__ void k_count_outdeg(int64_t S, const uint32_t* __restrict__ pcol, uint32_t* counts)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < S) atomicAdd(counts + (pcol[e] & kIndexMask), 1u);
+}
+
 __global__ void k_fill_push(int64_t N, const int64_t* __restrict__ prow, const uint32_t* __restrict__ pcol,
                             const float2* __restrict__ pw, const int64_t* __restrict__ qrow, uint32_t* cursor,
-                            uint32_t* qcol, float2* qw)
+                            uint32_t* qcol, float2* qw, uint16_t* qpos)
 {
     const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -993,16 +1082,19 @@ __global__ void k_fill_push(int64_t N, const int64_t* __restrict__ prow, const u
         const int64_t d = qrow[src] + pos;
         qcol[d] = (uint32_t)i | (c & kKindBit);
         qw[d] = pw[e];
+        if (qpos) qpos[d] = (uint16_t)(e - prow[i]);
     }
 }
 
 // Sort every push row by postsynaptic index (warp per row, rows up to
 // kSortCap entries in shared memory; longer rows are flagged).
 constexpr int kSortCap = 2048;
+static_assert(kSortCap <= 2048, "the row slot takes 11 bits of the sort key");
 constexpr int kSortWarps = 4;
 
 __global__ void __launch_bounds__(kSortWarps * 32) k_sort_push_rows(int64_t N, const int64_t* __restrict__ qrow,
-                                                                    uint32_t* qcol, float2* qw, unsigned* too_long)
+                                                                    uint32_t* qcol, float2* qw, uint16_t* qpos,
+                                                                    unsigned* too_long)
 {
     extern __shared__ unsigned long long ssm[];
     const int lane = threadIdx.x & 31;
@@ -1013,9 +1105,12 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_push_rows(int64_t N, c
     const int64_t len = e1 - e0;
     if (len <= 1) return;
     if (len > kSortCap) { if (lane == 0) atomicAdd(too_long, 1u); return; }
-    // key = post << 32 | kind bit | original slot; posts are distinct in a row
+    // key = post << 32 | kind bit | pull-row position << 11 | slot: rows are ordered by
+    // (postsynaptic neuron, kind, position in its pull row), a deterministic order even
+    // when one pair of neurons has several synapses
     unsigned long long* key = ssm + (size_t)wid * kSortCap;
     float2* wtmp = reinterpret_cast<float2*>(ssm + (size_t)kSortWarps * kSortCap) + (size_t)wid * kSortCap;
+    uint16_t* ptmp = reinterpret_cast<uint16_t*>(ssm + (size_t)2 * kSortWarps * kSortCap) + (size_t)wid * kSortCap;
     int Kp = 1;
     while (Kp < len) Kp <<= 1;
     for (int k = lane; k < Kp; k += 32) {
@@ -1023,8 +1118,9 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_push_rows(int64_t N, c
         if (k < len) {
             const uint32_t c = qcol[e0 + k];
             kk = ((unsigned long long)(c & kIndexMask) << 32) | (unsigned long long)(c & kKindBit) |
-                 (unsigned long long)k;
+                 (qpos ? ((unsigned long long)qpos[e0 + k] << 11) : 0ull) | (unsigned long long)k;
             wtmp[k] = qw[e0 + k];
+            if (qpos) ptmp[k] = qpos[e0 + k];
         }
         key[k] = kk;
     }
@@ -1045,7 +1141,8 @@ __global__ void __launch_bounds__(kSortWarps * 32) k_sort_push_rows(int64_t N, c
     for (int k = lane; k < len; k += 32) {
         const unsigned long long kk = key[k];
         qcol[e0 + k] = (uint32_t)(kk >> 32) | (uint32_t)(kk & kKindBit);
-        qw[e0 + k] = wtmp[(int)(kk & 0x7fffffffull)];
+        qw[e0 + k] = wtmp[(int)(kk & 0x7ffull)];
+        if (qpos) qpos[e0 + k] = ptmp[(int)(kk & 0x7ffull)];
     }
 }
 

@@ -214,9 +214,15 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          DTB_MODE_AUTO pulls instead of pushing
  * DTB_TUNE_USE_GRAPHS      capture chunks in CUDA graphs (0/1)
  * DTB_TUNE_STEP_VARIANT    register budget of the step kernels: 0 = two
- *                          resident CTAs per SM (no spills), 1 = three */
+ *                          resident CTAs per SM (no spills), 1 = three
+ * DTB_TUNE_PULL_METHOD     how DTB_MODE_PULL propagates (bit-identical either
+ *                          way): 1 = every postsynaptic row gathers its firing
+ *                          inputs; 2 = ordered push: firing rows scatter into
+ *                          per-neuron slots that the next update sums in pull
+ *                          order (needs the push CSR); 0 = ordered push while
+ *                          at most 10 % of the neurons propagate, else rows */
 enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,
-       DTB_TUNE_STEP_VARIANT = 4 };
+       DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5 };
 int dtb_block_set_tuning(dtb_block* b, int key, int64_t value);
 int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value);
 

@@ -1,0 +1,73 @@
+"""Ordered push: DTB_MODE_PULL propagated by scattering firing rows into
+per-neuron slots summed in pull-row order must equal the row gather bit for
+bit (and hence models/block.py's torch.sparse.mm order)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from digital_twin_brain_b200 import Network, synthetic
+from digital_twin_brain_b200._lib import (FIELD_ACTIVE, FIELD_I_SYN, FIELD_J, FIELD_T_LAST, FIELD_V,
+                                          TUNE_PULL_METHOD)
+from tests._helpers import GOLDEN, decay_like_reference, unpack
+from tests.test_gpu_parity import class_decay_like_reference
+
+pytestmark = pytest.mark.gpu
+
+ROWS, SLOTS = 1, 2
+
+
+def _state(net):
+    return [net.get(f) for f in (FIELD_V, FIELD_J, FIELD_T_LAST, FIELD_I_SYN, FIELD_ACTIVE)]
+
+
+def test_ordered_push_matches_reference_golden():
+    g = np.load(os.path.join(GOLDEN, "single_block_2k.npz"))
+    spec = synthetic.config_single_block()
+    net = Network.from_spec(spec, device=0, build_push=True, class_decay=class_decay_like_reference(spec))
+    net.set_tuning(TUNE_PULL_METHOD, SLOTS)
+    every = int(g["v_every"])
+    act_ref = unpack(g["active"], spec.N)
+    for c in range(int(g["steps"]) // every):
+        s, m, na = net.run(every, noise_rate=0.01, mode="pull")
+        assert np.array_equal(s, g["sums"][c * every:(c + 1) * every])
+        assert np.array_equal(net.get(FIELD_V), g["V"][c])
+        assert np.array_equal(net.get(FIELD_ACTIVE).astype(bool), act_ref[(c + 1) * every - 1])
+    assert np.array_equal(net.get(FIELD_J), g["J_final"])
+    assert np.array_equal(net.get(FIELD_I_SYN), g["I_syn_final"])
+
+
+@pytest.mark.parametrize("rate,K", [(0.01, 100), (0.05, 200), (0.3, 60)],
+                         ids=["sparse", "overflowing_rows", "dense"])
+def test_ordered_push_equals_row_gather(rate, K):
+    """Rows with more than 8 contributions per step fall back to the warp gather inside the same kernel."""
+    spec = synthetic.whole_brain(R=6, mean_size=700, sigma=0.5, K=K, gen_seed=3, name=f"wb6_K{K}")
+    a = Network.from_spec(spec, device=0)
+    b = Network.from_spec(spec, device=0)
+    a.set_tuning(TUNE_PULL_METHOD, ROWS)
+    b.set_tuning(TUNE_PULL_METHOD, SLOTS)
+    for n in (1, 37, 64, 5):
+        sa, ma, na = a.run(n, noise_rate=rate, mode="pull")
+        sb, mb, nb = b.run(n, noise_rate=rate, mode="pull")
+        assert np.array_equal(sa, sb) and np.array_equal(na, nb)
+        np.testing.assert_array_equal(ma, mb)
+        for x, y in zip(_state(a), _state(b)):
+            assert np.array_equal(x, y)
+    assert na.sum() > 0
+
+
+def test_ordered_push_npz_positions_and_method_switches():
+    """Host-built CSRs (file order inside rows) carry the pull-row positions into the push CSR;
+    switching methods between runs keeps the state exact."""
+    d = os.path.join(GOLDEN, "small_blocks")
+    a = Network.from_npz(d, dt=0.1, seed=11, device=0)
+    b = Network.from_npz(d, dt=0.1, seed=11, device=0)
+    a.set_tuning(TUNE_PULL_METHOD, ROWS)
+    for k, n in enumerate((20, 33, 7, 40)):
+        b.set_tuning(TUNE_PULL_METHOD, SLOTS if k % 2 == 0 else ROWS)
+        sa, _, _ = a.run(n, noise_rate=0.02, mode="pull")
+        sb, _, _ = b.run(n, noise_rate=0.02, mode="pull")
+        assert np.array_equal(sa, sb)
+        for x, y in zip(_state(a), _state(b)):
+            assert np.array_equal(x, y)
