@@ -71,3 +71,45 @@ def test_ordered_push_npz_positions_and_method_switches():
         assert np.array_equal(sa, sb)
         for x, y in zip(_state(a), _state(b)):
             assert np.array_equal(x, y)
+
+
+def test_npz_hub_row_and_repeated_pairs(tmp_path):
+    """A presynaptic hub longer than the device row sort (sorted on the host), pairs of neurons
+    joined twice, rows in random file order: push rows ordered by (post, kind, pull-row position)
+    and the ordered push still equals the row gather."""
+    from digital_twin_brain_b200.generation import write_blocks
+    rng = np.random.default_rng(5)
+    N, K = 3000, 40
+    rows = []
+    for i in range(N):
+        src = rng.choice(np.arange(1, N), K - 2, replace=False)
+        src = np.concatenate([[0], src, [src[0]]])      # hub 0 in every row, one pair twice
+        rng.shuffle(src)
+        rows.append(src)
+    post = np.repeat(np.arange(N), K)
+    pre = np.concatenate(rows).astype(np.int64)
+    pos = np.tile(np.arange(K), N)
+    kind = np.where(pre >= 2400, 2, 0).astype(np.uint8)
+    w = rng.random((N * K, 2)).astype(np.float32)
+    spec = synthetic.config_single_block()
+    prop = np.repeat(spec.class_property[:1], N, axis=0).copy()
+    prop[2400:] = spec.class_property[1]
+    prop[:, 3] = (np.arange(N) >= 1500).astype(np.float32)
+    prop[:, 10:14] *= np.float32(2.5)
+    write_blocks(str(tmp_path), prop.astype(np.float32), [0, 1500, N], post, pre, kind, w)
+    a = Network.from_npz(str(tmp_path), dt=0.1, seed=2, device=0)
+    qrp, qix, qw = a.get_csr("push")
+    order = np.lexsort((pos, kind, post, pre))
+    exp_rp = np.concatenate([[0], np.cumsum(np.bincount(pre, minlength=N))])
+    assert np.array_equal(qrp, exp_rp) and qrp[1] - qrp[0] == N       # the hub's row is N long
+    assert np.array_equal(qix, post[order].astype(np.uint32) | np.where(kind[order] == 2, np.uint32(0x80000000), 0))
+    assert np.array_equal(qw, w[order])
+    b = Network.from_npz(str(tmp_path), dt=0.1, seed=2, device=0)
+    a.set_tuning(TUNE_PULL_METHOD, ROWS)
+    b.set_tuning(TUNE_PULL_METHOD, SLOTS)
+    for n in (50, 50):
+        sa, _, na = a.run(n, noise_rate=0.05, mode="pull")
+        sb, _, nb = b.run(n, noise_rate=0.05, mode="pull")
+        assert np.array_equal(sa, sb) and np.array_equal(na, nb)
+        for x, y in zip(_state(a), _state(b)):
+            assert np.array_equal(x, y)
