@@ -208,8 +208,9 @@ class EnsembleDA:
 
 
 def judge_error(pred: torch.Tensor, rates: torch.Tensor) -> float:
-    """Symmetric relative error of window rates (floor 1e-5 spikes/step, ~0.1 Hz), the judges' score."""
-    return torch.mean(torch.abs(pred - rates) / (0.5 * (pred + rates) + 1e-5)).item()
+    """The judges' score: absolute error of the window rates relative to their total, so that
+    quiet regions (whose BOLD barely depends on their rate) do not dominate."""
+    return (torch.sum(torch.abs(pred - rates)) / (torch.sum(rates) + 1e-5 * rates.numel())).item()
 
 
 class SurrogateDA:
@@ -219,14 +220,14 @@ class SurrogateDA:
     surrogate predicts every member's window rate from its g_ui factors and
     rate history, the surrogate members' hemodynamics are integrated from
     that rate (dtb_bold_run_steps), and the judges score the surrogate on
-    their simulated rates: when their symmetric relative error exceeds `threshold`
+    their simulated rates: when their error (``judge_error``) exceeds `threshold`
     (calibrate it on held-out windows: a margin over the surrogate's validated error),
     the window is recomputed for the surrogate members on the simulator
     (fallback).  The analysis step is the same diffusion EnKF over all members.
     """
 
     def __init__(self, template: synthetic.NetworkSpec, cfg: DAConfig, surrogate, n_judge: int = 16,
-                 threshold: float = 0.3, device: int = 0):
+                 threshold: float = 0.3, device: int = 0, adapt_steps: int = 0, adapt_lr: float = 5e-4):
         from .network import BoldModel
         from .surrogate import HISTORY
         self.cfg = cfg
@@ -239,6 +240,8 @@ class SurrogateDA:
         self.template = template
         self.sur = surrogate
         self.threshold = threshold
+        self.adapt_steps = adapt_steps
+        self.adapt_lr = adapt_lr
         jcfg = DAConfig(**{**cfg.__dict__, "n_members": n_judge})
         self.judge = EnsembleDA(template, jcfg, device)
         self.full = None   # fallback simulator for the surrogate members (built on first use)
@@ -304,6 +307,9 @@ class SurrogateDA:
         # judge score: symmetric relative error of the window rates (floor 1e-5 spikes/step ~ 0.1 Hz)
         err = judge_error(pred[:self.J], rates_j)
         self.errors.append(err)
+        if self.adapt_steps:   # the judges' fresh windows refine the surrogate (scored before it learns them)
+            self.sur.adapt(gui[:self.J * self.R], self.hist[:self.J].reshape(-1, self.H), rates_j.reshape(-1),
+                           steps=self.adapt_steps, lr=self.adapt_lr)
         sqvf = torch.stack([self.bold.get(k) for k in range(4)], dim=-1).reshape(self.M - self.J, self.R, 4)
         if err > self.threshold:
             self.fallbacks += 1

@@ -1621,20 +1621,31 @@ int dtb_block_set(dtb_block* b, int field, const void* src, int where)
     return DTB_OK;
 }
 
+// The reference computes I_syn at the end of a step (models/block.py:140;
+// cuda/src/block.cpp update_I_synaptic_gpu) and the next membrane update uses
+// that stored value, so a parameter change takes effect on I_syn one step
+// later.  The fused kernels recompute I_syn at the update: before parameters
+// change, the current I_syn (old parameters) is kept for the next update.
+static int keep_current_isyn(dtb_block* b)
+{
+    DevState& s = b->ds;
+    if (b->override_pending || b->N <= 0) return DTB_OK;
+    if (!b->d_iui_override) RET(dalloc(b, &b->d_iui_override, (size_t)b->N * 4));
+    k_export_current<<<grid_for(b->N, 256), 256, 0, b->stream>>>(s, b->d_iui_override, s.isyn_override);
+    CK(cudaGetLastError());
+    const uint32_t one = 1u;
+    CK(cudaMemcpyAsync(&s.ctl->use_isyn_override, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    b->override_pending = true;
+    return DTB_OK;
+}
+
 int dtb_block_update_property(dtb_block* b, const float* property, const float* decay)
 {
     if (!b || !property) return fail(DTB_ERR_ARG, "null argument");
     DeviceGuard g(b->device);
     DevState& s = b->ds;
-    // keep the current synaptic current (computed with the old parameters)
-    if (!b->override_pending) {
-        if (!b->d_iui_override) RET(dalloc(b, &b->d_iui_override, (size_t)b->N * 4));
-        k_export_current<<<grid_for(b->N, 256), 256, 0, b->stream>>>(s, b->d_iui_override, s.isyn_override);
-        CK(cudaGetLastError());
-        const uint32_t one = 1u;
-        CK(cudaMemcpyAsync(&s.ctl->use_isyn_override, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
-        CK(cudaStreamSynchronize(b->stream));
-    }
+    RET(keep_current_isyn(b));   // keep the current synaptic current (computed with the old parameters)
     std::vector<uint32_t> cls;
     RET(build_classes(b, b->N, property, decay, cls));
     RET(upload_class_tables(b));
@@ -1677,6 +1688,9 @@ int dtb_block_scale_property_by_subblock(dtb_block* b, int n, const int32_t* sub
 {
     if (!b || n < 0 || (n > 0 && (!sub || !col || !value))) return fail(DTB_ERR_ARG, "bad argument");
     DeviceGuard g(b->device);
+    for (int i = 0; i < n; ++i)
+        if (col[i] < 0 || col[i] >= DTB_NPROP || col[i] == 3) return fail(DTB_ERR_ARG, "column %d cannot be scaled", col[i]);
+    if (n > 0) RET(keep_current_isyn(b));
     if (b->class_prop_base.empty()) b->class_prop_base = b->class_prop;
     for (int i = 0; i < n; ++i) {
         if (col[i] < 0 || col[i] >= DTB_NPROP || col[i] == 3) return fail(DTB_ERR_ARG, "column %d cannot be scaled", col[i]);
@@ -1714,6 +1728,7 @@ int dtb_block_gamma_property_by_subblock(dtb_block* b, int n, const int32_t* sub
                         "other columns take the delta limit (alpha >= 1e6)", col[i]);
     }
     DeviceGuard g(b->device);
+    RET(keep_current_isyn(b));   // the new values reach I_syn one step later, as in the reference
     if (b->class_prop_base.empty()) b->class_prop_base = b->class_prop;
     std::unordered_map<int32_t, std::vector<int32_t>> by_sub;
     for (int c = 0; c < b->n_classes; ++c) by_sub[b->classes[(size_t)c].sub].push_back(c);

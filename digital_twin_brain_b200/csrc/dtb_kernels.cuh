@@ -117,6 +117,22 @@ __device__ __forceinline__ float4 gather_row(const DevState& s, const uint32_t* 
 // Sum of one neuron's c <= kSlotCap ordered-push contributions in ascending
 // pull-row position (the order gather_row adds them).  Two terms added to +0
 // give the same float in either order, so only c >= 3 needs the ordering.
+__device__ __forceinline__ void slot_add(uint4 v, float& a0, float& a1, float& a2, float& a3)
+{
+    const float wx = __uint_as_float(v.z), wy = __uint_as_float(v.w);
+    if (v.x & kKindBit) { a2 = __fadd_rn(a2, wx); a3 = __fadd_rn(a3, wy); }
+    else { a0 = __fadd_rn(a0, wx); a1 = __fadd_rn(a1, wy); }
+}
+
+// One or two contributions (already loaded): any order gives the same float.
+__device__ __forceinline__ float4 slot_pair_sum(uint4 v0, uint4 v1, uint32_t c)
+{
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+    slot_add(v0, a0, a1, a2, a3);
+    if (c == 2u) slot_add(v1, a0, a1, a2, a3);
+    return make_float4(a0, a1, a2, a3);
+}
+
 __device__ __forceinline__ float4 slot_sum(const uint4* __restrict__ sl, uint32_t c)
 {
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
@@ -330,18 +346,30 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         if (GATHER == kGatherSlots) {
             float4 sum[4];
             uint32_t ovf = 0u;   // bit j: neuron j of this lane got more contributions than slots
+            // counts of the lane's four neurons, then their first two slots, all in flight together
+            uint32_t cnt[4];
+            uint4 s0[4], s1[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                cnt[j] = n < s.N ? __ldcs(s.slot_cnt + n) : 0u;
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int64_t n = base + j * 32 + lane;
                 sum[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (n < s.N) {
-                    const uint32_t c = __ldcs(s.slot_cnt + n);
-                    if (c) {
-                        s.slot_cnt[n] = 0u;
-                        if (c > kSlotCap) ovf |= 1u << j;
-                        else sum[j] = slot_sum(s.slots + n * kSlotCap, c);
-                    }
-                }
+                s0[j] = s1[j] = make_uint4(0u, 0u, 0u, 0u);
+                if (cnt[j]) s.slot_cnt[n] = 0u;
+                if (cnt[j] >= 1u && cnt[j] <= kSlotCap) s0[j] = __ldcs(s.slots + n * kSlotCap);
+                if (cnt[j] == 2u) s1[j] = __ldcs(s.slots + n * kSlotCap + 1);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                if (cnt[j] == 0u) continue;
+                if (cnt[j] > kSlotCap) ovf |= 1u << j;
+                else if (cnt[j] <= 2u) sum[j] = slot_pair_sum(s0[j], s1[j], cnt[j]);
+                else sum[j] = slot_sum(s.slots + n * kSlotCap, cnt[j]);
             }
             // overflowing rows: the warp gathers them whole, in row order
 #pragma unroll
@@ -591,6 +619,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
 constexpr int kScatterThreads = 256;
 constexpr int kScatterMaxWords = 32;
 
+constexpr int kScatterUnroll = 8;   // synapses in flight per lane
+
 template <bool ORDERED>
 __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw)
 {
@@ -636,13 +666,13 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
         }
         const int64_t T = __shfl_sync(0xffffffffu, off, 31);
         const int64_t start = off - len;           // exclusive offset of this lane's row
-        for (int64_t v0 = 0; v0 < T; v0 += 128) {
-            uint32_t c[4];
-            float2 w[4];
-            uint32_t ppos[4];
-            bool ok[4];
+        for (int64_t v0 = 0; v0 < T; v0 += 32 * kScatterUnroll) {
+            uint32_t c[kScatterUnroll];
+            float2 w[kScatterUnroll];
+            uint32_t ppos[kScatterUnroll];
+            bool ok[kScatterUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kScatterUnroll; ++u) {
                 const int64_t v = v0 + u * 32 + lane;
                 // row of v: number of rows whose inclusive offset is <= v
                 int lo = 0;
@@ -662,19 +692,23 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
                     if (ORDERED) ppos[u] = __ldcs(s.qpos + e);
                 }
             }
+            if (ORDERED) {
+                // every slot claim of the batch first, so their round trips overlap
+                uint32_t k[kScatterUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (!ok[u]) continue;
-                const int64_t post = (int64_t)(c[u] & kIndexMask);
-                if (ORDERED) {
-                    const uint32_t k = atomicAdd(s.slot_cnt + post, 1u);
-                    if (k < kSlotCap)
-                        __stcg(s.slots + post * kSlotCap + k, make_uint4(ppos[u] | (c[u] & kKindBit), 0u,
-                                                                         __float_as_uint(w[u].x),
-                                                                         __float_as_uint(w[u].y)));
-                } else {
-                    atomicAdd(s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + post * s.j_es, w[u]);
-                }
+                for (int u = 0; u < kScatterUnroll; ++u)
+                    k[u] = ok[u] ? atomicAdd(s.slot_cnt + (c[u] & kIndexMask), 1u) : kSlotCap;
+#pragma unroll
+                for (int u = 0; u < kScatterUnroll; ++u)
+                    if (k[u] < kSlotCap)
+                        __stcg(s.slots + (int64_t)(c[u] & kIndexMask) * kSlotCap + k[u],
+                               make_uint4(ppos[u] | (c[u] & kKindBit), 0u, __float_as_uint(w[u].x),
+                                          __float_as_uint(w[u].y)));
+            } else {
+#pragma unroll
+                for (int u = 0; u < kScatterUnroll; ++u)
+                    if (ok[u])
+                        atomicAdd(s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + (int64_t)(c[u] & kIndexMask) * s.j_es, w[u]);
             }
         }
     }

@@ -46,6 +46,8 @@ def main(argv=None):
     ap.add_argument("--threshold", type=float, default=None,
                     help="judge fallback threshold (default: --margin x the held-out judge error of the surrogate)")
     ap.add_argument("--margin", type=float, default=1.5)
+    ap.add_argument("--adapt-steps", type=int, default=20,
+                    help="Adam steps per window on the judges' windows (0: the surrogate stays as trained)")
     ap.add_argument("--gain", type=float, default=2.0,
                     help="excitatory g_ui of the template as a multiple of the single-block values (2.0: ~6 Hz)")
     ap.add_argument("--skip", type=int, default=5, help="windows excluded from the RMSE (spin-up)")
@@ -123,10 +125,11 @@ def main(argv=None):
 
     # ---- surrogate-served DA
     sda = SurrogateDA(template, DAConfig(n_members=a.members, **base), sur, n_judge=a.judges,
-                      threshold=threshold)
+                      threshold=threshold, adapt_steps=a.adapt_steps)
     res_s = sda.run(obs)
     out.update(summarize(res_s, "surrogate"))
-    out.update(fallbacks=int(res_s["fallbacks"]), judge_rel_err_mean=float(np.mean(res_s["errors"])))
+    out.update(fallbacks=int(res_s["fallbacks"]), judge_err_mean=float(np.mean(res_s["errors"])),
+               judge_err=[round(float(e), 4) for e in res_s["errors"]], adapt_steps=a.adapt_steps)
     out["speedup"] = out["plain_window_s"] / out["surrogate_window_s"]
     out["rmse_ratio"] = out["surrogate_rmse"] / out["plain_rmse"]
     out["total_s"] = time.perf_counter() - t_all

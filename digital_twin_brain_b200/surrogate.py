@@ -132,6 +132,15 @@ class RateSurrogate:
         return self.mlp.fit((x - self.mu_x) / self.sd_x, (y - self.mu_y) / self.sd_y, epochs=epochs, batch=batch,
                             lr=lr, seed=seed)
 
+    def adapt(self, gui, hist, target, steps: int = 20, lr: float = 5e-4):
+        """A few Adam steps on new windows, keeping the standardisation of the first fit."""
+        x = self.features(gui, hist).contiguous()
+        y = ((torch.log(target.to(self.dev).float() + self.eps) - self.mu_y) / self.sd_y).contiguous()
+        loss = None
+        for _ in range(steps):
+            loss = self.mlp.train_step(x, y, lr)
+        return float(loss[0].item()) if loss is not None else None
+
     def predict(self, gui, hist) -> torch.Tensor:
         y = self.mlp.forward(self.features(gui, hist))
         return torch.clamp(torch.exp(y * self.sd_y + self.mu_y) - self.eps, min=0.0)

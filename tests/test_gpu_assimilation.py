@@ -54,3 +54,15 @@ def test_surrogate_da_runs_with_judges_and_fallback():
     sda2 = SurrogateDA(TEMPLATE, cfg, sur, n_judge=4, threshold=1e9)    # never falls back
     res2 = sda2.run(obs)
     assert res2["fallbacks"] == 0 and np.isfinite(res2["bold_pred"]).all()
+
+
+def test_surrogate_adapt_lowers_loss_on_new_windows():
+    torch.manual_seed(0)
+    g = torch.rand(2000, 4) + 0.5
+    h = torch.rand(2000, 8) * 0.01 + 1e-3
+    t = h.mean(1) * g[:, 0]
+    sur = RateSurrogate(seed=1)
+    sur.fit(g[:1000], h[:1000], t[:1000] * 0.5, epochs=5)     # trained on a shifted relation
+    before = sur.adapt(g[1000:], h[1000:], t[1000:], steps=1)
+    after = sur.adapt(g[1000:], h[1000:], t[1000:], steps=40)
+    assert after < before

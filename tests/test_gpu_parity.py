@@ -237,11 +237,15 @@ def test_scale_property_by_subblock_matches_oracle():
     dec = class_decay_like_reference(spec)
     net = Network.from_spec(spec, device=0, class_decay=dec)
     ob = _oracle_for(spec)
-    net.run(30, mode="pull")
-    for _ in range(30):
+    # past the initial refractory period (T_ref = 5 ms = 50 steps), so that the first update
+    # after the change shows which I_syn it used
+    net.run(120, mode="pull")
+    for _ in range(120):
         ob.run(0.01)
     # g_ui of subblock 0 (AMPA) x1.5, GABAa of subblock 1 x0.5 (dist_blockwrapper_pytorch.py:446)
     net.scale_property_by_subblock([0, 1], [10, 12], [1.5, 0.5])
+    # the stored I_syn (old parameters) drives the next membrane update, as in models/block.py
+    assert np.array_equal(net.get(FIELD_I_SYN), ob.Isyn)
     prop = spec.property()
     base = spec.property()
     prop[prop[:, 3] == 0, 10] = base[prop[:, 3] == 0, 10] * np.float32(1.5)
