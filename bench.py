@@ -37,6 +37,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "synaptic events/s & sim-s/wall-s at 2B syn; DA window time surrogate vs plain"
 UNIT = "events/s"
+# ncu DRAM traffic of the profile case (profiles/k_step_k_scatter_profile_case.md):
+# k_scatter<0> 188.3 MB for 2.162e6 events, k_step<0,1,0,2> 466.5 MB for 1.0552e7 neurons
+SCATTER_DRAM_BYTES_PER_EVENT = 188.275712e6 / 2162020.5
+UPDATE_DRAM_BYTES_PER_NEURON = 466.510592e6 / 10552023
 
 
 def parse():
@@ -168,6 +172,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
     import torch.distributed as dist
     from digital_twin_brain_b200 import Network, synthetic
+    from digital_twin_brain_b200._lib import TUNE_PULL_METHOD
 
     dev = local_rank
     torch.cuda.set_device(dev)
@@ -250,9 +255,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     evs = kt["events_per_step"]
     nact = evs / spec.K
     upd_bytes = N * (4 + 16 + 4 + 4) + N * (4 + 16) + 2 * N / 8          # V,J,t_last,class r; V,J w; 2 bitmasks
+    prop_bytes = N / 8 + 16 * nact + 12 * evs                              # bitmask, row pointers, (post, w) of rows
+    ordered = mode == "pull" and net.get_tuning(TUNE_PULL_METHOD) != 1 and kt["propagate_ms"] > 0 and \
+        nact / N <= 0.1
     if mode == "push":
-        prop_bytes = N / 8 + 16 * nact + 12 * evs                          # bitmask, row pointers, (post, w) of rows
         kernels = {"update": (kt["update_ms"], upd_bytes), "scatter": (kt["propagate_ms"], prop_bytes)}
+    elif ordered:
+        # ordered push: + pull-row positions, slot writes; the update reads counts and slots
+        kernels = {"slots+update": (kt["update_ms"], upd_bytes + 4 * N + 16 * evs),
+                   "ordered scatter": (kt["propagate_ms"], prop_bytes + 2 * evs + 16 * evs)}
     else:
         fused = upd_bytes + 8 * N + 4 * S + 8 * evs                        # + row ptrs, all indices, active weights
         kernels = {"gather+update": (kt["update_ms"], fused)}
@@ -266,8 +277,16 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = d_bytes / (d_ms * 1e-3) / 1e9 if d_ms > 0 else 0.0
     step_bytes = sum(b for _, b in kernels.values())
+    # DRAM bytes per launch from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the profile case
+    # (python -m digital_twin_brain_b200.profile_case: 1.06e7 neurons, 2.16e6 events per step), scaled by
+    # the units a launch processes: the scatter's traffic is one J sector read and written per event
+    traffic = None
+    if dom == "scatter":
+        traffic = SCATTER_DRAM_BYTES_PER_EVENT * evs
+    elif dom == "update":
+        traffic = UPDATE_DRAM_BYTES_PER_NEURON * N
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": dom, "algorithmic_bytes_per_launch": d_bytes, "launch_ms": d_ms,
+                "traffic": traffic, "kernel": dom, "algorithmic_bytes_per_launch": d_bytes, "launch_ms": d_ms,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
 
     cpu = None

@@ -250,7 +250,7 @@ class SurrogateDA:
         self.low = self.judge.low
         self.high = self.judge.high
         self.gen = torch.Generator(device=self.dev)
-        self.gen.manual_seed(cfg.seed + 1)
+        self.gen.manual_seed(cfg.seed)          # the same random walk and perturbations as EnsembleDA
         self.rng = np.random.default_rng(cfg.seed)
         self.hist = None   # [M, R, HISTORY] window rates
         self.H = HISTORY

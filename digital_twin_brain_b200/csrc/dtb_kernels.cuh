@@ -296,6 +296,52 @@ __global__ void k_samples(DevState s)
     s.samp_v[row * s.n_samples + i] = s.V[n];
 }
 
+// ------------------------------------------------------------ staged state loads
+// Bulk asynchronous copies (cp.async.bulk, the TMA engine; no multicast) of a
+// tile's V, t_last, class ids and both J planes into shared memory, issued by
+// lane 0 one tile ahead, so that the loads of tile k+1 are in flight while tile
+// k computes.  Completion is counted on a per-warp, per-buffer mbarrier.
+constexpr int kStageBytes = kWarpNeurons * (4 + 4 + 4 + 8 + 8);   // 3584 per tile buffer
+constexpr int kStagedSmem = (kStepThreads / 32) * 2 * kStageBytes;
+constexpr uint32_t kErrStageTimeout = 1u;                        // Ctl::err bit
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void stage_issue(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
+// Lane 0: the five copies of tile `base` into buffer `buf` (16-byte aligned, whole tile).
+__device__ __forceinline__ void stage_tile(const DevState& s, int64_t base, unsigned char* buf, uint32_t mbar)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier generic reads of buf first
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"((uint32_t)kStageBytes)
+                 : "memory");
+    const uint32_t d = smem_u32(buf);
+    stage_issue(d, s.V + base, kWarpNeurons * 4, mbar);
+    stage_issue(d + kWarpNeurons * 4, s.tlast + base, kWarpNeurons * 4, mbar);
+    stage_issue(d + kWarpNeurons * 8, s.cls + base, kWarpNeurons * 4, mbar);
+    stage_issue(d + kWarpNeurons * 12, s.J2 + base, kWarpNeurons * 8, mbar);
+    stage_issue(d + kWarpNeurons * 20, s.J2 + s.j_ps + base, kWarpNeurons * 8, mbar);
+}
+
+// Bounded wait for a buffer's copies; false after the limit (the caller then loads from global).
+__device__ __forceinline__ bool stage_wait(uint32_t mbar, uint32_t parity)
+{
+    for (uint32_t it = 0; it < (1u << 20); ++it) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
 // ------------------------------------------------------------ step kernel
 // Persistent: the grid is sized to the resident CTAs, and every warp streams a
 // contiguous run of 128-neuron tiles (tiles_per_warp of them).  In a tile a
@@ -305,10 +351,13 @@ __global__ void k_samples(DevState s)
 // subblock, so the CTA-wide barrier and the done-count happen once per CTA.
 // MINB = resident CTAs per SM the register budget is sized for (2: no spills,
 // 3: more warps, a few spills); the autotuner picks per network.
-template <int GATHER, bool UPDATE, bool FORCED, int MINB = 2>
+template <int GATHER, bool UPDATE, bool FORCED, int MINB = 2, bool STAGED = false>
 __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int tiles_per_warp)
 {
+    static_assert(!STAGED || GATHER == 0, "staged loads are for the update without gather");
     constexpr int kWarps = kStepThreads / 32;
+    extern __shared__ __align__(128) unsigned char stage_smem[];   // STAGED: [warp][2][kStageBytes]
+    __shared__ __align__(8) unsigned long long stage_bar[kWarps][2];
     __shared__ int sh_sub[kWarps];
     __shared__ uint32_t sh_spk[kWarps];
     __shared__ uint32_t sh_nact[kWarps];
@@ -340,9 +389,35 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     unsigned long long acc_ev = 0;
     bool flushed = false;
 
+    // STAGED: whole tiles are copied one ahead into two per-warp buffers (the J planes
+    // must start on 16 bytes: the host stages only split-plane layouts with even N)
+    unsigned char* my_stage = stage_smem + (size_t)wid * 2 * kStageBytes;
+    if (STAGED) {
+        if (lane == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&stage_bar[wid][0])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&stage_bar[wid][1])) : "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (tile0 < tile1 && (tile0 + 1) * kWarpNeurons <= s.N)
+                stage_tile(s, tile0 * kWarpNeurons, my_stage, smem_u32(&stage_bar[wid][0]));
+        }
+        __syncwarp();
+    }
+
     for (int64_t tile = tile0; tile < tile1; ++tile) {
         const int64_t base = tile * kWarpNeurons;
         float4 Jn[4];
+        const int it = (int)(tile - tile0);
+        const int sb = it & 1;
+        bool staged = false;   // this tile's state is in my_stage[sb]
+        if (STAGED) {
+            if (lane == 0 && tile + 1 < tile1 && (tile + 2) * kWarpNeurons <= s.N)
+                stage_tile(s, base + kWarpNeurons, my_stage + (sb ^ 1) * kStageBytes,
+                           smem_u32(&stage_bar[wid][sb ^ 1]));
+            if (base + kWarpNeurons <= s.N) {
+                staged = stage_wait(smem_u32(&stage_bar[wid][sb]), (uint32_t)((it >> 1) & 1));
+                if (!staged && lane == 0) atomicOr(&s.ctl->err, kErrStageTimeout);
+            }
+        }
         if (GATHER == kGatherSlots) {
             float4 sum[4];
             uint32_t ovf = 0u;   // bit j: neuron j of this lane got more contributions than slots
@@ -439,12 +514,24 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             valid[j] = n < s.N;
             c_in[j] = 0u;          // class 0 exists whenever N > 0: keeps the shuffle below in bounds
             if (valid[j]) {
-                v_in[j] = __ldcs(s.V + n);
-                tl_in[j] = __ldcs(s.tlast + n);
-                c_in[j] = __ldcs(s.cls + n);
-                if (!GATHER) J_in[j] = load_J(s, n);
+                if (STAGED && staged) {
+                    const unsigned char* bsm = my_stage + sb * kStageBytes;
+                    const int k = j * 32 + lane;
+                    v_in[j] = reinterpret_cast<const float*>(bsm)[k];
+                    tl_in[j] = reinterpret_cast<const float*>(bsm + kWarpNeurons * 4)[k];
+                    c_in[j] = reinterpret_cast<const uint32_t*>(bsm + kWarpNeurons * 8)[k];
+                    const float2 a = reinterpret_cast<const float2*>(bsm + kWarpNeurons * 12)[k];
+                    const float2 b2 = reinterpret_cast<const float2*>(bsm + kWarpNeurons * 20)[k];
+                    J_in[j] = make_float4(a.x, a.y, b2.x, b2.y);
+                } else {
+                    v_in[j] = __ldcs(s.V + n);
+                    tl_in[j] = __ldcs(s.tlast + n);
+                    c_in[j] = __ldcs(s.cls + n);
+                    if (!GATHER) J_in[j] = load_J(s, n);
+                }
             }
         }
+        if (STAGED) __syncwarp();   // every lane has read the buffer before lane 0 refills it
         // Noise words: counter {tile*32 + lane, stream, step}; inside an ensemble the
         // tile and stream are the member's own (members start on 128-neuron tiles),
         // so a member draws the same noise as when it is simulated alone.

@@ -52,6 +52,8 @@ def main(argv=None):
                     help="excitatory g_ui of the template as a multiple of the single-block values (2.0: ~6 Hz)")
     ap.add_argument("--skip", type=int, default=5, help="windows excluded from the RMSE (spin-up)")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--plain-seeds", type=int, default=2,
+                    help="plain runs with different DA seeds (their RMSE spread is the yardstick for the surrogate)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     dev = torch.device("cuda", 0)
@@ -92,12 +94,19 @@ def main(argv=None):
                windows=a.windows, steps_per_window=a.steps_per_window,
                neurons_per_member=template.N, synapses_per_member=template.S)
 
-    # ---- plain: every member on the simulator
-    plain = EnsembleDA(template, DAConfig(n_members=a.members, **base))
-    res_p = plain.run(obs)
-    out.update(summarize(res_p, "plain"))
-    del plain
-    torch.cuda.empty_cache()
+    # ---- plain: every member on the simulator (first seed = the surrogate run's seed)
+    plain_rmse = []
+    for k in range(max(1, a.plain_seeds)):
+        plain = EnsembleDA(template, DAConfig(n_members=a.members, **{**base, "seed": a.seed + 1000 * k}))
+        res_k = plain.run(obs)
+        sk = summarize(res_k, "plain")
+        plain_rmse.append(sk["plain_rmse"])
+        if k == 0:
+            res_p = res_k
+            out.update(sk)
+        del plain
+        torch.cuda.empty_cache()
+    out["plain_rmse_by_seed"] = plain_rmse
 
     # ---- surrogate training windows (a separate random-walk ensemble)
     t0 = time.perf_counter()
@@ -132,6 +141,14 @@ def main(argv=None):
                judge_err=[round(float(e), 4) for e in res_s["errors"]], adapt_steps=a.adapt_steps)
     out["speedup"] = out["plain_window_s"] / out["surrogate_window_s"]
     out["rmse_ratio"] = out["surrogate_rmse"] / out["plain_rmse"]
+    # windows served by the surrogate (no fallback), after the first
+    fb = np.array(res_s["errors"]) > threshold
+    ws = np.array(res_s["window_s"])
+    served = [w for i, w in enumerate(ws) if i > 0 and not fb[i]]
+    if served:
+        out["surrogate_served_window_s"] = float(np.mean(served))
+        out["speedup_served_windows"] = out["plain_window_s"] / out["surrogate_served_window_s"]
+    out["plain_rmse_seed_spread"] = float(np.max(plain_rmse) / np.min(plain_rmse) - 1.0) if len(plain_rmse) > 1 else None
     out["total_s"] = time.perf_counter() - t_all
     line = json.dumps(out)
     print(line)
