@@ -289,8 +289,10 @@ static int alloc_state(dtb_block* b)
     s.N = N;
     s.n_words = ((N + 127) / 128) * 4;
     RET(dalloc(b, &s.V, (size_t)N));
-    RET(dalloc(b, &s.J2, 2 * (size_t)N));
-    s.j_ps = N;   // split layout: excitatory pairs, then inhibitory pairs
+    // split receptor-pair planes, the second starting on a 128-neuron boundary (1 KB)
+    const int64_t jps = ((N + kWarpNeurons - 1) / kWarpNeurons) * kWarpNeurons;
+    RET(dalloc(b, &s.J2, 2 * (size_t)jps));
+    s.j_ps = jps;   // split layout: excitatory pairs, then inhibitory pairs
     s.j_es = 1;
     RET(dalloc(b, &s.tlast, (size_t)N));
     RET(dalloc(b, &s.isyn_override, (size_t)N));
@@ -299,7 +301,7 @@ static int alloc_state(dtb_block* b)
     RET(dalloc(b, &s.ctl, 1));
     RET(dalloc(b, &s.unmapped_nact, 1));
     RET(dalloc(b, &b->d_err, 4));
-    CK(cudaMemsetAsync(s.J2, 0, sizeof(float2) * 2 * (size_t)N, b->stream));
+    CK(cudaMemsetAsync(s.J2, 0, sizeof(float2) * 2 * (size_t)jps, b->stream));
     CK(cudaMemsetAsync(s.tlast, 0, sizeof(float) * (size_t)N, b->stream));
     for (int p = 0; p < 2; ++p) CK(cudaMemsetAsync(s.bits[p], 0, sizeof(uint32_t) * (size_t)s.n_words, b->stream));
     CK(cudaMemsetAsync(s.abits, 0, sizeof(uint32_t) * (size_t)s.n_words, b->stream));
@@ -549,7 +551,7 @@ static void launch_step_m(dtb_block* b, const DevState& s)
 }
 
 // Update with staged (bulk-copied, one tile ahead) state loads: split J planes
-// whose second plane starts on 16 bytes (even N).
+// whose second plane starts on 16 bytes (even plane stride).
 template <bool U, bool F>
 static void launch_step_staged(dtb_block* b, const DevState& s)
 {
@@ -565,7 +567,7 @@ static void launch_step_staged(dtb_block* b, const DevState& s)
     k_step<0, U, F, 2, true><<<grid, kStepThreads, kStagedSmem, b->stream>>>(s, tpw);
 }
 
-static bool staged_layout(const DevState& s) { return s.j_es == 1 && s.j_ps == s.N && (s.N % 2) == 0; }
+static bool staged_layout(const DevState& s) { return s.j_es == 1 && s.j_ps >= s.N && (s.j_ps % 2) == 0; }
 
 template <int G, bool U, bool F>
 static void launch_step(dtb_block* b, const DevState& s)
@@ -1900,7 +1902,8 @@ int dtb_block_save(dtb_block* b, const char* path)
     float t = 0.0f;
     CK(cudaStreamSynchronize(b->stream));
     CK(cudaMemcpy(V.data(), b->ds.V, 4 * N, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(J.data(), b->ds.J2, 16 * N, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(J.data(), b->ds.J2, 8 * N, cudaMemcpyDeviceToHost));                       // AMPA, NMDA plane
+    CK(cudaMemcpy(reinterpret_cast<float2*>(J.data()) + N, b->ds.J2 + b->ds.j_ps, 8 * N, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(T.data(), b->ds.tlast, 4 * N, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&t, &b->ds.ctl->t, 4, cudaMemcpyDeviceToHost));
     const uint32_t ov = b->override_pending ? 1u : 0u;
@@ -1943,7 +1946,8 @@ int dtb_block_load(dtb_block* b, const char* path)
     if (!ok) return fail(DTB_ERR_FORMAT, "truncated checkpoint %s", path);
     CK(cudaStreamSynchronize(b->stream));
     CK(cudaMemcpy(b->ds.V, V.data(), 4 * N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->ds.J2, J.data(), 16 * N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->ds.J2, J.data(), 8 * N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->ds.J2 + b->ds.j_ps, reinterpret_cast<const float2*>(J.data()) + N, 8 * N, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b->ds.tlast, T.data(), 4 * N, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(&b->ds.ctl->t, &t, 4, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(&b->ds.ctl->steps_done, &steps, 8, cudaMemcpyHostToDevice));

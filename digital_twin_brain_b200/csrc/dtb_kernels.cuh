@@ -389,8 +389,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     unsigned long long acc_ev = 0;
     bool flushed = false;
 
-    // STAGED: whole tiles are copied one ahead into two per-warp buffers (the J planes
-    // must start on 16 bytes: the host stages only split-plane layouts with even N)
+    // STAGED: whole tiles are copied one ahead into two per-warp buffers (the second J
+    // plane must start on 16 bytes: the host stages only split planes with an even stride)
     unsigned char* my_stage = stage_smem + (size_t)wid * 2 * kStageBytes;
     if (STAGED) {
         if (lane == 0) {

@@ -1,6 +1,6 @@
 """The update kernel with staged state loads (bulk copies one tile ahead into
 shared memory, DTB_TUNE_STEP_VARIANT = 2) computes exactly what the plain
-update computes, including a partial last tile and the odd-N fallback."""
+update computes, including a partial last tile and an odd neuron count."""
 import numpy as np
 import pytest
 
@@ -11,7 +11,7 @@ from digital_twin_brain_b200._lib import (FIELD_ACTIVE, FIELD_I_SYN, FIELD_J, FI
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("N", [3002, 3001, 128 * 40], ids=["partial_tile", "odd_fallback", "whole_tiles"])
+@pytest.mark.parametrize("N", [3002, 3001, 128 * 40], ids=["partial_tile", "odd_n", "whole_tiles"])
 def test_staged_update_equals_plain(N):
     spec = synthetic.single_block(N, 60, name=f"staged_{N}")
     nets = []
