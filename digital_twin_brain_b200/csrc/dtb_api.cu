@@ -551,20 +551,21 @@ static void launch_step_m(dtb_block* b, const DevState& s)
 }
 
 // Update with staged (bulk-copied, one tile ahead) state loads: split J planes
-// whose second plane starts on 16 bytes (even plane stride).
-template <bool U, bool F>
+// whose second plane starts on 16 bytes (even plane stride).  M = resident
+// CTAs per SM its registers are budgeted for.
+template <bool U, bool F, int M>
 static void launch_step_staged(dtb_block* b, const DevState& s)
 {
     static int per_sm = 0;
     if (!per_sm) {
-        cudaFuncSetAttribute(k_step<0, U, F, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<0, U, F, 2, true>, kStepThreads, kStagedSmem);
+        cudaFuncSetAttribute(k_step<0, U, F, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<0, U, F, M, true>, kStepThreads, kStagedSmem);
         if (per_sm < 1) per_sm = 1;
     }
     unsigned grid;
     int tpw;
     step_grid(b, per_sm, grid, tpw);
-    k_step<0, U, F, 2, true><<<grid, kStepThreads, kStagedSmem, b->stream>>>(s, tpw);
+    k_step<0, U, F, M, true><<<grid, kStepThreads, kStagedSmem, b->stream>>>(s, tpw);
 }
 
 static bool staged_layout(const DevState& s) { return s.j_es == 1 && s.j_ps >= s.N && (s.j_ps % 2) == 0; }
@@ -573,7 +574,8 @@ template <int G, bool U, bool F>
 static void launch_step(dtb_block* b, const DevState& s)
 {
     if constexpr (G == 0) {
-        if (b->step_variant == 2 && staged_layout(s)) { launch_step_staged<U, F>(b, s); return; }
+        if (b->step_variant == 2 && staged_layout(s)) { launch_step_staged<U, F, 2>(b, s); return; }
+        if (b->step_variant == 3 && staged_layout(s)) { launch_step_staged<U, F, 3>(b, s); return; }
     }
     if (b->step_variant == 1) launch_step_m<G, U, F, 3>(b, s);
     else launch_step_m<G, U, F, 2>(b, s);
@@ -1434,7 +1436,7 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         break;
     case DTB_TUNE_USE_GRAPHS: b->use_graphs = value != 0; break;
     case DTB_TUNE_STEP_VARIANT:
-        if (value < 0 || value > 2) return fail(DTB_ERR_ARG, "step variant must be 0, 1 or 2");
+        if (value < 0 || value > 3) return fail(DTB_ERR_ARG, "step variant must be 0..3");
         b->step_variant = (int)value;
         break;
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
@@ -1467,8 +1469,8 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
         const int mode = b->has_push ? DTB_MODE_PUSH : DTB_MODE_PULL;
         float best_u = 1e30f;
         int best_v = 0;
-        for (int v = 0; v < 3; ++v) {
-            if (v == 2 && !staged_layout(b->ds)) continue;
+        for (int v = 0; v < 4; ++v) {
+            if (v >= 2 && !staged_layout(b->ds)) continue;
             b->step_variant = v;
             float o[4];
             RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, mode, o));

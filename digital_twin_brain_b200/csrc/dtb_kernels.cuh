@@ -418,6 +418,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 if (!staged && lane == 0) atomicOr(&s.ctl->err, kErrStageTimeout);
             }
         }
+        unsigned char* stage_buf = my_stage + sb * kStageBytes;
         if (GATHER == kGatherSlots) {
             float4 sum[4];
             uint32_t ovf = 0u;   // bit j: neuron j of this lane got more contributions than slots
@@ -514,15 +515,17 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             valid[j] = n < s.N;
             c_in[j] = 0u;          // class 0 exists whenever N > 0: keeps the shuffle below in bounds
             if (valid[j]) {
-                if (STAGED && staged) {
-                    const unsigned char* bsm = my_stage + sb * kStageBytes;
-                    const int k = j * 32 + lane;
-                    v_in[j] = reinterpret_cast<const float*>(bsm)[k];
-                    tl_in[j] = reinterpret_cast<const float*>(bsm + kWarpNeurons * 4)[k];
-                    c_in[j] = reinterpret_cast<const uint32_t*>(bsm + kWarpNeurons * 8)[k];
-                    const float2 a = reinterpret_cast<const float2*>(bsm + kWarpNeurons * 12)[k];
-                    const float2 b2 = reinterpret_cast<const float2*>(bsm + kWarpNeurons * 20)[k];
-                    J_in[j] = make_float4(a.x, a.y, b2.x, b2.y);
+                if (STAGED) {
+                    // the tile's state lives in the stage buffer: the copies' (or, for a
+                    // partial tile, this lane's own loads, written below)
+                    if (!staged) {
+                        const int k = j * 32 + lane;
+                        reinterpret_cast<float*>(stage_buf)[k] = __ldcs(s.V + n);
+                        reinterpret_cast<float*>(stage_buf + kWarpNeurons * 4)[k] = __ldcs(s.tlast + n);
+                        reinterpret_cast<uint32_t*>(stage_buf + kWarpNeurons * 8)[k] = __ldcs(s.cls + n);
+                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 12)[k] = __ldcs(s.J2 + n);
+                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 20)[k] = __ldcs(s.J2 + s.j_ps + n);
+                    }
                 } else {
                     v_in[j] = __ldcs(s.V + n);
                     tl_in[j] = __ldcs(s.tlast + n);
@@ -531,7 +534,11 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 }
             }
         }
-        if (STAGED) __syncwarp();   // every lane has read the buffer before lane 0 refills it
+        if (STAGED) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                c_in[j] = valid[j] ? reinterpret_cast<const uint32_t*>(stage_buf + kWarpNeurons * 8)[j * 32 + lane] : 0u;
+        }
         // Noise words: counter {tile*32 + lane, stream, step}; inside an ensemble the
         // tile and stream are the member's own (members start on 128-neuron tiles),
         // so a member draws the same noise as when it is simulated alone.
@@ -561,8 +568,20 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         uint32_t ev_lane = 0;
         auto neuron = [&](int j, const ParamClass& p) {
             const int64_t n = base + j * 32 + lane;
-            const float v = v_in[j];
-            const float4 J = GATHER ? Jn[j] : J_in[j];
+            float v, tl;
+            float4 J;
+            if (STAGED) {
+                const int k = j * 32 + lane;
+                v = reinterpret_cast<const float*>(stage_buf)[k];
+                tl = reinterpret_cast<const float*>(stage_buf + kWarpNeurons * 4)[k];
+                const float2 a = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 12)[k];
+                const float2 b2 = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 20)[k];
+                J = make_float4(a.x, a.y, b2.x, b2.y);
+            } else {
+                v = v_in[j];
+                tl = tl_in[j];
+                J = GATHER ? Jn[j] : J_in[j];
+            }
             float isyn;
             if (use_override) isyn = s.isyn_override[n];
             else if (s.gnrn) isyn = isyn_g(mul4(p.g, __ldcs(s.gnrn + n)), p.Vu, v, J);   // gamma-distributed g_ui
@@ -570,7 +589,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             const float mainp = __fmul_rn(-p.gL, __fsub_rn(v, p.VL));
             const float cd = __fadd_rn(__fadd_rn(mainp, isyn), p.Iext);
             const float vn = __fadd_rn(v, __fmul_rn(p.rCdt, cd));
-            const bool notsat = t >= __fadd_rn(tl_in[j], p.Tref);
+            const bool notsat = t >= __fadd_rn(tl, p.Tref);
             const float vs = notsat ? vn : p.Vreset;
             bool a = vs >= p.Vth;
             const float vmin = isnan(vs) ? vs : (isnan(p.Vth) ? p.Vth : (vs < p.Vth ? vs : p.Vth));
@@ -654,6 +673,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             }
             __threadfence();   // this lane's atomics before the CTA's done-count
         }
+        if (STAGED) __syncwarp();   // every lane is done with the buffer before lane 0 refills it
     }
     if (flushed) __threadfence();
 

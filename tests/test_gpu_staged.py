@@ -11,11 +11,12 @@ from digital_twin_brain_b200._lib import (FIELD_ACTIVE, FIELD_I_SYN, FIELD_J, FI
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("variant", [2, 3])
 @pytest.mark.parametrize("N", [3002, 3001, 128 * 40], ids=["partial_tile", "odd_n", "whole_tiles"])
-def test_staged_update_equals_plain(N):
+def test_staged_update_equals_plain(N, variant):
     spec = synthetic.single_block(N, 60, name=f"staged_{N}")
     nets = []
-    for variant in (0, 2):
+    for variant in (0, variant):
         net = Network.from_spec(spec, device=0)
         net.set_tuning(TUNE_STEP_VARIANT, variant)
         net.set_tuning(TUNE_CHUNK, 1)            # every step starts with the plain (gather-free) update
