@@ -37,10 +37,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "synaptic events/s & sim-s/wall-s at 2B syn; DA window time surrogate vs plain"
 UNIT = "events/s"
-# ncu DRAM traffic of the profile case (profiles/k_step_k_scatter_profile_case.md):
-# k_scatter<0> 188.3 MB for 2.162e6 events, k_step<0,1,0,2> 466.5 MB for 1.0552e7 neurons
-SCATTER_DRAM_BYTES_PER_EVENT = 188.275712e6 / 2162020.5
-UPDATE_DRAM_BYTES_PER_NEURON = 466.510592e6 / 10552023
+# ncu DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, one pass each) of the whole-brain
+# workload itself (profiles/whole_brain_dram_traffic.md): k_scatter<0> 1.303 GB per launch for
+# 2.346e7 events, staged update 1.108 GB per launch for 2.345e7 neurons
+SCATTER_DRAM_BYTES_PER_EVENT = (943.26e6 + 360.44e6) / 23462598
+UPDATE_DRAM_BYTES_PER_NEURON = (688.37e6 + 419.80e6) / 23448955
 
 
 def parse():
@@ -277,9 +278,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = d_bytes / (d_ms * 1e-3) / 1e9 if d_ms > 0 else 0.0
     step_bytes = sum(b for _, b in kernels.values())
-    # DRAM bytes per launch from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the profile case
-    # (python -m digital_twin_brain_b200.profile_case: 1.06e7 neurons, 2.16e6 events per step), scaled by
-    # the units a launch processes: the scatter's traffic is one J sector read and written per event
+    # DRAM bytes per launch measured by ncu on this workload, per unit processed (events, neurons)
     traffic = None
     if dom == "scatter":
         traffic = SCATTER_DRAM_BYTES_PER_EVENT * evs
