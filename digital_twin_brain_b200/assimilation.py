@@ -272,13 +272,25 @@ class SurrogateDA:
     def hp(self):
         return sigmoid_torch(self.hp_log, self.low, self.high)
 
-    def burn_in(self, steps: int | None = None):
-        """One judge window to seed every member's rate history with the judges' regional mean."""
+    def burn_in(self, windows: int = 1, steps: int | None = None):
+        """`windows` judge windows before the assimilation seed the rate histories: the judges'
+        own, and the judges' regional mean for every other member.  With adaptation on, the
+        surrogate also learns from each of these windows."""
         self.judge.hp_log = self.hp_log[:self.J].clone()
         self.judge.apply_hp()
-        self.judge.evolve(steps)
-        r = torch.from_numpy(self.judge.window_rates()).to(self.dev).float().mean(0)       # [R]
-        self.hist = r.reshape(1, self.R, 1).repeat(self.M, 1, self.H)
+        gui = self.hp.reshape(self.M, self.R, self.n_hp)[:self.J].reshape(-1, self.n_hp)
+        jh = None
+        for _ in range(max(1, windows)):
+            self.judge.evolve(steps)
+            r = torch.from_numpy(self.judge.window_rates()).to(self.dev).float()      # [J, R]
+            if jh is not None and self.adapt_steps:
+                h = torch.cat([jh[:, :, :1].repeat(1, 1, self.H - jh.shape[2]), jh], 2) if jh.shape[2] < self.H else jh
+                self.sur.adapt(gui, h.reshape(-1, self.H), r.reshape(-1), steps=self.adapt_steps, lr=self.adapt_lr)
+            jh = r[:, :, None] if jh is None else torch.cat([jh, r[:, :, None]], 2)[:, :, -self.H:]
+        if jh.shape[2] < self.H:
+            jh = torch.cat([jh[:, :, :1].repeat(1, 1, self.H - jh.shape[2]), jh], 2)
+        self.hist = jh.mean(0, keepdim=True).repeat(self.M, 1, 1)
+        self.hist[:self.J] = jh
 
     def _fallback(self, hp_s: torch.Tensor, bold_sqvf: torch.Tensor):
         if self.full is None:

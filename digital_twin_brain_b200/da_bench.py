@@ -46,6 +46,8 @@ def main(argv=None):
     ap.add_argument("--threshold", type=float, default=None,
                     help="judge fallback threshold (default: --margin x the held-out judge error of the surrogate)")
     ap.add_argument("--margin", type=float, default=1.5)
+    ap.add_argument("--burn-in-windows", type=int, default=8,
+                    help="judge windows before the assimilation (histories, surrogate adaptation); timed")
     ap.add_argument("--adapt-steps", type=int, default=20,
                     help="Adam steps per window on the judges' windows (0: the surrogate stays as trained)")
     ap.add_argument("--gain", type=float, default=2.0,
@@ -135,10 +137,21 @@ def main(argv=None):
     # ---- surrogate-served DA
     sda = SurrogateDA(template, DAConfig(n_members=a.members, **base), sur, n_judge=a.judges,
                       threshold=threshold, adapt_steps=a.adapt_steps)
+    sda.hp_random_initialize()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    sda.burn_in(a.burn_in_windows)
+    torch.cuda.synchronize(dev)
+    t_burn = time.perf_counter() - t0
     res_s = sda.run(obs)
     out.update(summarize(res_s, "surrogate"))
     out.update(fallbacks=int(res_s["fallbacks"]), judge_err_mean=float(np.mean(res_s["errors"])),
                judge_err=[round(float(e), 4) for e in res_s["errors"]], adapt_steps=a.adapt_steps)
+    out["surrogate_burn_in_s"] = t_burn
+    out["burn_in_windows"] = a.burn_in_windows
+    out["plain_total_s"] = float(np.sum(res_p["window_s"]))
+    out["surrogate_total_s"] = float(np.sum(res_s["window_s"])) + t_burn
+    out["speedup_total"] = out["plain_total_s"] / out["surrogate_total_s"]
     out["speedup"] = out["plain_window_s"] / out["surrogate_window_s"]
     out["rmse_ratio"] = out["surrogate_rmse"] / out["plain_rmse"]
     # windows served by the surrogate (no fallback), after the first
