@@ -161,7 +161,6 @@ struct dtb_block {
     double pull_threshold = 0.05;
     int chunk = 32;
     int scatter_wpw = 32;         // bitmask words per warp in the push scatter
-    int scatter_mode = 0;         // 0: scan the bitmask, 1: read the update's active-row queue
     int step_variant = 0;         // 0: 2 resident CTAs/SM register budget, 1: 3
     // ordered push (bit-exact pull through per-neuron slots)
     bool has_qpos = false;
@@ -454,14 +453,6 @@ static int rebuild_groups(dtb_block* b, const int32_t* sub_to_region);
 
 static int finish_create(dtb_block* b)
 {
-    if (b->has_push && b->N > 0) {   // active-row queues for the queue scatter
-        DevState& s = b->ds;
-        RET(dalloc(b, &s.aq[0], (size_t)b->N));
-        RET(dalloc(b, &s.aq[1], (size_t)b->N));
-        RET(dalloc(b, &s.aq_cnt, 2));
-        CK(cudaMemsetAsync(s.aq_cnt, 0, 2 * sizeof(uint32_t), b->stream));
-        s.aq_on = b->scatter_mode;
-    }
     RET(rebuild_groups(b, nullptr));
     CK(cudaMallocHost((void**)&b->h_run, sizeof(RunParams)));
     RET(ensure_stats(b, 256));
@@ -646,21 +637,6 @@ static int launch_gather_only(dtb_block* b, const DevState& s, int gather = kGat
 
 static int launch_scatter(dtb_block* b, const DevState& s, bool ordered = false)
 {
-    if (s.aq_on) {   // persistent grid over the queue
-        static int per_sm[2] = {0, 0};
-        int& ps = per_sm[ordered ? 1 : 0];
-        if (!ps) {
-            if (ordered) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_scatter_queue<true>, kScatterThreads, 0);
-            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_scatter_queue<false>, kScatterThreads, 0);
-            if (ps < 1) ps = 1;
-        }
-        const unsigned grid = (unsigned)(std::max(1, b->n_sm) * ps);
-        if (ordered) k_scatter_queue<true><<<grid, kScatterThreads, 0, b->stream>>>(s);
-        else k_scatter_queue<false><<<grid, kScatterThreads, 0, b->stream>>>(s);
-        CK(cudaGetLastError());
-        b->launches++;
-        return DTB_OK;
-    }
     const int wpw = b->scatter_wpw;
     const int64_t warps = (s.n_words + wpw - 1) / wpw;
     const unsigned grid = grid_for(warps * 32, kScatterThreads);
@@ -1445,12 +1421,6 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         if (value < 1 || value > 32) return fail(DTB_ERR_ARG, "scatter words per warp must be 1..32");
         b->scatter_wpw = (int)value;
         break;
-    case DTB_TUNE_SCATTER_MODE:
-        if (value < 0 || value > 1) return fail(DTB_ERR_ARG, "scatter mode must be 0 (bitmask) or 1 (queue)");
-        if (value == 1 && !b->ds.aq_cnt) return fail(DTB_ERR_STATE, "the queue scatter needs the push CSR");
-        b->scatter_mode = (int)value;
-        b->ds.aq_on = (int)value;
-        break;
     case DTB_TUNE_PULL_METHOD:
         if (value < 0 || value > 2) return fail(DTB_ERR_ARG, "pull method must be 0 (auto), 1 (rows) or 2 (ordered push)");
         if (value == 2 && !b->has_qpos) return fail(DTB_ERR_STATE, "ordered push needs the push CSR with pull-row positions");
@@ -1485,7 +1455,6 @@ int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value)
     case DTB_TUNE_USE_GRAPHS: *value = b->use_graphs ? 1 : 0; break;
     case DTB_TUNE_STEP_VARIANT: *value = b->step_variant; break;
     case DTB_TUNE_PULL_METHOD: *value = b->pull_method; break;
-    case DTB_TUNE_SCATTER_MODE: *value = b->scatter_mode; break;
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
     }
     return DTB_OK;
@@ -1518,14 +1487,6 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
             if (o[2] < best_ms) { best_ms = o[2]; best_w = w; ev = o[3]; }
         }
         b->scatter_wpw = best_w;
-        if (b->ds.aq_cnt) {   // the queue scatter against the best bitmask width
-            const int keep = b->scatter_mode;
-            b->scatter_mode = 1; b->ds.aq_on = 1;
-            float o[4];
-            RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PUSH, o));
-            if (o[2] < best_ms) { best_ms = o[2]; ev = o[3]; }
-            else { b->scatter_mode = keep == 1 ? 0 : keep; b->ds.aq_on = b->scatter_mode; }
-        }
         push_ms = best_ms;
     }
     if (b->has_pull) {

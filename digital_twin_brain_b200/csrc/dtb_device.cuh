@@ -20,7 +20,6 @@ constexpr uint32_t kKindBit = 0x80000000u;
 constexpr uint32_t kIndexMask = 0x7fffffffu;
 constexpr int kWarpNeurons = 128;      // neurons owned by one warp in the step kernels
 constexpr uint32_t kSlotCap = 8;       // ordered-push contributions kept per neuron and step
-constexpr int kQueueBuf = 256;         // per-warp buffer of queued rows in the update kernel
 constexpr int kGatherRows = 1;         // k_step gathers whole pull rows
 constexpr int kGatherSlots = 2;        // k_step sums its ordered-push slots
 constexpr int kStepThreads = 256;      // 8 warps, 1024 neurons per CTA
@@ -110,11 +109,6 @@ struct DevState {
     // push CSR
     const int64_t* qrow; const uint32_t* qcol; const float2* qw;
     const uint16_t* qpos;       // [S] position of every push entry inside its pull row (nullable)
-    // active-row queue: the update appends every propagating neuron (any order), the
-    // queue scatter reads it instead of scanning the bitmask
-    int aq_on;
-    uint32_t* aq[2];            // [N] by step parity
-    uint32_t* aq_cnt;           // [2] entries of each queue
     // ordered push (bit-exact pull order at push cost): pending contributions per neuron
     uint32_t* slot_cnt;         // [N] contributions written since the neuron last consumed them
     uint4* slots;               // [N][kSlotCap] {pull-row position | kind bit, 0, w.x bits, w.y bits}

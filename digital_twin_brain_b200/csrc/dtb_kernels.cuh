@@ -189,8 +189,6 @@ __device__ void step_epilogue(const DevState& s, unsigned long long steps_done, 
     Ctl* ctl = s.ctl;
     const unsigned long long row = steps_done - ctl->run_base;
     const bool write = row < (unsigned long long)ctl->stats_cap;
-    // the next update appends to the other queue, whose scatter has finished
-    if (threadIdx.x == 0 && s.aq_cnt) s.aq_cnt[(steps_done + 1ull) & 1ull] = 0u;
     if (s.stats_ext) {   // k_stats folds the statistics right after this kernel
         if (threadIdx.x == 0) {
             if (write) s.st_nact[row] = atomicExch(s.unmapped_nact, 0u);
@@ -360,7 +358,6 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     constexpr int kWarps = kStepThreads / 32;
     extern __shared__ __align__(128) unsigned char stage_smem[];   // STAGED: [warp][2][kStageBytes]
     __shared__ __align__(8) unsigned long long stage_bar[kWarps][2];
-    __shared__ uint32_t qbuf[kWarps][kQueueBuf];   // rows this warp queues, flushed in runs
     __shared__ int sh_sub[kWarps];
     __shared__ uint32_t sh_spk[kWarps];
     __shared__ uint32_t sh_nact[kWarps];
@@ -391,17 +388,6 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     double acc_v = 0.0;
     unsigned long long acc_ev = 0;
     bool flushed = false;
-    int qn = 0;                                    // entries in qbuf[wid] (warp-uniform)
-    const uint32_t qpar = (uint32_t)(steps_done & 1ull);
-    auto queue_flush = [&]() {
-        __syncwarp();
-        uint32_t qb = 0;
-        if (lane == 0 && qn) qb = atomicAdd(s.aq_cnt + qpar, (uint32_t)qn);
-        qb = __shfl_sync(0xffffffffu, qb, 0);
-        for (int i = lane; i < qn; i += 32) s.aq[qpar][qb + i] = qbuf[wid][i];
-        __syncwarp();
-        qn = 0;
-    };
 
     // STAGED: whole tiles are copied one ahead into two per-warp buffers (the second J
     // plane must start on 16 bytes: the host stages only split planes with an even stride)
@@ -654,21 +640,6 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             cnt_spk += __popc(ma);
             cnt_nact += __popc(mn);
         }
-        if (s.aq_on && cnt_nact) {   // queue this tile's propagating neurons
-            if (qn + (int)cnt_nact > kQueueBuf) queue_flush();
-            const int mine = __popc(nav_m);
-            int incl = mine;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            int at = qn + incl - mine;
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if ((nav_m >> j) & 1u) qbuf[wid][at++] = (uint32_t)(base + j * 32 + lane);
-            qn += (int)cnt_nact;
-        }
 
         // ---- per-subblock statistics
         const int sub0 = __shfl_sync(0xffffffffu, mysub0, 0);
@@ -704,7 +675,6 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         }
         if (STAGED) __syncwarp();   // every lane is done with the buffer before lane 0 refills it
     }
-    if (s.aq_on && qn) queue_flush();
     if (flushed) __threadfence();
 
     // ---- CTA merge: one barrier, one set of atomics, one done-count per CTA
@@ -758,13 +728,34 @@ constexpr int kScatterMaxWords = 32;
 
 constexpr int kScatterUnroll = 8;   // synapses in flight per lane
 
-// Scatters the outgoing rows of `total` propagating neurons rows[0..total) (32 rows
-// at a time: a scan of their lengths spreads their synapses over the lanes, 8 per
-// lane in flight) into the pending J (float2 atomics) or, ORDERED, into the
-// per-neuron slots of the ordered push.
 template <bool ORDERED>
-__device__ __forceinline__ void scatter_rows(const DevState& s, const uint32_t* rows, int total, int lane)
+__global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw)
 {
+    __shared__ uint32_t sh_rows[kScatterThreads / 32][kScatterMaxWords * 32];
+    const unsigned long long steps_done = s.ctl->steps_done;
+    const uint32_t* __restrict__ bits = s.bits[(steps_done - 1ull) & 1ull];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t w0 = warp_global * wpw;
+    uint32_t* rows = sh_rows[wid];
+    uint32_t word = (lane < wpw && w0 + lane < s.n_words) ? __ldcs(bits + w0 + lane) : 0u;
+    // list the set bits of the window in neuron order
+    const int cnt = __popc(word);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    int pos = incl - cnt;
+    while (word) {
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        rows[pos++] = (uint32_t)((w0 + lane) * 32 + b);
+    }
+    __syncwarp();
     for (int r0 = 0; r0 < total; r0 += 32) {
         const bool has = r0 + lane < total;
         int64_t e0 = 0, len = 0;
@@ -827,55 +818,6 @@ __device__ __forceinline__ void scatter_rows(const DevState& s, const uint32_t* 
                         atomicAdd(s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + (int64_t)(c[u] & kIndexMask) * s.j_es, w[u]);
             }
         }
-    }
-}
-
-template <bool ORDERED>
-__global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw)
-{
-    __shared__ uint32_t sh_rows[kScatterThreads / 32][kScatterMaxWords * 32];
-    const unsigned long long steps_done = s.ctl->steps_done;
-    const uint32_t* __restrict__ bits = s.bits[(steps_done - 1ull) & 1ull];
-    const int lane = threadIdx.x & 31;
-    const int wid = threadIdx.x >> 5;
-    const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t w0 = warp_global * wpw;
-    uint32_t* rows = sh_rows[wid];
-    uint32_t word = (lane < wpw && w0 + lane < s.n_words) ? __ldcs(bits + w0 + lane) : 0u;
-    // list the set bits of the window in neuron order
-    const int cnt = __popc(word);
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    int pos = incl - cnt;
-    while (word) {
-        const int b = __ffs(word) - 1;
-        word &= word - 1;
-        rows[pos++] = (uint32_t)((w0 + lane) * 32 + b);
-    }
-    __syncwarp();
-    scatter_rows<ORDERED>(s, rows, total, lane);
-}
-
-// Push from the active-row queue the update filled: a persistent grid, every warp
-// takes batches of 32 queued rows (no bitmask scan, no idle warps).
-template <bool ORDERED>
-__global__ void __launch_bounds__(kScatterThreads) k_scatter_queue(DevState s)
-{
-    const unsigned long long steps_done = s.ctl->steps_done;
-    const uint32_t par = (uint32_t)((steps_done - 1ull) & 1ull);
-    const int64_t count = (int64_t)s.aq_cnt[par];
-    const uint32_t* __restrict__ q = s.aq[par];
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b * 32 < count; b += warps) {
-        const int64_t r0 = b * 32;
-        const int total = (int)(count - r0 < 32 ? count - r0 : 32);
-        scatter_rows<ORDERED>(s, q + r0, total, lane);
     }
 }
 

@@ -38,19 +38,15 @@ def test_ordered_push_matches_reference_golden():
     assert np.array_equal(net.get(FIELD_I_SYN), g["I_syn_final"])
 
 
-@pytest.mark.parametrize("queue", [0, 1], ids=["bitmask_scan", "row_queue"])
 @pytest.mark.parametrize("rate,K", [(0.01, 100), (0.05, 200), (0.3, 60)],
                          ids=["sparse", "overflowing_rows", "dense"])
-def test_ordered_push_equals_row_gather(rate, K, queue):
-    """Rows with more than 8 contributions per step fall back to the warp gather inside the same kernel;
-    the ordered scatter finds the firing rows by scanning the bitmask or from the update's queue."""
-    from digital_twin_brain_b200._lib import TUNE_SCATTER_MODE
+def test_ordered_push_equals_row_gather(rate, K):
+    """Rows with more than 8 contributions per step fall back to the warp gather inside the same kernel."""
     spec = synthetic.whole_brain(R=6, mean_size=700, sigma=0.5, K=K, gen_seed=3, name=f"wb6_K{K}")
     a = Network.from_spec(spec, device=0)
     b = Network.from_spec(spec, device=0)
     a.set_tuning(TUNE_PULL_METHOD, ROWS)
     b.set_tuning(TUNE_PULL_METHOD, SLOTS)
-    b.set_tuning(TUNE_SCATTER_MODE, queue)
     for n in (1, 37, 64, 5):
         sa, ma, na = a.run(n, noise_rate=rate, mode="pull")
         sb, mb, nb = b.run(n, noise_rate=rate, mode="pull")
