@@ -117,6 +117,20 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def combine_over_ranks(ms: float, events: float, world: int, device) -> tuple:
+    """Whole-job figures of N replicas: the slowest rank's device time, the events of all ranks."""
+    if world <= 1:
+        return ms, events
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms, events], dtype=torch.float64, device=device)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    tot = t.clone()
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(tot[1])
+
+
 # ---------------------------------------------------------------- CPU baseline
 def cpu_sample(scale: float, noise: float, seconds: float, max_steps: int, warmup: int = 2):
     """The reference algorithm (oracle port of models/block.py, OpenMP) on a scaled whole-brain network."""
@@ -225,15 +239,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ms = start.elapsed_time(end)
     events = net.get(10) - ev0
     launches = net.info().kernel_launches - l0
-    t = torch.tensor([ms, float(events)], dtype=torch.float64, device=f"cuda:{dev}")
-    if world > 1:
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        tot = t.clone()
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-        ms_max, events_all = float(mx[0]), float(tot[1])
-    else:
-        ms_max, events_all = ms, float(events)
+    ms_max, events_all = combine_over_ranks(ms, float(events), world, f"cuda:{dev}")
     value = events_all / (ms_max / 1000.0)
     sim_ratio = K * spec.dt / 1000.0 / (ms_max / 1000.0)
 
