@@ -1421,6 +1421,10 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         if (value < 1 || value > 32) return fail(DTB_ERR_ARG, "scatter words per warp must be 1..32");
         b->scatter_wpw = (int)value;
         break;
+    case DTB_TUNE_J_CACHE:
+        if (value < 0 || value > 1) return fail(DTB_ERR_ARG, "J cache policy must be 0 (stream) or 1 (keep)");
+        b->ds.j_keep = (int)value;
+        break;
     case DTB_TUNE_PULL_METHOD:
         if (value < 0 || value > 2) return fail(DTB_ERR_ARG, "pull method must be 0 (auto), 1 (rows) or 2 (ordered push)");
         if (value == 2 && !b->has_qpos) return fail(DTB_ERR_STATE, "ordered push needs the push CSR with pull-row positions");
@@ -1455,6 +1459,7 @@ int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value)
     case DTB_TUNE_USE_GRAPHS: *value = b->use_graphs ? 1 : 0; break;
     case DTB_TUNE_STEP_VARIANT: *value = b->step_variant; break;
     case DTB_TUNE_PULL_METHOD: *value = b->pull_method; break;
+    case DTB_TUNE_J_CACHE: *value = b->ds.j_keep; break;
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
     }
     return DTB_OK;
@@ -1487,6 +1492,14 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
             if (o[2] < best_ms) { best_ms = o[2]; best_w = w; ev = o[3]; }
         }
         b->scatter_wpw = best_w;
+        {   // J lines kept in L2 for the scatter vs streamed
+            const int keep = b->ds.j_keep;
+            b->ds.j_keep = 1 - keep;
+            float o[4];
+            RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PUSH, o));
+            if (o[2] < best_ms) { best_ms = o[2]; ev = o[3]; }
+            else b->ds.j_keep = keep;
+        }
         push_ms = best_ms;
     }
     if (b->has_pull) {

@@ -71,10 +71,18 @@ __device__ __forceinline__ float4 load_J(const DevState& s, int64_t n)
     return make_float4(a.x, a.y, b.x, b.y);
 }
 
+// j_keep: the update's J stores keep their L2 lines (normal priority) so that the
+// push scatter that follows finds part of J in L2 for its read-modify-writes;
+// otherwise they stream (evict first) like the rest of the state.
 __device__ __forceinline__ void store_J(const DevState& s, int64_t n, float4 J)
 {
-    __stcs(s.J2 + n * s.j_es, make_float2(J.x, J.y));
-    __stcs(s.J2 + s.j_ps + n * s.j_es, make_float2(J.z, J.w));
+    if (s.j_keep) {
+        __stcg(s.J2 + n * s.j_es, make_float2(J.x, J.y));
+        __stcg(s.J2 + s.j_ps + n * s.j_es, make_float2(J.z, J.w));
+    } else {
+        __stcs(s.J2 + n * s.j_es, make_float2(J.x, J.y));
+        __stcs(s.J2 + s.j_ps + n * s.j_es, make_float2(J.z, J.w));
+    }
 }
 
 __device__ __forceinline__ bool test_bit(const uint32_t* __restrict__ bits, int64_t n)

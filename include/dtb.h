@@ -223,9 +223,11 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          inputs; 2 = ordered push: firing rows scatter into
  *                          per-neuron slots that the next update sums in pull
  *                          order (needs the push CSR); 0 = ordered push while
- *                          at most 10 % of the neurons propagate, else rows */
+ *                          at most 10 % of the neurons propagate, else rows
+ * DTB_TUNE_J_CACHE         0 = the update streams J (evict first), 1 = its J
+ *                          stores keep normal L2 priority for the scatter */
 enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,
-       DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5 };
+       DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5, DTB_TUNE_J_CACHE = 6 };
 int dtb_block_set_tuning(dtb_block* b, int key, int64_t value);
 int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value);
 
