@@ -164,11 +164,11 @@ struct dtb_block {
     int step_variant = 0;         // 0: 2 resident CTAs/SM register budget, 1: 3
     // ordered push (bit-exact pull through per-neuron slots)
     bool has_qpos = false;
-    int pull_method = 0;          // 0: ordered push while activity <= slot_threshold, 1: row gather, 2: ordered push
+    int pull_method = 0;          // 0: auto, 1: row gather, 2: ordered push (slots), 3: ordered push (masks)
     double slot_threshold = 0.1;
     // graphs: one chunk graph per propagation method (push, pull rows, pull slots)
-    cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
-    int graph_len[4] = {0, 0, 0, 0};
+    cudaGraphExec_t graph[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    int graph_len[5] = {0, 0, 0, 0, 0};
     bool use_graphs = true;
     // attached BOLD
     int bold_R = 0;
@@ -602,7 +602,7 @@ static int launch_src(dtb_block* b, const DevState& s)
     return DTB_OK;
 }
 
-// gather: 0 none, kGatherRows (fused pull gather), kGatherSlots (ordered-push slots)
+// gather: 0 none, kGatherRows (fused pull gather), kGatherSlots / kGatherMasks (ordered push)
 static int launch_update(dtb_block* b, const DevState& s, int gather, bool forced)
 {
     if (s.N <= 0) return DTB_OK;
@@ -613,10 +613,12 @@ static int launch_update(dtb_block* b, const DevState& s, int gather, bool force
     if (forced) {
         if (gather == kGatherRows) launch_step<kGatherRows, true, true>(b, s);
         else if (gather == kGatherSlots) launch_step<kGatherSlots, true, true>(b, s);
+        else if (gather == kGatherMasks) launch_step<kGatherMasks, true, true>(b, s);
         else launch_step<0, true, true>(b, s);
     } else {
         if (gather == kGatherRows) launch_step<kGatherRows, true, false>(b, s);
         else if (gather == kGatherSlots) launch_step<kGatherSlots, true, false>(b, s);
+        else if (gather == kGatherMasks) launch_step<kGatherMasks, true, false>(b, s);
         else launch_step<0, true, false>(b, s);
     }
     CK(cudaGetLastError());
@@ -629,20 +631,23 @@ static int launch_gather_only(dtb_block* b, const DevState& s, int gather = kGat
 {
     if (s.N <= 0) return DTB_OK;
     if (gather == kGatherSlots) launch_step<kGatherSlots, false, false>(b, s);
+    else if (gather == kGatherMasks) launch_step<kGatherMasks, false, false>(b, s);
     else launch_step<kGatherRows, false, false>(b, s);
     CK(cudaGetLastError());
     b->launches++;
     return DTB_OK;
 }
 
-static int launch_scatter(dtb_block* b, const DevState& s, bool ordered = false)
+// how: kScatterJ (push), kScatterSlots / kScatterMasks (ordered push)
+static int launch_scatter(dtb_block* b, const DevState& s, int how = kScatterJ)
 {
     const int wpw = b->scatter_wpw;
     const int64_t warps = (s.n_words + wpw - 1) / wpw;
     const unsigned grid = grid_for(warps * 32, kScatterThreads);
     if (grid == 0) return DTB_OK;
-    if (ordered) k_scatter<true><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
-    else k_scatter<false><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
+    if (how == kScatterSlots) k_scatter<kScatterSlots><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
+    else if (how == kScatterMasks) k_scatter<kScatterMasks><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
+    else k_scatter<kScatterJ><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
     CK(cudaGetLastError());
     b->launches++;
     return DTB_OK;
@@ -656,6 +661,7 @@ static void drop_graphs(dtb_block* b)
 // Internal propagation methods: DTB_MODE_PUSH, DTB_MODE_PULL (row gather) and
 // the ordered push that DTB_MODE_PULL resolves to while activity is low.
 constexpr int kModeSlots = 3;
+constexpr int kModeMasks = 4;
 
 static int ensure_slots(dtb_block* b)
 {
@@ -671,6 +677,21 @@ static int ensure_slots(dtb_block* b)
     return DTB_OK;
 }
 
+static bool masks_possible(const dtb_block* b) { return b->has_qpos && b->has_push && b->max_in <= 32 * kMaskWords; }
+
+static int ensure_masks(dtb_block* b)
+{
+    DevState& s = b->ds;
+    if (s.pmask) return DTB_OK;
+    const size_t words = (size_t)std::max<int64_t>(b->N, 1) * 2 * kMaskWords;
+    uint32_t* m = nullptr;
+    RET(dalloc(b, &m, words));
+    CK(cudaMemsetAsync(m, 0, sizeof(uint32_t) * words, b->stream));
+    s.pmask = m;
+    drop_graphs(b);
+    return DTB_OK;
+}
+
 // n steps with one propagation method (no host synchronisation).
 static int enqueue_steps(dtb_block* b, int n, int mode)
 {
@@ -681,14 +702,16 @@ static int enqueue_steps(dtb_block* b, int n, int mode)
             RET(launch_update(b, s, 0, false));
             RET(launch_scatter(b, s));
         }
-    } else if (mode == kModeSlots) {
+    } else if (mode == kModeSlots || mode == kModeMasks) {
+        const int g = mode == kModeSlots ? kGatherSlots : kGatherMasks;
+        const int how = mode == kModeSlots ? kScatterSlots : kScatterMasks;
         RET(launch_update(b, s, 0, false));
-        RET(launch_scatter(b, s, true));
+        RET(launch_scatter(b, s, how));
         for (int k = 1; k < n; ++k) {
-            RET(launch_update(b, s, kGatherSlots, false));
-            RET(launch_scatter(b, s, true));
+            RET(launch_update(b, s, g, false));
+            RET(launch_scatter(b, s, how));
         }
-        RET(launch_gather_only(b, s, kGatherSlots));
+        RET(launch_gather_only(b, s, g));
     } else {
         RET(launch_update(b, s, 0, false));
         for (int k = 1; k < n; ++k) RET(launch_update(b, s, kGatherRows, false));
@@ -737,8 +760,17 @@ static int resolve_method(dtb_block* b, int m)
 {
     if (m != DTB_MODE_PULL || !b->has_qpos || !b->has_push || b->pull_method == 1) return m;
     if (b->pull_method == 2) return kModeSlots;
+    if (b->pull_method == 3) return kModeMasks;
     const double f = b->last_frac < 0.0 ? 0.0 : b->last_frac;
-    return f <= b->slot_threshold ? kModeSlots : m;
+    if (f > b->slot_threshold) return m;
+    return masks_possible(b) ? kModeMasks : kModeSlots;
+}
+
+static int ensure_method(dtb_block* b, int mm)
+{
+    if (mm == kModeSlots) return ensure_slots(b);
+    if (mm == kModeMasks) return ensure_masks(b);
+    return DTB_OK;
 }
 
 static int set_run_params(dtb_block* b, float noise_rate, int isolated)
@@ -1330,7 +1362,7 @@ int dtb_block_run(dtb_block* b, int n_steps, float noise_rate, int isolated, int
     while (done < n_steps) {
         const int m = choose_mode(b, mode);
         const int mm = resolve_method(b, m);
-        if (mm == kModeSlots) RET(ensure_slots(b));
+        RET(ensure_method(b, mm));
         const uint32_t cap = b->stats_cap;
         int n = (int)std::min<int64_t>(n_steps - done, (int64_t)std::min<uint32_t>(cap, (uint32_t)b->chunk));
         RET(set_run_params(b, noise_rate, isolated));
@@ -1355,7 +1387,7 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
     RET(check_src_steps(b, n_steps));
     DeviceGuard g(b->device);
     const int m = resolve_method(b, choose_mode(b, mode));
-    if (m == kModeSlots) RET(ensure_slots(b));
+    RET(ensure_method(b, m));
     RET(ensure_stats(b, (uint32_t)n_steps));
     RET(set_run_params(b, noise_rate, isolated));
     unsigned long long ev0 = 0, ev1 = 0;
@@ -1369,17 +1401,19 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
     auto rec = [&](int i) { return cudaEventRecord(ev[(size_t)i], b->stream); };
     int rc = DTB_OK;
     int done_steps = 0;
-    if (m == DTB_MODE_PUSH || m == kModeSlots) {
-        const bool ord = m == kModeSlots;
+    if (m == DTB_MODE_PUSH || m == kModeSlots || m == kModeMasks) {
+        const bool ord = m != DTB_MODE_PUSH;
+        const int g = m == kModeSlots ? kGatherSlots : kGatherMasks;
+        const int how = m == kModeSlots ? kScatterSlots : (m == kModeMasks ? kScatterMasks : kScatterJ);
         for (int st = 0; st < n_steps && rc == DTB_OK && k + 6 <= n_ev; ++st) {
-            rec(k); rc = launch_update(b, b->ds, (ord && st > 0) ? kGatherSlots : 0, false); rec(k + 1);
+            rec(k); rc = launch_update(b, b->ds, (ord && st > 0) ? g : 0, false); rec(k + 1);
             kind.push_back(0); k += 2;
             if (rc != DTB_OK) break;
-            rec(k); rc = launch_scatter(b, b->ds, ord); rec(k + 1); kind.push_back(1); k += 2;
+            rec(k); rc = launch_scatter(b, b->ds, how); rec(k + 1); kind.push_back(1); k += 2;
             done_steps++;
         }
         if (ord && rc == DTB_OK) {
-            rec(k); rc = launch_gather_only(b, b->ds, kGatherSlots); rec(k + 1); kind.push_back(2); k += 2;
+            rec(k); rc = launch_gather_only(b, b->ds, g); rec(k + 1); kind.push_back(2); k += 2;
         }
     } else {
         rec(k); rc = launch_update(b, b->ds, 0, false); rec(k + 1); kind.push_back(0); k += 2;
@@ -1426,8 +1460,12 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         b->ds.j_keep = (int)value;
         break;
     case DTB_TUNE_PULL_METHOD:
-        if (value < 0 || value > 2) return fail(DTB_ERR_ARG, "pull method must be 0 (auto), 1 (rows) or 2 (ordered push)");
-        if (value == 2 && !b->has_qpos) return fail(DTB_ERR_STATE, "ordered push needs the push CSR with pull-row positions");
+        if (value < 0 || value > 3)
+            return fail(DTB_ERR_ARG, "pull method must be 0 (auto), 1 (rows), 2 (ordered push, slots) or 3 (masks)");
+        if (value >= 2 && !b->has_qpos) return fail(DTB_ERR_STATE, "ordered push needs the push CSR with pull-row positions");
+        if (value == 3 && !masks_possible(b))
+            return fail(DTB_ERR_STATE, "position masks hold in-degrees up to %d (max in-degree %lld)", 32 * kMaskWords,
+                        (long long)b->max_in);
         b->pull_method = (int)value;
         break;
     case DTB_TUNE_CHUNK:

@@ -22,6 +22,8 @@ constexpr int kWarpNeurons = 128;      // neurons owned by one warp in the step 
 constexpr uint32_t kSlotCap = 8;       // ordered-push contributions kept per neuron and step
 constexpr int kGatherRows = 1;         // k_step gathers whole pull rows
 constexpr int kGatherSlots = 2;        // k_step sums its ordered-push slots
+constexpr int kGatherMasks = 3;        // k_step sums the pull entries its position masks mark
+constexpr int kMaskWords = 4;          // position-mask words per kind: in-degree up to 128
 constexpr int kStepThreads = 256;      // 8 warps, 1024 neurons per CTA
 
 // One deduplicated row of the 22-column property matrix
@@ -113,6 +115,7 @@ struct DevState {
     // ordered push (bit-exact pull order at push cost): pending contributions per neuron
     uint32_t* slot_cnt;         // [N] contributions written since the neuron last consumed them
     uint4* slots;               // [N][kSlotCap] {pull-row position | kind bit, 0, w.x bits, w.y bits}
+    uint32_t* pmask;            // [N][2][kMaskWords] pull-row positions that fired (excitatory, inhibitory)
     // statistics
     int n_sub;
     uint32_t* sub_spk;          // [n_sub] accumulators (active)

@@ -169,6 +169,44 @@ __device__ __forceinline__ float4 slot_sum(const uint4* __restrict__ sl, uint32_
     return make_float4(a0, a1, a2, a3);
 }
 
+// Sum of the pull entries a neuron's position masks mark, in ascending position
+// (the order gather_row adds them): excitatory and inhibitory pairs are summed
+// separately, as gather_row's two accumulator pairs are.  Up to 8 weights are
+// loaded before they are added.
+__device__ __forceinline__ float4 mask_sum(const DevState& s, int64_t n, uint4 ex, uint4 in)
+{
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float2* __restrict__ pw = s.pw + __ldg(s.prow + n);
+#pragma unroll
+    for (int kind = 0; kind < 2; ++kind) {
+        const uint4 m4 = kind ? in : ex;
+        uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
+        float x = 0.0f, y = 0.0f;
+#pragma unroll
+        for (int wi = 0; wi < 4; ++wi) {
+            uint32_t word = mw[wi];
+            while (word) {
+                uint32_t pos[8];
+                int k = 0;
+                while (word && k < 8) {
+                    const int bit = __ffs(word) - 1;
+                    word &= word - 1u;
+                    pos[k++] = (uint32_t)(wi * 32 + bit);
+                }
+                float2 w[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    if (i < k) w[i] = __ldg(pw + pos[i]);
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    if (i < k) { x = __fadd_rn(x, w[i].x); y = __fadd_rn(y, w[i].y); }
+            }
+        }
+        if (kind) { a.z = x; a.w = y; } else { a.x = x; a.y = y; }
+    }
+    return a;
+}
+
 // ------------------------------------------------------------ BOLD step
 // models/bold_model_pytorch.py:43-78 in float64 for region r with input u
 // (q before v before f_in before s, f_in clamped at 0).
@@ -427,7 +465,30 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             }
         }
         unsigned char* stage_buf = my_stage + sb * kStageBytes;
-        if (GATHER == kGatherSlots) {
+        if (GATHER == kGatherMasks) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                if (n >= s.N) continue;
+                uint4* pm = reinterpret_cast<uint4*>(s.pmask + n * (2 * kMaskWords));
+                const uint4 ex = __ldcs(pm), in = __ldcs(pm + 1);
+                float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+                if ((ex.x | ex.y | ex.z | ex.w | in.x | in.y | in.z | in.w) != 0u) {
+                    pm[0] = make_uint4(0u, 0u, 0u, 0u);
+                    pm[1] = make_uint4(0u, 0u, 0u, 0u);
+                    sum = mask_sum(s, n, ex, in);
+                }
+                Jn[j] = add4(load_J(s, n), sum);   // models/block.py:71-73
+            }
+            if (!UPDATE) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t n = base + j * 32 + lane;
+                    if (n < s.N) store_J(s, n, Jn[j]);
+                }
+                continue;
+            }
+        } else if (GATHER == kGatherSlots) {
             float4 sum[4];
             uint32_t ovf = 0u;   // bit j: neuron j of this lane got more contributions than slots
             // counts of the lane's four neurons, then their first two slots, all in flight together
@@ -735,8 +796,9 @@ constexpr int kScatterThreads = 256;
 constexpr int kScatterMaxWords = 32;
 
 constexpr int kScatterUnroll = 8;   // synapses in flight per lane
+constexpr int kScatterJ = 0, kScatterSlots = 1, kScatterMasks = 2;
 
-template <bool ORDERED>
+template <int MODE>
 __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw)
 {
     __shared__ uint32_t sh_rows[kScatterThreads / 32][kScatterMaxWords * 32];
@@ -803,11 +865,18 @@ __global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw
                 if (ok[u]) {
                     const int64_t e = re0 + (v - rs);
                     c[u] = __ldcs(s.qcol + e);
-                    w[u] = __ldcs(s.qw + e);
-                    if (ORDERED) ppos[u] = __ldcs(s.qpos + e);
+                    if (MODE != kScatterMasks) w[u] = __ldcs(s.qw + e);
+                    if (MODE != kScatterJ) ppos[u] = __ldcs(s.qpos + e);
                 }
             }
-            if (ORDERED) {
+            if (MODE == kScatterMasks) {
+#pragma unroll
+                for (int u = 0; u < kScatterUnroll; ++u)
+                    if (ok[u])
+                        atomicOr(s.pmask + (int64_t)(c[u] & kIndexMask) * (2 * kMaskWords) +
+                                     ((c[u] & kKindBit) ? kMaskWords : 0) + (ppos[u] >> 5),
+                                 1u << (ppos[u] & 31));
+            } else if (MODE == kScatterSlots) {
                 // every slot claim of the batch first, so their round trips overlap
                 uint32_t k[kScatterUnroll];
 #pragma unroll

@@ -218,12 +218,16 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          two and three with the state of the next tile
  *                          bulk-copied to shared memory while the current one
  *                          computes
- * DTB_TUNE_PULL_METHOD     how DTB_MODE_PULL propagates (bit-identical either
+ * DTB_TUNE_PULL_METHOD     how DTB_MODE_PULL propagates (bit-identical every
  *                          way): 1 = every postsynaptic row gathers its firing
  *                          inputs; 2 = ordered push: firing rows scatter into
  *                          per-neuron slots that the next update sums in pull
- *                          order (needs the push CSR); 0 = ordered push while
- *                          at most 10 % of the neurons propagate, else rows
+ *                          order; 3 = ordered push: firing rows set one bit per
+ *                          pull-row position in per-neuron masks (in-degree up
+ *                          to 128) and the next update sums the marked pull
+ *                          entries in order (2 and 3 need the push CSR); 0 =
+ *                          masks, else slots, while at most 10 % of the neurons
+ *                          propagate, else rows
  * DTB_TUNE_J_CACHE         0 = the update streams J (evict first), 1 = its J
  *                          stores keep normal L2 priority for the scatter */
 enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,

@@ -15,18 +15,19 @@ from tests.test_gpu_parity import class_decay_like_reference
 
 pytestmark = pytest.mark.gpu
 
-ROWS, SLOTS = 1, 2
+ROWS, SLOTS, MASKS = 1, 2, 3
 
 
 def _state(net):
     return [net.get(f) for f in (FIELD_V, FIELD_J, FIELD_T_LAST, FIELD_I_SYN, FIELD_ACTIVE)]
 
 
-def test_ordered_push_matches_reference_golden():
+@pytest.mark.parametrize("method", [SLOTS, MASKS], ids=["slots", "masks"])
+def test_ordered_push_matches_reference_golden(method):
     g = np.load(os.path.join(GOLDEN, "single_block_2k.npz"))
     spec = synthetic.config_single_block()
     net = Network.from_spec(spec, device=0, build_push=True, class_decay=class_decay_like_reference(spec))
-    net.set_tuning(TUNE_PULL_METHOD, SLOTS)
+    net.set_tuning(TUNE_PULL_METHOD, method)
     every = int(g["v_every"])
     act_ref = unpack(g["active"], spec.N)
     for c in range(int(g["steps"]) // every):
@@ -38,15 +39,17 @@ def test_ordered_push_matches_reference_golden():
     assert np.array_equal(net.get(FIELD_I_SYN), g["I_syn_final"])
 
 
-@pytest.mark.parametrize("rate,K", [(0.01, 100), (0.05, 200), (0.3, 60)],
+@pytest.mark.parametrize("method", [SLOTS, MASKS], ids=["slots", "masks"])
+@pytest.mark.parametrize("rate,K", [(0.01, 100), (0.05, 120), (0.3, 60)],
                          ids=["sparse", "overflowing_rows", "dense"])
-def test_ordered_push_equals_row_gather(rate, K):
-    """Rows with more than 8 contributions per step fall back to the warp gather inside the same kernel."""
+def test_ordered_push_equals_row_gather(rate, K, method):
+    """Slots: rows with more than 8 contributions per step fall back to the warp gather inside the same
+    kernel.  Masks: one bit per pull-row position (in-degree up to 128)."""
     spec = synthetic.whole_brain(R=6, mean_size=700, sigma=0.5, K=K, gen_seed=3, name=f"wb6_K{K}")
     a = Network.from_spec(spec, device=0)
     b = Network.from_spec(spec, device=0)
     a.set_tuning(TUNE_PULL_METHOD, ROWS)
-    b.set_tuning(TUNE_PULL_METHOD, SLOTS)
+    b.set_tuning(TUNE_PULL_METHOD, method)
     for n in (1, 37, 64, 5):
         sa, ma, na = a.run(n, noise_rate=rate, mode="pull")
         sb, mb, nb = b.run(n, noise_rate=rate, mode="pull")
@@ -64,8 +67,8 @@ def test_ordered_push_npz_positions_and_method_switches():
     a = Network.from_npz(d, dt=0.1, seed=11, device=0)
     b = Network.from_npz(d, dt=0.1, seed=11, device=0)
     a.set_tuning(TUNE_PULL_METHOD, ROWS)
-    for k, n in enumerate((20, 33, 7, 40)):
-        b.set_tuning(TUNE_PULL_METHOD, SLOTS if k % 2 == 0 else ROWS)
+    for k, n in enumerate((20, 33, 7, 40, 11, 9)):
+        b.set_tuning(TUNE_PULL_METHOD, (SLOTS, ROWS, MASKS)[k % 3])
         sa, _, _ = a.run(n, noise_rate=0.02, mode="pull")
         sb, _, _ = b.run(n, noise_rate=0.02, mode="pull")
         assert np.array_equal(sa, sb)
@@ -105,11 +108,23 @@ def test_npz_hub_row_and_repeated_pairs(tmp_path):
     assert np.array_equal(qix, post[order].astype(np.uint32) | np.where(kind[order] == 2, np.uint32(0x80000000), 0))
     assert np.array_equal(qw, w[order])
     b = Network.from_npz(str(tmp_path), dt=0.1, seed=2, device=0)
+    c = Network.from_npz(str(tmp_path), dt=0.1, seed=2, device=0)
     a.set_tuning(TUNE_PULL_METHOD, ROWS)
     b.set_tuning(TUNE_PULL_METHOD, SLOTS)
+    c.set_tuning(TUNE_PULL_METHOD, MASKS)
     for n in (50, 50):
         sa, _, na = a.run(n, noise_rate=0.05, mode="pull")
-        sb, _, nb = b.run(n, noise_rate=0.05, mode="pull")
-        assert np.array_equal(sa, sb) and np.array_equal(na, nb)
-        for x, y in zip(_state(a), _state(b)):
-            assert np.array_equal(x, y)
+        for other in (b, c):
+            so, _, no = other.run(n, noise_rate=0.05, mode="pull")
+            assert np.array_equal(sa, so) and np.array_equal(na, no)
+            for x, y in zip(_state(a), _state(other)):
+                assert np.array_equal(x, y)
+
+
+def test_masks_refused_beyond_128_inputs():
+    from digital_twin_brain_b200._lib import DtbError
+    spec = synthetic.single_block(600, 200, name="k200")
+    net = Network.from_spec(spec, device=0)
+    with pytest.raises(DtbError):
+        net.set_tuning(TUNE_PULL_METHOD, MASKS)
+    net.run(20, noise_rate=0.02, mode="pull")      # auto: slots (in-degree 200 > 128)
