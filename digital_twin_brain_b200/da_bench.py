@@ -46,7 +46,7 @@ def main(argv=None):
     ap.add_argument("--threshold", type=float, default=None,
                     help="judge fallback threshold (default: --margin x the held-out judge error of the surrogate)")
     ap.add_argument("--margin", type=float, default=1.5)
-    ap.add_argument("--burn-in-windows", type=int, default=8,
+    ap.add_argument("--burn-in-windows", type=int, default=1,
                     help="judge windows before the assimilation (histories, surrogate adaptation); timed")
     ap.add_argument("--adapt-steps", type=int, default=20,
                     help="Adam steps per window on the judges' windows (0: the surrogate stays as trained)")
