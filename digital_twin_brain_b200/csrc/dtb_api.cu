@@ -518,12 +518,15 @@ static int launch_stats(dtb_block* b, const DevState& s)
 
 // Persistent step kernels: as many CTAs as are resident at once, each warp
 // streaming a contiguous run of tiles.
+// Dynamic shared memory of the step kernels: the mask gather's per-warp entry lists.
+static constexpr int step_dyn_smem(int g) { return g == kGatherMasks ? (kStepThreads / 32) * kMaskList * 10 : 0; }
+
 template <int G, bool U, bool F, int M>
 static int step_blocks_per_sm()
 {
     static int v = 0;
     if (!v) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_step<G, U, F, M>, kStepThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_step<G, U, F, M>, kStepThreads, step_dyn_smem(G));
         if (v < 1) v = 1;
     }
     return v;
@@ -547,7 +550,7 @@ static void launch_step_m(dtb_block* b, const DevState& s)
     unsigned grid;
     int tpw;
     step_grid(b, step_blocks_per_sm<G, U, F, M>(), grid, tpw);
-    k_step<G, U, F, M><<<grid, kStepThreads, 0, b->stream>>>(s, tpw);
+    k_step<G, U, F, M><<<grid, kStepThreads, step_dyn_smem(G), b->stream>>>(s, tpw);
 }
 
 // Update with staged (bulk-copied, one tile ahead) state loads: split J planes

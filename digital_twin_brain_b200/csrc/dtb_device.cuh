@@ -24,6 +24,7 @@ constexpr int kGatherRows = 1;         // k_step gathers whole pull rows
 constexpr int kGatherSlots = 2;        // k_step sums its ordered-push slots
 constexpr int kGatherMasks = 3;        // k_step sums the pull entries its position masks mark
 constexpr int kMaskWords = 4;          // position-mask words per kind: in-degree up to 128
+constexpr int kMaskList = 256;         // marked entries a warp gathers together per tile
 constexpr int kStepThreads = 256;      // 8 warps, 1024 neurons per CTA
 
 // One deduplicated row of the 22-column property matrix

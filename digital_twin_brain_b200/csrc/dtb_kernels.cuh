@@ -466,20 +466,87 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         }
         unsigned char* stage_buf = my_stage + sb * kStageBytes;
         if (GATHER == kGatherMasks) {
+            // The warp lists every marked pull entry of its 128 neurons (a lane's entries
+            // contiguous, neuron by neuron, excitatory then inhibitory, ascending position),
+            // loads their weights together, then every lane adds its own in that order.
+            uint16_t* lrel = reinterpret_cast<uint16_t*>(stage_smem + (size_t)wid * kMaskList * 10);
+            float2* lw = reinterpret_cast<float2*>(stage_smem + (size_t)wid * kMaskList * 10 + kMaskList * 2);
+            const int64_t rbase = __ldg(s.prow + base);             // entries relative to the tile's first row
+            uint4 mx[4], mi[4];
+            int nx[4], ni[4];
+            int mine = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                mx[j] = mi[j] = make_uint4(0u, 0u, 0u, 0u);
+                if (n < s.N) {
+                    uint4* pm = reinterpret_cast<uint4*>(s.pmask + n * (2 * kMaskWords));
+                    mx[j] = __ldcs(pm);
+                    mi[j] = __ldcs(pm + 1);
+                }
+                nx[j] = __popc(mx[j].x) + __popc(mx[j].y) + __popc(mx[j].z) + __popc(mx[j].w);
+                ni[j] = __popc(mi[j].x) + __popc(mi[j].y) + __popc(mi[j].z) + __popc(mi[j].w);
+                mine += nx[j] + ni[j];
+            }
+            int incl = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            const bool listed = total <= kMaskList;
+            float4 sum[4];
+            if (listed) {
+                int at = incl - mine;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (nx[j] + ni[j] == 0) continue;
+                    const int64_t n = base + j * 32 + lane;
+                    const uint32_t rel0 = (uint32_t)(__ldg(s.prow + n) - rbase);
+#pragma unroll
+                    for (int kind = 0; kind < 2; ++kind) {
+                        const uint4 m4 = kind ? mi[j] : mx[j];
+                        const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
+#pragma unroll
+                        for (int wi = 0; wi < 4; ++wi) {
+                            uint32_t word = mw[wi];
+                            while (word) {
+                                const int bit = __ffs(word) - 1;
+                                word &= word - 1u;
+                                lrel[at++] = (uint16_t)(rel0 + (uint32_t)(wi * 32 + bit));
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                const float2* __restrict__ pwt = s.pw + rbase;
+                for (int i = lane; i < total; i += 32) lw[i] = __ldg(pwt + lrel[i]);
+                __syncwarp();
+                int rd = incl - mine;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int k = 0; k < nx[j]; ++k) { const float2 w = lw[rd++]; a.x = __fadd_rn(a.x, w.x); a.y = __fadd_rn(a.y, w.y); }
+                    for (int k = 0; k < ni[j]; ++k) { const float2 w = lw[rd++]; a.z = __fadd_rn(a.z, w.x); a.w = __fadd_rn(a.w, w.y); }
+                    sum[j] = a;
+                }
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int64_t n = base + j * 32 + lane;
                 if (n >= s.N) continue;
-                uint4* pm = reinterpret_cast<uint4*>(s.pmask + n * (2 * kMaskWords));
-                const uint4 ex = __ldcs(pm), in = __ldcs(pm + 1);
-                float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
-                if ((ex.x | ex.y | ex.z | ex.w | in.x | in.y | in.z | in.w) != 0u) {
+                if (nx[j] + ni[j]) {
+                    uint4* pm = reinterpret_cast<uint4*>(s.pmask + n * (2 * kMaskWords));
                     pm[0] = make_uint4(0u, 0u, 0u, 0u);
                     pm[1] = make_uint4(0u, 0u, 0u, 0u);
-                    sum = mask_sum(s, n, ex, in);
+                    if (!listed) sum[j] = mask_sum(s, n, mx[j], mi[j]);   // a tile with many inputs
+                } else {
+                    sum[j] = make_float4(0.f, 0.f, 0.f, 0.f);
                 }
-                Jn[j] = add4(load_J(s, n), sum);   // models/block.py:71-73
+                Jn[j] = add4(load_J(s, n), sum[j]);   // models/block.py:71-73
             }
+            __syncwarp();   // the list is reused by the next tile
             if (!UPDATE) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
