@@ -765,8 +765,7 @@ static int resolve_method(dtb_block* b, int m)
     if (b->pull_method == 2) return kModeSlots;
     if (b->pull_method == 3) return kModeMasks;
     const double f = b->last_frac < 0.0 ? 0.0 : b->last_frac;
-    if (f > b->slot_threshold) return m;
-    return masks_possible(b) ? kModeMasks : kModeSlots;
+    return f <= b->slot_threshold ? kModeSlots : m;   // slots measured faster than masks on B200
 }
 
 static int ensure_method(dtb_block* b, int mm)

@@ -226,8 +226,8 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          pull-row position in per-neuron masks (in-degree up
  *                          to 128) and the next update sums the marked pull
  *                          entries in order (2 and 3 need the push CSR); 0 =
- *                          masks, else slots, while at most 10 % of the neurons
- *                          propagate, else rows
+ *                          slots while at most 10 % of the neurons propagate,
+ *                          else rows
  * DTB_TUNE_J_CACHE         0 = the update streams J (evict first), 1 = its J
  *                          stores keep normal L2 priority for the scatter */
 enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,
