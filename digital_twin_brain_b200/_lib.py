@@ -23,7 +23,7 @@ FIELD_V, FIELD_J, FIELD_I_UI, FIELD_I_SYN, FIELD_T_LAST, FIELD_ACTIVE, FIELD_NEW
     FIELD_SUB_COUNT, FIELD_EVENTS, FIELD_WINDOW_SPIKES, FIELD_G_FACTOR = range(13)
 
 TUNE_SCATTER_WORDS, TUNE_CHUNK, TUNE_PULL_THRESHOLD_PPM, TUNE_USE_GRAPHS, TUNE_STEP_VARIANT, TUNE_PULL_METHOD, \
-    TUNE_J_CACHE = range(7)
+    TUNE_J_CACHE, TUNE_SCATTER_VARIANT = range(8)
 
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "out of memory", 4: "I/O error", 5: "format error",
           6: "invalid state", 7: "limit exceeded"}

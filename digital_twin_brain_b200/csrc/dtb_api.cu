@@ -161,6 +161,7 @@ struct dtb_block {
     double pull_threshold = 0.05;
     int chunk = 32;
     int scatter_wpw = 32;         // bitmask words per warp in the push scatter
+    int scatter_variant = 0;      // 0: registers unbounded, 1: budgeted for 6 resident CTAs per SM
     int step_variant = 0;         // 0: 2 resident CTAs/SM register budget, 1: 3
     // ordered push (bit-exact pull through per-neuron slots)
     bool has_qpos = false;
@@ -648,9 +649,11 @@ static int launch_scatter(dtb_block* b, const DevState& s, int how = kScatterJ)
     const int64_t warps = (s.n_words + wpw - 1) / wpw;
     const unsigned grid = grid_for(warps * 32, kScatterThreads);
     if (grid == 0) return DTB_OK;
-    if (how == kScatterSlots) k_scatter<kScatterSlots><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
-    else if (how == kScatterMasks) k_scatter<kScatterMasks><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
-    else k_scatter<kScatterJ><<<grid, kScatterThreads, 0, b->stream>>>(s, wpw);
+    const size_t smem = sizeof(uint32_t) * 32 * (size_t)wpw * (kScatterThreads / 32);   // <= 32 KB
+    if (how == kScatterSlots) k_scatter<kScatterSlots><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
+    else if (how == kScatterMasks) k_scatter<kScatterMasks><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
+    else if (b->scatter_variant == 1) k_scatter<kScatterJ, 6><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
+    else k_scatter<kScatterJ><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
     CK(cudaGetLastError());
     b->launches++;
     return DTB_OK;
@@ -1457,6 +1460,10 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         if (value < 1 || value > 32) return fail(DTB_ERR_ARG, "scatter words per warp must be 1..32");
         b->scatter_wpw = (int)value;
         break;
+    case DTB_TUNE_SCATTER_VARIANT:
+        if (value < 0 || value > 1) return fail(DTB_ERR_ARG, "scatter variant must be 0 or 1");
+        b->scatter_variant = (int)value;
+        break;
     case DTB_TUNE_J_CACHE:
         if (value < 0 || value > 1) return fail(DTB_ERR_ARG, "J cache policy must be 0 (stream) or 1 (keep)");
         b->ds.j_keep = (int)value;
@@ -1500,6 +1507,7 @@ int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value)
     case DTB_TUNE_STEP_VARIANT: *value = b->step_variant; break;
     case DTB_TUNE_PULL_METHOD: *value = b->pull_method; break;
     case DTB_TUNE_J_CACHE: *value = b->ds.j_keep; break;
+    case DTB_TUNE_SCATTER_VARIANT: *value = b->scatter_variant; break;
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
     }
     return DTB_OK;
@@ -1525,13 +1533,17 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
     }
     if (b->has_push) {
         const int cand[6] = {1, 2, 4, 8, 16, 32};
-        for (int w : cand) {
-            b->scatter_wpw = w;
-            float o[4];
-            RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PUSH, o));
-            if (o[2] < best_ms) { best_ms = o[2]; best_w = w; ev = o[3]; }
-        }
+        int best_sv = b->scatter_variant;
+        for (int sv = 0; sv < 2; ++sv)
+            for (int w : cand) {
+                b->scatter_wpw = w;
+                b->scatter_variant = sv;
+                float o[4];
+                RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PUSH, o));
+                if (o[2] < best_ms) { best_ms = o[2]; best_w = w; best_sv = sv; ev = o[3]; }
+            }
         b->scatter_wpw = best_w;
+        b->scatter_variant = best_sv;
         {   // J lines kept in L2 for the scatter vs streamed
             const int keep = b->ds.j_keep;
             b->ds.j_keep = 1 - keep;

@@ -865,17 +865,19 @@ constexpr int kScatterMaxWords = 32;
 constexpr int kScatterUnroll = 8;   // synapses in flight per lane
 constexpr int kScatterJ = 0, kScatterSlots = 1, kScatterMasks = 2;
 
-template <int MODE>
-__global__ void __launch_bounds__(kScatterThreads) k_scatter(DevState s, int wpw)
+// MINB: resident CTAs per SM the registers are budgeted for; the row lists take
+// wpw * 32 entries per warp of dynamic shared memory.
+template <int MODE, int MINB = 1>
+__global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, int wpw)
 {
-    __shared__ uint32_t sh_rows[kScatterThreads / 32][kScatterMaxWords * 32];
+    extern __shared__ uint32_t sh_rows_dyn[];
     const unsigned long long steps_done = s.ctl->steps_done;
     const uint32_t* __restrict__ bits = s.bits[(steps_done - 1ull) & 1ull];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t w0 = warp_global * wpw;
-    uint32_t* rows = sh_rows[wid];
+    uint32_t* rows = sh_rows_dyn + (size_t)wid * wpw * 32;
     uint32_t word = (lane < wpw && w0 + lane < s.n_words) ? __ldcs(bits + w0 + lane) : 0u;
     // list the set bits of the window in neuron order
     const int cnt = __popc(word);

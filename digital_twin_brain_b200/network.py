@@ -182,7 +182,8 @@ class Network:
         _lib.call("dtb_block_autotune", self._h, int(n_steps), float(noise_rate), _ptr(r))
         return dict(scatter_words=int(r[0]), push_ms=float(r[1]), pull_ms=float(r[2]), activity=float(r[3]),
                     pull_threshold=float(r[4]), step_variant=int(r[5]),
-                    j_cache=self.get_tuning(_lib.TUNE_J_CACHE))
+                    j_cache=self.get_tuning(_lib.TUNE_J_CACHE),
+                    scatter_variant=self.get_tuning(_lib.TUNE_SCATTER_VARIANT))
 
     def step_forced(self, forced_active=None, forced_new_active=None, noise_rate: float | None = 0.01,
                     isolated: bool = False, mode: str = "pull"):

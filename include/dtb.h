@@ -229,9 +229,11 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          slots while at most 10 % of the neurons propagate,
  *                          else rows
  * DTB_TUNE_J_CACHE         0 = the update streams J (evict first), 1 = its J
- *                          stores keep normal L2 priority for the scatter */
+ *                          stores keep normal L2 priority for the scatter
+ * DTB_TUNE_SCATTER_VARIANT push scatter registers: 0 = unbounded, 1 = budgeted
+ *                          for six resident CTAs per SM */
 enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,
-       DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5, DTB_TUNE_J_CACHE = 6 };
+       DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5, DTB_TUNE_J_CACHE = 6, DTB_TUNE_SCATTER_VARIANT = 7 };
 int dtb_block_set_tuning(dtb_block* b, int key, int64_t value);
 int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value);
 

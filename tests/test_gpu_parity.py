@@ -175,14 +175,17 @@ def test_autotune_and_tuning_knobs():
         net.set_tuning(TUNE_SCATTER_WORDS, 0)
 
 
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("wpw", [1, 4, 32])
-def test_scatter_shapes_agree_with_pull_under_forcing(wpw):
-    """One push step from identical state at several launch shapes vs the exact pull step."""
-    from digital_twin_brain_b200._lib import TUNE_SCATTER_WORDS
+def test_scatter_shapes_agree_with_pull_under_forcing(wpw, variant):
+    """One push step from identical state at several launch shapes and register budgets vs the
+    exact pull step."""
+    from digital_twin_brain_b200._lib import TUNE_SCATTER_VARIANT, TUNE_SCATTER_WORDS
     spec = synthetic.single_block(8000, 100, name="n8k")
     a = Network.from_spec(spec, device=0)
     b = Network.from_spec(spec, device=0)
     a.set_tuning(TUNE_SCATTER_WORDS, wpw)
+    a.set_tuning(TUNE_SCATTER_VARIANT, variant)
     for _ in range(80):
         a.run(1, mode="push")
         b.run(1, mode="pull")
