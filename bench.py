@@ -294,6 +294,21 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "traffic": traffic, "kernel": dom, "algorithmic_bytes_per_launch": d_bytes, "launch_ms": d_ms,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
 
+    # the push scatter's own ceiling: float2 atomics per second on this GPU, measured live with the
+    # same count into J-sized targets, destinations inside region-sized windows
+    atomic = None
+    if mode == "push" and kt["propagate_ms"] > 0:
+        import ctypes
+        from digital_twin_brain_b200 import _lib
+        pm = ctypes.c_float()
+        _lib.call("dtb_measure_atomic_rate", dev, int(N), int(max(evs, 1)), int(max(1, N // spec.R)),
+                  ctypes.byref(pm))
+        peak_ops = evs / (pm.value * 1e-3) / 1e9
+        got_ops = evs / (kt["propagate_ms"] * 1e-3) / 1e9
+        atomic = {"bound": "l2_atomics", "achieved": got_ops, "peak": peak_ops, "unit": "G float2 atomics/s",
+                  "frac": got_ops / peak_ops, "kernel": "scatter",
+                  "probe": f"dtb_measure_atomic_rate(N={N}, ops={int(evs)}, window={N // spec.R})"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_sample(scale=1 / 64, noise=args.noise, seconds=15.0, max_steps=10_000)
@@ -316,6 +331,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "kernel_ms": kt, "tune": tune, "build_s": t_build, "device_gb": info.device_bytes / 1e9,
                 "gpu_launches": int(launches),
                 "roofline": roofline,
+                "atomic_roofline": atomic,
                 "step_roofline": {"bytes_per_step": step_bytes, "ms": kt["step_ms"],
                                   "achieved_gbs": step_bytes / (kt["step_ms"] * 1e-3) / 1e9 if kt["step_ms"] else 0},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

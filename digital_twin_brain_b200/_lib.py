@@ -81,6 +81,7 @@ _SIGS = {
     "dtb_block_scale_property_by_subblock": [c_vp, c_int, c_vp, c_vp, c_vp],
     "dtb_block_gamma_property_by_subblock": [c_vp, c_int, c_vp, c_vp, c_vp, c_vp],
     "dtb_block_set_input_spikes": [c_vp, c_i64, c_vp, c_i64, c_vp],
+    "dtb_measure_atomic_rate": [c_int, c_i64, c_i64, c_i64, c_vp],
     "dtb_block_update_conn_weight": [c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
     "dtb_block_save": [c_vp, c_char_p],
     "dtb_block_load": [c_vp, c_char_p],

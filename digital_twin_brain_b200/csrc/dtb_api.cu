@@ -1922,6 +1922,40 @@ int dtb_block_set_input_spikes(dtb_block* b, int64_t n_src, const uint32_t* neur
     return DTB_OK;
 }
 
+int dtb_measure_atomic_rate(int device, int64_t n_targets, int64_t n_ops, int64_t window, float* ms_out)
+{
+    if (!ms_out || n_targets < 1 || n_targets > (int64_t)kIndexMask || n_ops < 1 || window < 1)
+        return fail(DTB_ERR_ARG, "bad argument");
+    DeviceGuard g(device);
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    uint32_t* idx = nullptr; float2* J = nullptr;
+    cudaEvent_t a = nullptr, z = nullptr;
+    cudaError_t e = cudaMalloc(&idx, sizeof(uint32_t) * (size_t)n_ops);
+    if (e == cudaSuccess) e = cudaMalloc(&J, sizeof(float2) * (size_t)n_targets);
+    if (e == cudaSuccess) e = cudaMemset(J, 0, sizeof(float2) * (size_t)n_targets);
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&z);
+    if (e == cudaSuccess) {
+        k_probe_fill<<<grid_for(n_ops, 256), 256>>>(idx, n_ops, (uint32_t)n_targets,
+                                                    (uint32_t)std::min<int64_t>(window, n_targets), 12345u);
+        for (int w = 0; w < 2; ++w) k_probe_red<<<sms * 16, 256>>>(idx, n_ops, J);
+        cudaEventRecord(a);
+        for (int r = 0; r < 10; ++r) k_probe_red<<<sms * 16, 256>>>(idx, n_ops, J);
+        cudaEventRecord(z);
+        e = cudaEventSynchronize(z);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, z);
+        *ms_out = ms / 10.0f;
+    }
+    if (a) cudaEventDestroy(a);
+    if (z) cudaEventDestroy(z);
+    cudaFree(idx);
+    cudaFree(J);
+    if (e != cudaSuccess) return fail(DTB_ERR_CUDA, "atomic-rate probe: %s", cudaGetErrorString(e));
+    return DTB_OK;
+}
+
 int dtb_block_update_conn_weight(dtb_block* b, int64_t n, const uint8_t* channel, const uint32_t* post,
                                  const uint32_t* pre, const float* value)
 {

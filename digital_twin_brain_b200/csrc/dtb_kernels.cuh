@@ -1504,4 +1504,25 @@ __global__ void k_fill4(float4* p, int64_t n, float4 val)
     if (i < n) p[i] = val;
 }
 
+// ------------------------------------------------------------ atomic-rate probe
+// The push scatter's ceiling: float2 atomics at n_ops targets drawn inside a
+// window of `window` neurons that moves with the op index (a region's
+// intra-region synapses), or anywhere in [0, n) when window >= n.
+__global__ void k_probe_fill(uint32_t* idx, int64_t n_ops, uint32_t n, uint32_t window, uint32_t seed)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_ops) return;
+    uint32_t x = (uint32_t)i * 2654435761u ^ seed;
+    x ^= x >> 13; x *= 0x5bd1e995u; x ^= x >> 15;
+    const uint32_t w = window < n ? window : n;
+    const uint32_t start = (uint32_t)(((uint64_t)(i / 100) * 100u) % n);
+    idx[i] = (uint32_t)(((uint64_t)start + (x % w)) % n);
+}
+
+__global__ void k_probe_red(const uint32_t* __restrict__ idx, int64_t n_ops, float2* J)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_ops; i += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(J + __ldcs(idx + i), make_float2(1.0f, 0.5f));
+}
+
 }  // namespace dtb

@@ -296,6 +296,14 @@ int dtb_block_gamma_property_by_subblock(dtb_block* b, int n, const int32_t* sub
 int dtb_block_set_input_spikes(dtb_block* b, int64_t n_src, const uint32_t* neurons, int64_t T,
                                const uint8_t* spikes);
 
+/* Measurement helper, no counterpart in the reference: the rate of float2
+ * atomic additions (the push scatter's per-synapse operation) on `device`,
+ * n_ops of them into n_targets float2 targets, each target drawn inside a
+ * window of `window` consecutive targets that moves with the operation index
+ * (window >= n_targets: anywhere).  ms_out = milliseconds for the n_ops.
+ * Allocates and frees its own device buffers. */
+int dtb_measure_atomic_rate(int device, int64_t n_targets, int64_t n_ops, int64_t window, float* ms_out);
+
 /* models/block.py:172-177 block.update_conn_weight: set the channel weight
  * of existing synapses (channel[i], post[i], pre[i]) to value[i]. */
 int dtb_block_update_conn_weight(dtb_block* b, int64_t n, const uint8_t* channel, const uint32_t* post,
