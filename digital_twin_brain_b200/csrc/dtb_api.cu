@@ -557,19 +557,19 @@ static void launch_step_m(dtb_block* b, const DevState& s)
 // Update with staged (bulk-copied, one tile ahead) state loads: split J planes
 // whose second plane starts on 16 bytes (even plane stride).  M = resident
 // CTAs per SM its registers are budgeted for.
-template <int G, bool U, bool F, int M>
+template <bool U, bool F, int M>
 static void launch_step_staged(dtb_block* b, const DevState& s)
 {
     static int per_sm = 0;
     if (!per_sm) {
-        cudaFuncSetAttribute(k_step<G, U, F, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<G, U, F, M, true>, kStepThreads, kStagedSmem);
+        cudaFuncSetAttribute(k_step<0, U, F, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStagedSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<0, U, F, M, true>, kStepThreads, kStagedSmem);
         if (per_sm < 1) per_sm = 1;
     }
     unsigned grid;
     int tpw;
     step_grid(b, per_sm, grid, tpw);
-    k_step<G, U, F, M, true><<<grid, kStepThreads, kStagedSmem, b->stream>>>(s, tpw);
+    k_step<0, U, F, M, true><<<grid, kStepThreads, kStagedSmem, b->stream>>>(s, tpw);
 }
 
 static bool staged_layout(const DevState& s) { return s.j_es == 1 && s.j_ps >= s.N && (s.j_ps % 2) == 0; }
@@ -577,9 +577,9 @@ static bool staged_layout(const DevState& s) { return s.j_es == 1 && s.j_ps >= s
 template <int G, bool U, bool F>
 static void launch_step(dtb_block* b, const DevState& s)
 {
-    if constexpr (U && (G == 0 || G == kGatherSlots)) {
-        if (b->step_variant == 2 && staged_layout(s)) { launch_step_staged<G, U, F, 2>(b, s); return; }
-        if (b->step_variant == 3 && staged_layout(s)) { launch_step_staged<G, U, F, 3>(b, s); return; }
+    if constexpr (G == 0) {
+        if (b->step_variant == 2 && staged_layout(s)) { launch_step_staged<U, F, 2>(b, s); return; }
+        if (b->step_variant == 3 && staged_layout(s)) { launch_step_staged<U, F, 3>(b, s); return; }
     }
     if (b->step_variant == 1) launch_step_m<G, U, F, 3>(b, s);
     else launch_step_m<G, U, F, 2>(b, s);
@@ -650,9 +650,8 @@ static int launch_scatter(dtb_block* b, const DevState& s, int how = kScatterJ)
     const unsigned grid = grid_for(warps * 32, kScatterThreads);
     if (grid == 0) return DTB_OK;
     const size_t smem = sizeof(uint32_t) * 32 * (size_t)wpw * (kScatterThreads / 32);   // <= 32 KB
-    // the ordered scatters wait on returned slot claims: fewer synapses per lane, more warps
-    if (how == kScatterSlots) k_scatter<kScatterSlots, 6, 4><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
-    else if (how == kScatterMasks) k_scatter<kScatterMasks, 6, 4><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
+    if (how == kScatterSlots) k_scatter<kScatterSlots><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
+    else if (how == kScatterMasks) k_scatter<kScatterMasks><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
     else if (b->scatter_variant == 1) k_scatter<kScatterJ, 6><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
     else k_scatter<kScatterJ><<<grid, kScatterThreads, smem, b->stream>>>(s, wpw);
     CK(cudaGetLastError());

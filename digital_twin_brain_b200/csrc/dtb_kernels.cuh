@@ -347,8 +347,7 @@ __global__ void k_samples(DevState s)
 // tile's V, t_last, class ids and both J planes into shared memory, issued by
 // lane 0 one tile ahead, so that the loads of tile k+1 are in flight while tile
 // k computes.  Completion is counted on a per-warp, per-buffer mbarrier.
-constexpr int kStageState = kWarpNeurons * (4 + 4 + 4 + 8 + 8);   // V, t_last, class, J planes: 3584
-constexpr int kStageBytes = kStageState + kWarpNeurons * 4;         // + ordered-push slot counts: 4096
+constexpr int kStageBytes = kWarpNeurons * (4 + 4 + 4 + 8 + 8);   // 3584 per tile buffer
 constexpr int kStagedSmem = (kStepThreads / 32) * 2 * kStageBytes;
 constexpr uint32_t kErrStageTimeout = 1u;                        // Ctl::err bit
 
@@ -364,19 +363,17 @@ __device__ __forceinline__ void stage_issue(uint32_t dst, const void* src, uint3
 }
 
 // Lane 0: the five copies of tile `base` into buffer `buf` (16-byte aligned, whole tile).
-__device__ __forceinline__ void stage_tile(const DevState& s, int64_t base, unsigned char* buf, uint32_t mbar,
-                                           bool with_cnt)
+__device__ __forceinline__ void stage_tile(const DevState& s, int64_t base, unsigned char* buf, uint32_t mbar)
 {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier generic reads of buf first
-    const uint32_t bytes = with_cnt ? (uint32_t)kStageBytes : (uint32_t)kStageState;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(bytes) : "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"((uint32_t)kStageBytes)
+                 : "memory");
     const uint32_t d = smem_u32(buf);
     stage_issue(d, s.V + base, kWarpNeurons * 4, mbar);
     stage_issue(d + kWarpNeurons * 4, s.tlast + base, kWarpNeurons * 4, mbar);
     stage_issue(d + kWarpNeurons * 8, s.cls + base, kWarpNeurons * 4, mbar);
     stage_issue(d + kWarpNeurons * 12, s.J2 + base, kWarpNeurons * 8, mbar);
     stage_issue(d + kWarpNeurons * 20, s.J2 + s.j_ps + base, kWarpNeurons * 8, mbar);
-    if (with_cnt) stage_issue(d + kStageState, s.slot_cnt + base, kWarpNeurons * 4, mbar);
 }
 
 // Bounded wait for a buffer's copies; false after the limit (the caller then loads from global).
@@ -403,8 +400,7 @@ __device__ __forceinline__ bool stage_wait(uint32_t mbar, uint32_t parity)
 template <int GATHER, bool UPDATE, bool FORCED, int MINB = 2, bool STAGED = false>
 __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int tiles_per_warp)
 {
-    static_assert(!STAGED || GATHER == 0 || GATHER == kGatherSlots, "staged loads: plain update or slot sums");
-    constexpr bool kStageCnt = GATHER == kGatherSlots;
+    static_assert(!STAGED || GATHER == 0, "staged loads are for the update without gather");
     constexpr int kWarps = kStepThreads / 32;
     extern __shared__ __align__(128) unsigned char stage_smem[];   // STAGED: [warp][2][kStageBytes]
     __shared__ __align__(8) unsigned long long stage_bar[kWarps][2];
@@ -448,7 +444,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&stage_bar[wid][1])) : "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             if (tile0 < tile1 && (tile0 + 1) * kWarpNeurons <= s.N)
-                stage_tile(s, tile0 * kWarpNeurons, my_stage, smem_u32(&stage_bar[wid][0]), kStageCnt);
+                stage_tile(s, tile0 * kWarpNeurons, my_stage, smem_u32(&stage_bar[wid][0]));
         }
         __syncwarp();
     }
@@ -462,27 +458,13 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         if (STAGED) {
             if (lane == 0 && tile + 1 < tile1 && (tile + 2) * kWarpNeurons <= s.N)
                 stage_tile(s, base + kWarpNeurons, my_stage + (sb ^ 1) * kStageBytes,
-                           smem_u32(&stage_bar[wid][sb ^ 1]), kStageCnt);
+                           smem_u32(&stage_bar[wid][sb ^ 1]));
             if (base + kWarpNeurons <= s.N) {
                 staged = stage_wait(smem_u32(&stage_bar[wid][sb]), (uint32_t)((it >> 1) & 1));
                 if (!staged && lane == 0) atomicOr(&s.ctl->err, kErrStageTimeout);
             }
         }
         unsigned char* stage_buf = my_stage + sb * kStageBytes;
-        if (STAGED && !staged) {   // a partial tile (or a copy that timed out): this lane's own entries
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int64_t n = base + j * 32 + lane;
-                if (n >= s.N) continue;
-                const int k = j * 32 + lane;
-                reinterpret_cast<float*>(stage_buf)[k] = __ldcs(s.V + n);
-                reinterpret_cast<float*>(stage_buf + kWarpNeurons * 4)[k] = __ldcs(s.tlast + n);
-                reinterpret_cast<uint32_t*>(stage_buf + kWarpNeurons * 8)[k] = __ldcs(s.cls + n);
-                reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 12)[k] = __ldcs(s.J2 + n);
-                reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 20)[k] = __ldcs(s.J2 + s.j_ps + n);
-                if (kStageCnt) reinterpret_cast<uint32_t*>(stage_buf + kStageState)[k] = __ldcs(s.slot_cnt + n);
-            }
-        }
         if (GATHER == kGatherMasks) {
             // The warp lists every marked pull entry of its 128 neurons (a lane's entries
             // contiguous, neuron by neuron, excitatory then inhibitory, ascending position),
@@ -582,8 +564,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int64_t n = base + j * 32 + lane;
-                if (STAGED) cnt[j] = n < s.N ? reinterpret_cast<const uint32_t*>(stage_buf + kStageState)[j * 32 + lane] : 0u;
-                else cnt[j] = n < s.N ? __ldcs(s.slot_cnt + n) : 0u;
+                cnt[j] = n < s.N ? __ldcs(s.slot_cnt + n) : 0u;
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -617,17 +598,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int64_t n = base + j * 32 + lane;
-                if (n < s.N) {
-                    float4 J0;
-                    if (STAGED) {
-                        const float2 a = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 12)[j * 32 + lane];
-                        const float2 b2 = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 20)[j * 32 + lane];
-                        J0 = make_float4(a.x, a.y, b2.x, b2.y);
-                    } else {
-                        J0 = load_J(s, n);
-                    }
-                    Jn[j] = add4(J0, sum[j]);   // models/block.py:71-73
-                }
+                if (n < s.N) Jn[j] = add4(load_J(s, n), sum[j]);   // models/block.py:71-73
             }
             if (!UPDATE) {
 #pragma unroll
@@ -681,7 +652,16 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             c_in[j] = 0u;          // class 0 exists whenever N > 0: keeps the shuffle below in bounds
             if (valid[j]) {
                 if (STAGED) {
-                    // the tile's state lives in the stage buffer
+                    // the tile's state lives in the stage buffer: the copies' (or, for a
+                    // partial tile, this lane's own loads, written below)
+                    if (!staged) {
+                        const int k = j * 32 + lane;
+                        reinterpret_cast<float*>(stage_buf)[k] = __ldcs(s.V + n);
+                        reinterpret_cast<float*>(stage_buf + kWarpNeurons * 4)[k] = __ldcs(s.tlast + n);
+                        reinterpret_cast<uint32_t*>(stage_buf + kWarpNeurons * 8)[k] = __ldcs(s.cls + n);
+                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 12)[k] = __ldcs(s.J2 + n);
+                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 20)[k] = __ldcs(s.J2 + s.j_ps + n);
+                    }
                 } else {
                     v_in[j] = __ldcs(s.V + n);
                     tl_in[j] = __ldcs(s.tlast + n);
@@ -730,13 +710,9 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 const int k = j * 32 + lane;
                 v = reinterpret_cast<const float*>(stage_buf)[k];
                 tl = reinterpret_cast<const float*>(stage_buf + kWarpNeurons * 4)[k];
-                if (GATHER) {
-                    J = Jn[j];
-                } else {
-                    const float2 a = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 12)[k];
-                    const float2 b2 = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 20)[k];
-                    J = make_float4(a.x, a.y, b2.x, b2.y);
-                }
+                const float2 a = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 12)[k];
+                const float2 b2 = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 20)[k];
+                J = make_float4(a.x, a.y, b2.x, b2.y);
             } else {
                 v = v_in[j];
                 tl = tl_in[j];
@@ -891,7 +867,7 @@ constexpr int kScatterJ = 0, kScatterSlots = 1, kScatterMasks = 2;
 
 // MINB: resident CTAs per SM the registers are budgeted for; the row lists take
 // wpw * 32 entries per warp of dynamic shared memory.
-template <int MODE, int MINB = 1, int U = kScatterUnroll>
+template <int MODE, int MINB = 1>
 __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, int wpw)
 {
     extern __shared__ uint32_t sh_rows_dyn[];
@@ -936,13 +912,13 @@ __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, i
         }
         const int64_t T = __shfl_sync(0xffffffffu, off, 31);
         const int64_t start = off - len;           // exclusive offset of this lane's row
-        for (int64_t v0 = 0; v0 < T; v0 += 32 * U) {
-            uint32_t c[U];
-            float2 w[U];
-            uint32_t ppos[U];
-            bool ok[U];
+        for (int64_t v0 = 0; v0 < T; v0 += 32 * kScatterUnroll) {
+            uint32_t c[kScatterUnroll];
+            float2 w[kScatterUnroll];
+            uint32_t ppos[kScatterUnroll];
+            bool ok[kScatterUnroll];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
+            for (int u = 0; u < kScatterUnroll; ++u) {
                 const int64_t v = v0 + u * 32 + lane;
                 // row of v: number of rows whose inclusive offset is <= v
                 int lo = 0;
@@ -964,26 +940,26 @@ __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, i
             }
             if (MODE == kScatterMasks) {
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < kScatterUnroll; ++u)
                     if (ok[u])
                         atomicOr(s.pmask + (int64_t)(c[u] & kIndexMask) * (2 * kMaskWords) +
                                      ((c[u] & kKindBit) ? kMaskWords : 0) + (ppos[u] >> 5),
                                  1u << (ppos[u] & 31));
             } else if (MODE == kScatterSlots) {
                 // every slot claim of the batch first, so their round trips overlap
-                uint32_t k[U];
+                uint32_t k[kScatterUnroll];
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < kScatterUnroll; ++u)
                     k[u] = ok[u] ? atomicAdd(s.slot_cnt + (c[u] & kIndexMask), 1u) : kSlotCap;
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < kScatterUnroll; ++u)
                     if (k[u] < kSlotCap)
                         __stcg(s.slots + (int64_t)(c[u] & kIndexMask) * kSlotCap + k[u],
                                make_uint4(ppos[u] | (c[u] & kKindBit), 0u, __float_as_uint(w[u].x),
                                           __float_as_uint(w[u].y)));
             } else {
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < kScatterUnroll; ++u)
                     if (ok[u])
                         atomicAdd(s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + (int64_t)(c[u] & kIndexMask) * s.j_es, w[u]);
             }

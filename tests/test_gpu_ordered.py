@@ -128,23 +128,3 @@ def test_masks_refused_beyond_128_inputs():
     with pytest.raises(DtbError):
         net.set_tuning(TUNE_PULL_METHOD, MASKS)
     net.run(20, noise_rate=0.02, mode="pull")      # auto: slots (in-degree 200 > 128)
-
-
-@pytest.mark.parametrize("variant", [2, 3])
-@pytest.mark.parametrize("rate,K", [(0.01, 100), (0.05, 120)], ids=["sparse", "overflowing_rows"])
-def test_staged_slot_sums_equal_row_gather(rate, K, variant):
-    """The slot sums with the next tile's state and slot counts bulk-copied into shared memory."""
-    from digital_twin_brain_b200._lib import TUNE_STEP_VARIANT
-    spec = synthetic.whole_brain(R=6, mean_size=700, sigma=0.5, K=K, gen_seed=4, name=f"wb6s_K{K}")
-    a = Network.from_spec(spec, device=0)
-    b = Network.from_spec(spec, device=0)
-    a.set_tuning(TUNE_PULL_METHOD, ROWS)
-    b.set_tuning(TUNE_PULL_METHOD, SLOTS)
-    b.set_tuning(TUNE_STEP_VARIANT, variant)
-    for n in (1, 37, 64):
-        sa, ma, na = a.run(n, noise_rate=rate, mode="pull")
-        sb, mb, nb = b.run(n, noise_rate=rate, mode="pull")
-        assert np.array_equal(sa, sb) and np.array_equal(na, nb)
-        for x, y in zip(_state(a), _state(b)):
-            assert np.array_equal(x, y)
-    b.synchronize()
