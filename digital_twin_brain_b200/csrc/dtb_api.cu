@@ -131,6 +131,7 @@ struct dtb_block {
     uint32_t stream_id = 0;
     DevState ds{};
     std::vector<void*> allocs;
+    std::vector<size_t> alloc_bytes;
     int64_t dev_bytes = 0;
     // host mirrors
     std::vector<ParamClass> classes;
@@ -201,9 +202,27 @@ static int dalloc(dtb_block* b, T** p, size_t count)
                     cudaGetErrorString(e), (long long)b->dev_bytes);
     }
     b->allocs.push_back(q);
+    b->alloc_bytes.push_back(bytes);
     b->dev_bytes += (int64_t)bytes;
     *p = reinterpret_cast<T*>(q);
     return DTB_OK;
+}
+
+// Frees one allocation of the handle (after its stream is idle).
+template <typename T>
+static void dfree(dtb_block* b, T*& p)
+{
+    if (!p) return;
+    void* q = const_cast<void*>(reinterpret_cast<const void*>(p));
+    for (size_t i = 0; i < b->allocs.size(); ++i) {
+        if (b->allocs[i] != q) continue;
+        cudaFree(q);
+        b->dev_bytes -= (int64_t)b->alloc_bytes[i];
+        b->allocs[i] = b->allocs.back(); b->allocs.pop_back();
+        b->alloc_bytes[i] = b->alloc_bytes.back(); b->alloc_bytes.pop_back();
+        break;
+    }
+    p = nullptr;
 }
 
 static int ensure_pinned(dtb_block* b, size_t bytes)
@@ -1886,13 +1905,12 @@ int dtb_block_set_input_spikes(dtb_block* b, int64_t n_src, const uint32_t* neur
     if (!b || n_src < 0 || (n_src > 0 && (!neurons || !spikes || T < 1))) return fail(DTB_ERR_ARG, "bad argument");
     DeviceGuard g(b->device);
     DevState& s = b->ds;
-    if (n_src == 0) {
-        s.n_src = 0;
-        s.forced_active = nullptr;
-        s.forced_mask = nullptr;
-        drop_graphs(b);
-        return DTB_OK;
-    }
+    CK(cudaStreamSynchronize(b->stream));   // the previous buffers are no longer in use
+    drop_graphs(b);
+    s.n_src = 0;
+    s.forced_active = nullptr;
+    dfree(b, s.forced_mask); dfree(b, s.src_neuron); dfree(b, s.src_raster); dfree(b, s.src_val);
+    if (n_src == 0) return DTB_OK;
     std::vector<uint32_t> mask((size_t)s.n_words, 0u);
     for (int64_t i = 0; i < n_src; ++i) {
         if (neurons[i] >= (uint64_t)b->N) return fail(DTB_ERR_ARG, "input %lld: neuron %u out of range", (long long)i, neurons[i]);
@@ -2281,11 +2299,14 @@ int dtb_block_set_samples(dtb_block* b, int n, const uint32_t* idx, int64_t capa
     if (!b || n < 0 || (n > 0 && (!idx || capacity_steps < 1))) return fail(DTB_ERR_ARG, "bad argument");
     DeviceGuard g(b->device);
     DevState& s = b->ds;
-    s.n_samples = 0;
-    b->samples_written = 0;
-    if (n == 0) { drop_graphs(b); return DTB_OK; }
     for (int i = 0; i < n; ++i)
         if (idx[i] >= (uint64_t)b->N) return fail(DTB_ERR_ARG, "sample %d: neuron %u out of range", i, idx[i]);
+    CK(cudaStreamSynchronize(b->stream));   // the previous buffers are no longer in use
+    drop_graphs(b);
+    s.n_samples = 0;
+    b->samples_written = 0;
+    dfree(b, s.samples); dfree(b, s.samp_spk); dfree(b, s.samp_v);
+    if (n == 0) return DTB_OK;
     uint32_t* di = nullptr; uint8_t* sp = nullptr; float* sv = nullptr;
     RET(dalloc(b, &di, (size_t)n));
     RET(dalloc(b, &sp, (size_t)n * (size_t)capacity_steps));

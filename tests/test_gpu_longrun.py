@@ -96,6 +96,7 @@ def test_samples_subset_and_ring():
         ref_sp[i] = ob.active[idx]
         ref_v[i] = ob.V[idx]
     net = Network.from_spec(spec, device=0)
+    net.set_samples(np.arange(50), 1000)          # replaced (and freed) by the next call
     net.set_samples(idx, cap)
     net.run(100, 0.01, mode="pull", out=None)
     sp, v = net.get_samples()

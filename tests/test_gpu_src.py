@@ -50,3 +50,17 @@ def test_input_neurons_bit_exact_vs_reference(stepwise):
         b.run(noise_rate=0.01)
     with pytest.raises(DtbError):         # and so does the C ABI
         b.network.run(1, 0.01)
+
+
+def test_input_neurons_replaced_and_removed():
+    g = np.load(os.path.join(GOLDEN, "src_block_ref.npz"))
+    b = block(torch.from_numpy(g["prop"]), _w(g), delta_t=float(g["dt"]), src=torch.from_numpy(g["src"]),
+              seed=int(g["seed"]), device=0)
+    net = b.network
+    n_src = g["src"].shape[0]
+    before = net.info().device_bytes
+    net.set_input_spikes(np.arange(n_src), g["src"])        # replaced: same footprint afterwards
+    assert net.info().device_bytes == before
+    net.run(10, 0.01)
+    net.set_input_spikes([], None)                            # removed: the network runs free
+    net.run(500, 0.01)
