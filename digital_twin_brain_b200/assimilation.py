@@ -165,6 +165,12 @@ class EnsembleDA:
         self.hidden = self.hidden_state(self.evolve())
         return self.hidden
 
+    def get_bold_state(self) -> torch.Tensor:
+        """The (member, region) BOLD states s, q, v, f_in as [M, R, 4] (float64, device)."""
+        idx = self.region_idx.reshape(-1)
+        cols = [torch.from_numpy(self.net.get_bold(f)[idx]) for f in ("s", "q", "v", "f_in")]
+        return torch.stack(cols, dim=-1).reshape(self.M, self.R, 4).to(self.dev)
+
     def set_bold_state(self, sqvf: torch.Tensor):
         """bold.state_update (bold_model_pytorch.py:34-41) for the (member, region) BOLD states."""
         idx = self.region_idx.reshape(-1)
@@ -227,7 +233,8 @@ class SurrogateDA:
     """
 
     def __init__(self, template: synthetic.NetworkSpec, cfg: DAConfig, surrogate, n_judge: int = 16,
-                 threshold: float = 0.3, device: int = 0, adapt_steps: int = 0, adapt_lr: float = 5e-4):
+                 threshold: float = 0.3, device: int = 0, adapt_steps: int = 0, adapt_lr: float = 5e-4,
+                 bias_correct: bool = False):
         from .network import BoldModel
         from .surrogate import HISTORY
         self.cfg = cfg
@@ -247,6 +254,11 @@ class SurrogateDA:
         self.full = None   # fallback simulator for the surrogate members (built on first use)
         self.bold = BoldModel(n_regions=(self.M - self.J) * self.R, dtype=torch.float64, delta_t=template.dt / 1000.0,
                               device=device)
+        # bias_correct: the judges' BOLD is also integrated from their surrogate rates; the mean
+        # difference to their simulated BOLD (per region) corrects the surrogate members' BOLD
+        self.bias_correct = bias_correct
+        self.jbold = BoldModel(n_regions=self.J * self.R, dtype=torch.float64, delta_t=template.dt / 1000.0,
+                               device=device) if bias_correct else None
         self.low = self.judge.low
         self.high = self.judge.high
         self.gen = torch.Generator(device=self.dev)
@@ -311,6 +323,7 @@ class SurrogateDA:
         # judges: simulator
         self.judge.hp_log = self.hp_log[:self.J].clone()
         self.judge.apply_hp()
+        jstate = self.judge.get_bold_state() if self.bias_correct else None
         out_j = self.judge.evolve()
         rates_j = torch.from_numpy(self.judge.window_rates()).to(self.dev).float()
         # surrogate forecast of every member's window rate
@@ -331,6 +344,13 @@ class SurrogateDA:
         else:
             rates_s = pred[self.J:]
             sig = self.bold.run_steps(rates_s.reshape(-1).double(), cfg.steps_per_window, 1e-5)
+            if self.bias_correct:
+                for k in range(4):
+                    v = jstate[:, :, k].reshape(-1)
+                    self.jbold.set(k, v if k == 0 else torch.clamp(v, min=1e-5))
+                sig_j = self.jbold.run_steps(pred[:self.J].reshape(-1).double(), cfg.steps_per_window, 1e-5)
+                bias = (out_j[:, :, 5].double() - sig_j.reshape(self.J, self.R)).mean(0)      # [R]
+                sig = (sig.reshape(self.M - self.J, self.R) + bias).reshape(-1)
             st = [self.bold.get(k).float() for k in range(4)]
             out_s = torch.stack([rates_s.reshape(-1)] + st + [sig.float()], dim=-1).reshape(self.M - self.J, self.R, 6)
         out6 = torch.cat([out_j, out_s], dim=0)
