@@ -166,11 +166,11 @@ struct dtb_block {
     int step_variant = 0;         // 0: 2 resident CTAs/SM register budget, 1: 3
     // ordered push (bit-exact pull through per-neuron slots)
     bool has_qpos = false;
-    int pull_method = 0;          // 0: auto, 1: row gather, 2: ordered push (slots), 3: ordered push (masks)
+    int pull_method = 0;          // 0: auto, 1: row gather, 2: ordered push (slots), 3: (masks), 4: streamed gather
     double slot_threshold = 0.1;
     // graphs: one chunk graph per propagation method (push, pull rows, pull slots)
-    cudaGraphExec_t graph[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    int graph_len[5] = {0, 0, 0, 0, 0};
+    cudaGraphExec_t graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    int graph_len[6] = {0, 0, 0, 0, 0, 0};
     bool use_graphs = true;
     // attached BOLD
     int bold_R = 0;
@@ -539,7 +539,11 @@ static int launch_stats(dtb_block* b, const DevState& s)
 // Persistent step kernels: as many CTAs as are resident at once, each warp
 // streaming a contiguous run of tiles.
 // Dynamic shared memory of the step kernels: the mask gather's per-warp entry lists.
-static constexpr int step_dyn_smem(int g) { return g == kGatherMasks ? (kStepThreads / 32) * kMaskList * 10 : 0; }
+static constexpr int step_dyn_smem(int g)
+{
+    return g == kGatherMasks ? (kStepThreads / 32) * kMaskList * 10
+                             : (g == kGatherStream ? (kStepThreads / 32) * kStreamWarpBytes : 0);
+}
 
 template <int G, bool U, bool F, int M>
 static int step_blocks_per_sm()
@@ -637,11 +641,13 @@ static int launch_update(dtb_block* b, const DevState& s, int gather, bool force
         if (gather == kGatherRows) launch_step<kGatherRows, true, true>(b, s);
         else if (gather == kGatherSlots) launch_step<kGatherSlots, true, true>(b, s);
         else if (gather == kGatherMasks) launch_step<kGatherMasks, true, true>(b, s);
+        else if (gather == kGatherStream) launch_step<kGatherStream, true, true>(b, s);
         else launch_step<0, true, true>(b, s);
     } else {
         if (gather == kGatherRows) launch_step<kGatherRows, true, false>(b, s);
         else if (gather == kGatherSlots) launch_step<kGatherSlots, true, false>(b, s);
         else if (gather == kGatherMasks) launch_step<kGatherMasks, true, false>(b, s);
+        else if (gather == kGatherStream) launch_step<kGatherStream, true, false>(b, s);
         else launch_step<0, true, false>(b, s);
     }
     CK(cudaGetLastError());
@@ -655,6 +661,7 @@ static int launch_gather_only(dtb_block* b, const DevState& s, int gather = kGat
     if (s.N <= 0) return DTB_OK;
     if (gather == kGatherSlots) launch_step<kGatherSlots, false, false>(b, s);
     else if (gather == kGatherMasks) launch_step<kGatherMasks, false, false>(b, s);
+    else if (gather == kGatherStream) launch_step<kGatherStream, false, false>(b, s);
     else launch_step<kGatherRows, false, false>(b, s);
     CK(cudaGetLastError());
     b->launches++;
@@ -687,6 +694,7 @@ static void drop_graphs(dtb_block* b)
 // the ordered push that DTB_MODE_PULL resolves to while activity is low.
 constexpr int kModeSlots = 3;
 constexpr int kModeMasks = 4;
+constexpr int kModeStream = 5;
 
 static int ensure_slots(dtb_block* b)
 {
@@ -738,9 +746,10 @@ static int enqueue_steps(dtb_block* b, int n, int mode)
         }
         RET(launch_gather_only(b, s, g));
     } else {
+        const int g = mode == kModeStream ? kGatherStream : kGatherRows;
         RET(launch_update(b, s, 0, false));
-        for (int k = 1; k < n; ++k) RET(launch_update(b, s, kGatherRows, false));
-        RET(launch_gather_only(b, s));
+        for (int k = 1; k < n; ++k) RET(launch_update(b, s, g, false));
+        RET(launch_gather_only(b, s, g));
     }
     return DTB_OK;
 }
@@ -783,11 +792,12 @@ static int choose_mode(dtb_block* b, int mode)
 // positions and activity is low enough that rows rarely overflow their slots.
 static int resolve_method(dtb_block* b, int m)
 {
-    if (m != DTB_MODE_PULL || !b->has_qpos || !b->has_push || b->pull_method == 1) return m;
+    if (m != DTB_MODE_PULL || b->pull_method == 1) return m;
+    if (b->pull_method == 4 || !b->has_qpos || !b->has_push) return kModeStream;
     if (b->pull_method == 2) return kModeSlots;
     if (b->pull_method == 3) return kModeMasks;
     const double f = b->last_frac < 0.0 ? 0.0 : b->last_frac;
-    return f <= b->slot_threshold ? kModeSlots : m;   // slots measured faster than masks on B200
+    return f <= b->slot_threshold ? kModeSlots : kModeStream;   // slots measured faster than masks on B200
 }
 
 static int ensure_method(dtb_block* b, int mm)
@@ -1440,11 +1450,12 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
             rec(k); rc = launch_gather_only(b, b->ds, g); rec(k + 1); kind.push_back(2); k += 2;
         }
     } else {
+        const int g = m == kModeStream ? kGatherStream : kGatherRows;
         rec(k); rc = launch_update(b, b->ds, 0, false); rec(k + 1); kind.push_back(0); k += 2;
         for (int st = 1; st < n_steps && rc == DTB_OK && k + 4 <= n_ev; ++st) {
-            rec(k); rc = launch_update(b, b->ds, kGatherRows, false); rec(k + 1); kind.push_back(0); k += 2;
+            rec(k); rc = launch_update(b, b->ds, g, false); rec(k + 1); kind.push_back(0); k += 2;
         }
-        if (rc == DTB_OK) { rec(k); rc = launch_gather_only(b, b->ds); rec(k + 1); kind.push_back(1); k += 2; }
+        if (rc == DTB_OK) { rec(k); rc = launch_gather_only(b, b->ds, g); rec(k + 1); kind.push_back(1); k += 2; }
         done_steps = (int)kind.size() - 1;
     }
     b->steps += (uint64_t)done_steps;
@@ -1488,8 +1499,8 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         b->ds.j_keep = (int)value;
         break;
     case DTB_TUNE_PULL_METHOD:
-        if (value < 0 || value > 3)
-            return fail(DTB_ERR_ARG, "pull method must be 0 (auto), 1 (rows), 2 (ordered push, slots) or 3 (masks)");
+        if (value < 0 || value > 4)
+            return fail(DTB_ERR_ARG, "pull method must be 0 (auto), 1 (rows), 2 (slots), 3 (masks) or 4 (streamed)");
         if (value >= 2 && !b->has_qpos) return fail(DTB_ERR_STATE, "ordered push needs the push CSR with pull-row positions");
         if (value == 3 && !masks_possible(b))
             return fail(DTB_ERR_STATE, "position masks hold in-degrees up to %d (max in-degree %lld)", 32 * kMaskWords,

@@ -23,6 +23,8 @@ constexpr uint32_t kSlotCap = 8;       // ordered-push contributions kept per ne
 constexpr int kGatherRows = 1;         // k_step gathers whole pull rows
 constexpr int kGatherSlots = 2;        // k_step sums its ordered-push slots
 constexpr int kGatherMasks = 3;        // k_step sums the pull entries its position masks mark
+constexpr int kGatherStream = 4;       // k_step streams its tile's pull entries, chunk by chunk
+constexpr int kStreamWarpBytes = 129 * 8 + 8 + 128 * 16;   // row pointers (+pad) and row sums per warp
 constexpr int kMaskWords = 4;          // position-mask words per kind: in-degree up to 128
 constexpr int kMaskList = 256;         // marked entries a warp gathers together per tile
 constexpr int kStepThreads = 256;      // 8 warps, 1024 neurons per CTA

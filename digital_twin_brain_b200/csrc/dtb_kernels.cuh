@@ -608,6 +608,82 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 }
                 continue;
             }
+        } else if (GATHER == kGatherStream) {
+            // The warp streams the pull entries of its 128 rows in 32-entry chunks (coalesced
+            // index loads, 4 chunks in flight), tests their presynaptic bits and, for the
+            // firing ones, adds the weights to the row sums in entry order: the row order of
+            // gather_row, for every row at once.  Lane 0 does the (rare) additions.
+            int64_t* rp = reinterpret_cast<int64_t*>(stage_smem + (size_t)wid * kStreamWarpBytes);
+            float4* acc = reinterpret_cast<float4*>(stage_smem + (size_t)wid * kStreamWarpBytes + 129 * 8 + 8);
+            const int nrows = (int)(s.N - base < kWarpNeurons ? s.N - base : kWarpNeurons);
+            for (int i = lane; i <= nrows; i += 32) rp[i] = __ldg(s.prow + base + i);
+            for (int i = lane; i < kWarpNeurons; i += 32) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            __syncwarp();
+            const int64_t e0 = rp[0], e1 = rp[nrows];
+            uint32_t events = 0;
+            constexpr int UC = 4;
+            for (int64_t c = e0; c < e1; c += 32 * UC) {
+                uint32_t col[UC];
+                bool act[UC];
+#pragma unroll
+                for (int u = 0; u < UC; ++u) {
+                    const int64_t e = c + u * 32 + lane;
+                    col[u] = e < e1 ? __ldcs(s.pcol + e) : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < UC; ++u) {
+                    const int64_t e = c + u * 32 + lane;
+                    act[u] = e < e1 && test_bit(gbits, col[u] & kIndexMask);
+                }
+#pragma unroll
+                for (int u = 0; u < UC; ++u) {
+                    unsigned m = __ballot_sync(0xffffffffu, act[u]);
+                    if (!m) continue;
+                    const int64_t e = c + u * 32 + lane;
+                    float2 w = make_float2(0.f, 0.f);
+                    int r = 0;
+                    if (act[u]) {
+                        w = __ldg(s.pw + e);
+                        int lo = 0, hi = nrows;              // rp[lo] <= e < rp[hi]
+                        while (hi - lo > 1) {
+                            const int mid = (lo + hi) >> 1;
+                            if (rp[mid] <= e) lo = mid; else hi = mid;
+                        }
+                        r = lo;
+                    }
+                    events += __popc(m);
+                    while (m) {
+                        const int l = __ffs(m) - 1;
+                        m &= m - 1;
+                        const float wx = __shfl_sync(0xffffffffu, w.x, l);
+                        const float wy = __shfl_sync(0xffffffffu, w.y, l);
+                        const uint32_t cl = __shfl_sync(0xffffffffu, col[u], l);
+                        const int rl = __shfl_sync(0xffffffffu, r, l);
+                        if (lane == 0) {
+                            float4 a = acc[rl];
+                            if (cl & kKindBit) { a.z = __fadd_rn(a.z, wx); a.w = __fadd_rn(a.w, wy); }
+                            else { a.x = __fadd_rn(a.x, wx); a.y = __fadd_rn(a.y, wy); }
+                            acc[rl] = a;
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            if (!s.qrow) acc_ev += events;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                if (n < s.N) Jn[j] = add4(load_J(s, n), acc[j * 32 + lane]);   // models/block.py:71-73
+            }
+            __syncwarp();   // the row pointers and sums are rewritten by the next tile
+            if (!UPDATE) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t n = base + j * 32 + lane;
+                    if (n < s.N) store_J(s, n, Jn[j]);
+                }
+                continue;
+            }
         } else if (GATHER == kGatherRows) {
             float4 sum[4];
             uint32_t events = 0;

@@ -15,14 +15,14 @@ from tests.test_gpu_parity import class_decay_like_reference
 
 pytestmark = pytest.mark.gpu
 
-ROWS, SLOTS, MASKS = 1, 2, 3
+ROWS, SLOTS, MASKS, STREAM = 1, 2, 3, 4
 
 
 def _state(net):
     return [net.get(f) for f in (FIELD_V, FIELD_J, FIELD_T_LAST, FIELD_I_SYN, FIELD_ACTIVE)]
 
 
-@pytest.mark.parametrize("method", [SLOTS, MASKS], ids=["slots", "masks"])
+@pytest.mark.parametrize("method", [SLOTS, MASKS, STREAM], ids=["slots", "masks", "stream"])
 def test_ordered_push_matches_reference_golden(method):
     g = np.load(os.path.join(GOLDEN, "single_block_2k.npz"))
     spec = synthetic.config_single_block()
@@ -39,7 +39,7 @@ def test_ordered_push_matches_reference_golden(method):
     assert np.array_equal(net.get(FIELD_I_SYN), g["I_syn_final"])
 
 
-@pytest.mark.parametrize("method", [SLOTS, MASKS], ids=["slots", "masks"])
+@pytest.mark.parametrize("method", [SLOTS, MASKS, STREAM], ids=["slots", "masks", "stream"])
 @pytest.mark.parametrize("rate,K", [(0.01, 100), (0.05, 120), (0.3, 60)],
                          ids=["sparse", "overflowing_rows", "dense"])
 def test_ordered_push_equals_row_gather(rate, K, method):
@@ -67,8 +67,8 @@ def test_ordered_push_npz_positions_and_method_switches():
     a = Network.from_npz(d, dt=0.1, seed=11, device=0)
     b = Network.from_npz(d, dt=0.1, seed=11, device=0)
     a.set_tuning(TUNE_PULL_METHOD, ROWS)
-    for k, n in enumerate((20, 33, 7, 40, 11, 9)):
-        b.set_tuning(TUNE_PULL_METHOD, (SLOTS, ROWS, MASKS)[k % 3])
+    for k, n in enumerate((20, 33, 7, 40, 11, 9, 13, 5)):
+        b.set_tuning(TUNE_PULL_METHOD, (SLOTS, ROWS, MASKS, STREAM)[k % 4])
         sa, _, _ = a.run(n, noise_rate=0.02, mode="pull")
         sb, _, _ = b.run(n, noise_rate=0.02, mode="pull")
         assert np.array_equal(sa, sb)
@@ -109,12 +109,14 @@ def test_npz_hub_row_and_repeated_pairs(tmp_path):
     assert np.array_equal(qw, w[order])
     b = Network.from_npz(str(tmp_path), dt=0.1, seed=2, device=0)
     c = Network.from_npz(str(tmp_path), dt=0.1, seed=2, device=0)
+    d = Network.from_npz(str(tmp_path), dt=0.1, seed=2, device=0)
     a.set_tuning(TUNE_PULL_METHOD, ROWS)
     b.set_tuning(TUNE_PULL_METHOD, SLOTS)
     c.set_tuning(TUNE_PULL_METHOD, MASKS)
+    d.set_tuning(TUNE_PULL_METHOD, STREAM)
     for n in (50, 50):
         sa, _, na = a.run(n, noise_rate=0.05, mode="pull")
-        for other in (b, c):
+        for other in (b, c, d):
             so, _, no = other.run(n, noise_rate=0.05, mode="pull")
             assert np.array_equal(sa, so) and np.array_equal(na, no)
             for x, y in zip(_state(a), _state(other)):
