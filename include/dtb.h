@@ -225,9 +225,11 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          order; 3 = ordered push: firing rows set one bit per
  *                          pull-row position in per-neuron masks (in-degree up
  *                          to 128) and the next update sums the marked pull
- *                          entries in order (2 and 3 need the push CSR); 0 =
- *                          slots while at most 10 % of the neurons propagate,
- *                          else rows
+ *                          entries in order (2 and 3 need the push CSR); 4 =
+ *                          streamed gather: every warp streams its 128 rows'
+ *                          entries in coalesced chunks and adds the firing ones
+ *                          in row order; 0 = slots while at most 10 % of the
+ *                          neurons propagate, else the streamed gather
  * DTB_TUNE_J_CACHE         0 = the update streams J (evict first), 1 = its J
  *                          stores keep normal L2 priority for the scatter
  * DTB_TUNE_SCATTER_VARIANT push scatter registers: 0 = unbounded, 1 = budgeted
