@@ -234,7 +234,7 @@ class SurrogateDA:
 
     def __init__(self, template: synthetic.NetworkSpec, cfg: DAConfig, surrogate, n_judge: int = 16,
                  threshold: float = 0.3, device: int = 0, adapt_steps: int = 0, adapt_lr: float = 5e-4,
-                 bias_correct: bool = False):
+                 bias_correct: bool = False, spread: bool = False):
         from .network import BoldModel
         from .surrogate import HISTORY
         self.cfg = cfg
@@ -257,6 +257,9 @@ class SurrogateDA:
         # bias_correct: the judges' BOLD is also integrated from their surrogate rates; the mean
         # difference to their simulated BOLD (per region) corrects the surrogate members' BOLD
         self.bias_correct = bias_correct
+        # spread: surrogate rates get the judges' log-residual spread (mean-preserving lognormal
+        # noise), so the forecast ensemble keeps the variability simulated members have
+        self.spread = spread
         self.jbold = BoldModel(n_regions=self.J * self.R, dtype=torch.float64, delta_t=template.dt / 1000.0,
                                device=device) if bias_correct else None
         self.low = self.judge.low
@@ -343,6 +346,12 @@ class SurrogateDA:
             self.bold.set(2, out_s[:, :, 3].double()); self.bold.set(3, out_s[:, :, 4].double())
         else:
             rates_s = pred[self.J:]
+            if self.spread:
+                eps = 1e-6
+                res = torch.log(rates_j + eps) - torch.log(pred[:self.J] + eps)
+                sd = float(res.std())
+                z = torch.randn(rates_s.shape, generator=self.gen, device=self.dev)
+                rates_s = rates_s * torch.exp(sd * z - 0.5 * sd * sd)
             sig = self.bold.run_steps(rates_s.reshape(-1).double(), cfg.steps_per_window, 1e-5)
             if self.bias_correct:
                 for k in range(4):

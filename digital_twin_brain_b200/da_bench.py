@@ -48,7 +48,9 @@ def main(argv=None):
     ap.add_argument("--margin", type=float, default=1.5)
     ap.add_argument("--burn-in-windows", type=int, default=1,
                     help="judge windows before the assimilation (histories, surrogate adaptation); timed")
-    ap.add_argument("--bias-correct", type=int, default=1,
+    ap.add_argument("--spread", type=int, default=1,
+                    help="give the surrogate members' rates the judges' residual spread")
+    ap.add_argument("--bias-correct", type=int, default=0,
                     help="correct the surrogate members' BOLD by the judges' simulated-minus-surrogate mean")
     ap.add_argument("--adapt-steps", type=int, default=20,
                     help="Adam steps per window on the judges' windows (0: the surrogate stays as trained)")
@@ -138,7 +140,8 @@ def main(argv=None):
 
     # ---- surrogate-served DA
     sda = SurrogateDA(template, DAConfig(n_members=a.members, **base), sur, n_judge=a.judges,
-                      threshold=threshold, adapt_steps=a.adapt_steps, bias_correct=bool(a.bias_correct))
+                      threshold=threshold, adapt_steps=a.adapt_steps, bias_correct=bool(a.bias_correct),
+                      spread=bool(a.spread))
     sda.hp_random_initialize()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -149,7 +152,7 @@ def main(argv=None):
     out.update(summarize(res_s, "surrogate"))
     out.update(fallbacks=int(res_s["fallbacks"]), judge_err_mean=float(np.mean(res_s["errors"])),
                judge_err=[round(float(e), 4) for e in res_s["errors"]], adapt_steps=a.adapt_steps,
-               bias_correct=a.bias_correct)
+               bias_correct=a.bias_correct, spread=a.spread)
     out["surrogate_burn_in_s"] = t_burn
     out["burn_in_windows"] = a.burn_in_windows
     out["plain_total_s"] = float(np.sum(res_p["window_s"]))
