@@ -54,6 +54,12 @@ def test_surrogate_da_runs_with_judges_and_fallback():
     sda2 = SurrogateDA(TEMPLATE, cfg, sur, n_judge=4, threshold=1e9)    # never falls back
     res2 = sda2.run(obs)
     assert res2["fallbacks"] == 0 and np.isfinite(res2["bold_pred"]).all()
+    # adaptation, residual spread and judge-based BOLD correction on served windows
+    sda3 = SurrogateDA(TEMPLATE, cfg, sur, n_judge=4, threshold=1e9, adapt_steps=3, spread=True, bias_correct=True)
+    sda3.hp_random_initialize()
+    sda3.burn_in(2)
+    res3 = sda3.run(obs)
+    assert res3["fallbacks"] == 0 and np.isfinite(res3["bold_pred"]).all()
 
 
 def test_surrogate_adapt_lowers_loss_on_new_windows():
