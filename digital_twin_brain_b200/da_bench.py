@@ -48,7 +48,7 @@ def main(argv=None):
     ap.add_argument("--margin", type=float, default=1.5)
     ap.add_argument("--burn-in-windows", type=int, default=1,
                     help="judge windows before the assimilation (histories, surrogate adaptation); timed")
-    ap.add_argument("--spread", type=int, default=1,
+    ap.add_argument("--spread", type=int, default=0,
                     help="give the surrogate members' rates the judges' residual spread")
     ap.add_argument("--bias-correct", type=int, default=0,
                     help="correct the surrogate members' BOLD by the judges' simulated-minus-surrogate mean")
