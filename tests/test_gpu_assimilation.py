@@ -72,3 +72,22 @@ def test_surrogate_adapt_lowers_loss_on_new_windows():
     before = sur.adapt(g[1000:], h[1000:], t[1000:], steps=1)
     after = sur.adapt(g[1000:], h[1000:], t[1000:], steps=40)
     assert after < before
+
+
+def test_surrogate_beats_persistence_on_simulated_windows():
+    """Trained on windows this simulator generates, the surrogate forecasts held-out windows'
+    rates better than the method without it (the previous window's rate)."""
+    template = synthetic.whole_brain(R=8, mean_size=1500, sigma=0.3, K=60, gen_seed=5, name="da_sur",
+                                     g_ui=tuple(x * y for x, y in zip(synthetic.LIF["g_ui"], (2.0, 2.0, 1.0, 1.0))))
+    cfg = DAConfig(n_members=32, steps_per_window=1500, seed=4, hp_sigma=1.0)
+    g, h, t = collect_windows(template, cfg, windows=20)
+    n = g.shape[0]
+    perm = torch.from_numpy(np.random.default_rng(0).permutation(n))
+    tr, te = perm[: int(0.85 * n)], perm[int(0.85 * n):]
+    sur = RateSurrogate(seed=3)
+    sur.fit(g[tr], h[tr], t[tr], epochs=60)
+    eps = 1e-6
+    pred = sur.predict(g[te], h[te]).cpu()
+    err_net = float(torch.sqrt(torch.mean((torch.log(pred + eps) - torch.log(t[te] + eps)) ** 2)))
+    err_persist = float(torch.sqrt(torch.mean((torch.log(h[te][:, -1] + eps) - torch.log(t[te] + eps)) ** 2)))
+    assert err_net < 0.9 * err_persist, (err_net, err_persist)
