@@ -830,14 +830,17 @@ static int emit_stats(dtb_block* b, int rows, int64_t row0, float* sum_out, floa
     }
     const bool need_host = where == DTB_HOST || nact_host;
     if (need_host) {
-        RET(ensure_pinned(b, 2 * bs + bn + 64));
+        RET(ensure_pinned(b, 2 * bs + bn + 64));   // + the error word
         char* p = reinterpret_cast<char*>(b->pinned);
         if (where == DTB_HOST && bs) {
             if (sum_out) CK(cudaMemcpyAsync(p, b->ds.st_spk, bs, cudaMemcpyDeviceToHost, b->stream));
             if (mean_out) CK(cudaMemcpyAsync(p + bs, b->ds.st_mean, bs, cudaMemcpyDeviceToHost, b->stream));
         }
         CK(cudaMemcpyAsync(p + 2 * bs, b->ds.st_nact, bn, cudaMemcpyDeviceToHost, b->stream));
+        uint32_t* herr = reinterpret_cast<uint32_t*>(p + ((2 * bs + bn + 7) & ~(size_t)7));
+        CK(cudaMemcpyAsync(herr, &b->ds.ctl->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream));
         CK(cudaStreamSynchronize(b->stream));
+        if (*herr & kErrStageTimeout) return fail(DTB_ERR_CUDA, "a staged state copy did not complete in time");
         if (where == DTB_HOST) {
             if (sum_out && bs) std::memcpy(sum_out + row0 * ns, p, bs);
             if (mean_out && bs) std::memcpy(mean_out + row0 * ns, p + bs, bs);
