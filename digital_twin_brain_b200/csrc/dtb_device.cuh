@@ -117,7 +117,7 @@ struct DevState {
     const uint16_t* qpos;       // [S] position of every push entry inside its pull row (nullable)
     // ordered push (bit-exact pull order at push cost): pending contributions per neuron
     uint32_t* slot_cnt;         // [N] contributions written since the neuron last consumed them
-    uint4* slots;               // [kSlotCap][N] {pull-row position | kind bit, 0, w.x bits, w.y bits}
+    uint4* slots;               // [N][kSlotCap] {pull-row position | kind bit, 0, w.x bits, w.y bits}
     uint32_t* pmask;            // [N][2][kMaskWords] pull-row positions that fired (excitatory, inhibitory)
     // statistics
     int n_sub;

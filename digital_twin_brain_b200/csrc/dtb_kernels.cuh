@@ -141,8 +141,7 @@ __device__ __forceinline__ float4 slot_pair_sum(uint4 v0, uint4 v1, uint32_t c)
     return make_float4(a0, a1, a2, a3);
 }
 
-// Slots are slot-major: slot k of neuron n at sl[k * N] from sl = slots + n.
-__device__ __forceinline__ float4 slot_sum(const uint4* __restrict__ sl, int64_t N, uint32_t c)
+__device__ __forceinline__ float4 slot_sum(const uint4* __restrict__ sl, uint32_t c)
 {
     float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
     auto add = [&](uint4 v) {
@@ -152,14 +151,14 @@ __device__ __forceinline__ float4 slot_sum(const uint4* __restrict__ sl, int64_t
     };
     if (c <= 2u) {
         add(__ldcs(sl));
-        if (c == 2u) add(__ldcs(sl + N));
+        if (c == 2u) add(__ldcs(sl + 1));
     } else {
         uint32_t last = 0u;
         for (uint32_t r = 0; r < c; ++r) {
             uint4 best = make_uint4(0u, 0u, 0u, 0u);
             uint32_t bp = 0xffffffffu;
             for (uint32_t k = 0; k < c; ++k) {
-                const uint4 v = sl[(int64_t)k * N];
+                const uint4 v = sl[k];
                 const uint32_t p = v.x & kIndexMask;
                 if ((r == 0u || p > last) && p < bp) { bp = p; best = v; }
             }
@@ -573,8 +572,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 sum[j] = make_float4(0.f, 0.f, 0.f, 0.f);
                 s0[j] = s1[j] = make_uint4(0u, 0u, 0u, 0u);
                 if (cnt[j]) s.slot_cnt[n] = 0u;
-                if (cnt[j] >= 1u && cnt[j] <= kSlotCap) s0[j] = __ldcs(s.slots + n);
-                if (cnt[j] == 2u) s1[j] = __ldcs(s.slots + s.N + n);
+                if (cnt[j] >= 1u && cnt[j] <= kSlotCap) s0[j] = __ldcs(s.slots + n * kSlotCap);
+                if (cnt[j] == 2u) s1[j] = __ldcs(s.slots + n * kSlotCap + 1);
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -582,7 +581,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 if (cnt[j] == 0u) continue;
                 if (cnt[j] > kSlotCap) ovf |= 1u << j;
                 else if (cnt[j] <= 2u) sum[j] = slot_pair_sum(s0[j], s1[j], cnt[j]);
-                else sum[j] = slot_sum(s.slots + n, s.N, cnt[j]);
+                else sum[j] = slot_sum(s.slots + n * kSlotCap, cnt[j]);
             }
             // overflowing rows: the warp gathers them whole, in row order
 #pragma unroll
@@ -1031,7 +1030,7 @@ __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, i
 #pragma unroll
                 for (int u = 0; u < kScatterUnroll; ++u)
                     if (k[u] < kSlotCap)
-                        __stcg(s.slots + (int64_t)k[u] * s.N + (int64_t)(c[u] & kIndexMask),
+                        __stcg(s.slots + (int64_t)(c[u] & kIndexMask) * kSlotCap + k[u],
                                make_uint4(ppos[u] | (c[u] & kKindBit), 0u, __float_as_uint(w[u].x),
                                           __float_as_uint(w[u].y)));
             } else {
