@@ -39,9 +39,9 @@ def main(argv=None):
     ap.add_argument("--K", type=int, default=100)
     ap.add_argument("--windows", type=int, default=50)
     ap.add_argument("--steps-per-window", type=int, default=8000)
-    ap.add_argument("--train-windows", type=int, default=18)
+    ap.add_argument("--train-windows", type=int, default=30)
     ap.add_argument("--epochs", type=int, default=60)
-    ap.add_argument("--train-sigma", type=float, default=1.0,
+    ap.add_argument("--train-sigma", type=float, default=2.0,
                     help="random-walk variance of the training ensemble (wider than the DA walk for coverage)")
     ap.add_argument("--threshold", type=float, default=None,
                     help="judge fallback threshold (default: --margin x the held-out judge error of the surrogate)")
