@@ -27,6 +27,7 @@ import torch
 
 from . import synthetic
 from .network import Network
+from .surrogate import with_context
 
 
 def diffusion_enkf(w_hat: torch.Tensor, bold_sigma: float, bold_t: torch.Tensor, solo_rate: float,
@@ -300,7 +301,8 @@ class SurrogateDA:
             r = torch.from_numpy(self.judge.window_rates()).to(self.dev).float()      # [J, R]
             if jh is not None and self.adapt_steps:
                 h = torch.cat([jh[:, :, :1].repeat(1, 1, self.H - jh.shape[2]), jh], 2) if jh.shape[2] < self.H else jh
-                self.sur.adapt(gui, h.reshape(-1, self.H), r.reshape(-1), steps=self.adapt_steps, lr=self.adapt_lr)
+                self.sur.adapt(gui, with_context(h, self.sur.context), r.reshape(-1), steps=self.adapt_steps,
+                               lr=self.adapt_lr)
             jh = r[:, :, None] if jh is None else torch.cat([jh, r[:, :, None]], 2)[:, :, -self.H:]
         if jh.shape[2] < self.H:
             jh = torch.cat([jh[:, :, :1].repeat(1, 1, self.H - jh.shape[2]), jh], 2)
@@ -331,12 +333,12 @@ class SurrogateDA:
         rates_j = torch.from_numpy(self.judge.window_rates()).to(self.dev).float()
         # surrogate forecast of every member's window rate
         gui = hp.reshape(-1, self.n_hp)
-        pred = self.sur.predict(gui, self.hist.reshape(-1, self.H)).reshape(self.M, self.R)
+        pred = self.sur.predict(gui, with_context(self.hist, self.sur.context)).reshape(self.M, self.R)
         # judge score: symmetric relative error of the window rates (floor 1e-5 spikes/step ~ 0.1 Hz)
         err = judge_error(pred[:self.J], rates_j)
         self.errors.append(err)
         if self.adapt_steps:   # the judges' fresh windows refine the surrogate (scored before it learns them)
-            self.sur.adapt(gui[:self.J * self.R], self.hist[:self.J].reshape(-1, self.H), rates_j.reshape(-1),
+            self.sur.adapt(gui[:self.J * self.R], with_context(self.hist[:self.J], self.sur.context), rates_j.reshape(-1),
                            steps=self.adapt_steps, lr=self.adapt_lr)
         sqvf = torch.stack([self.bold.get(k) for k in range(4)], dim=-1).reshape(self.M - self.J, self.R, 4)
         if err > self.threshold:
@@ -400,10 +402,12 @@ class SurrogateDA:
 
 
 def collect_windows(template: synthetic.NetworkSpec, cfg: DAConfig, windows: int, device: int = 0,
-                    history: int = 8):
+                    history: int = 8, context: int | None = None):
     """Training windows for the surrogate: an ensemble with random-walk g_ui factors (the DA
-    forecast without analysis); returns (gui [n,4], hist [n,history], target [n]) over all
-    (member, region, window) with a full history."""
+    forecast without analysis); returns (gui [n,4], hist [n, history + context], target [n])
+    over all (member, region, window) with a full history (see surrogate.with_context)."""
+    from .surrogate import CONTEXT
+    context = CONTEXT if context is None else context
     da = EnsembleDA(template, cfg, device)
     da.hp_random_initialize()
     hps, rates = [], []
@@ -419,7 +423,7 @@ def collect_windows(template: synthetic.NetworkSpec, cfg: DAConfig, windows: int
     g, h, t = [], [], []
     for w in range(history, windows):
         g.append(hp[w].reshape(-1, 4))
-        h.append(rt[w - history:w].permute(1, 2, 0).reshape(-1, history))
+        h.append(with_context(rt[w - history:w].permute(1, 2, 0), context))
         t.append(rt[w].reshape(-1))
     del da
     return torch.cat(g), torch.cat(h), torch.cat(t)

@@ -27,7 +27,7 @@ import torch
 
 from . import synthetic
 from .assimilation import DAConfig, EnsembleDA, SurrogateDA, collect_windows, judge_error, log_torch
-from .surrogate import RateSurrogate
+from .surrogate import HISTORY, RateSurrogate
 
 
 def main(argv=None):
@@ -130,7 +130,7 @@ def main(argv=None):
     pred = sur.predict(g[te], h[te]).cpu()
     eps = 1e-6
     lerr_net = float(torch.sqrt(torch.mean((torch.log(pred + eps) - torch.log(tgt[te] + eps)) ** 2)))
-    lerr_persist = float(torch.sqrt(torch.mean((torch.log(h[te][:, -1] + eps) - torch.log(tgt[te] + eps)) ** 2)))
+    lerr_persist = float(torch.sqrt(torch.mean((torch.log(h[te][:, HISTORY - 1] + eps) - torch.log(tgt[te] + eps)) ** 2)))
     val_err = judge_error(pred, tgt[te])
     threshold = a.threshold if a.threshold is not None else a.margin * val_err
     out.update(heldout_judge_err=val_err, threshold=threshold)

@@ -104,21 +104,37 @@ class MLP:
 
 HISTORY = 8
 N_GUI = 4
+CONTEXT = 2     # the member's mean rate over all its regions in the last CONTEXT windows
+
+
+def with_context(hist: torch.Tensor, context: int = CONTEXT) -> torch.Tensor:
+    """[M, R, HISTORY] rate histories -> [M * R, HISTORY + context]: every region's own history
+    and its member's mean over regions of the last `context` windows (the input the other
+    regions send it)."""
+    M, R, H = hist.shape
+    if context == 0:
+        return hist.reshape(-1, H)
+    ctx = hist[:, :, H - context:].mean(dim=1, keepdim=True).expand(M, R, context)
+    return torch.cat([hist, ctx], dim=2).reshape(-1, H + context)
 
 
 class RateSurrogate:
-    """Next-window firing rate of a region from its g_ui factors and the rates of the
-    previous HISTORY windows (input 4 + 8 = 12, hidden 2 x 256 GELU, one output)."""
+    """Next-window firing rate of a region from its g_ui factors, the rates of the previous
+    HISTORY windows and its member's mean rate over the last CONTEXT windows (input
+    4 + 8 + 2 = 14, hidden 2 x 256 GELU, one output)."""
 
-    def __init__(self, hidden: int = 256, seed: int = 0, device: int = 0, eps: float = 1e-6):
-        self.mlp = MLP(N_GUI + HISTORY, hidden, seed, device)
+    def __init__(self, hidden: int = 256, seed: int = 0, device: int = 0, eps: float = 1e-6,
+                 context: int = CONTEXT):
+        self.context = context
+        self.mlp = MLP(N_GUI + HISTORY + context, hidden, seed, device)
         self.dev = self.mlp.dev
         self.eps = eps
         self.mu_x = self.sd_x = None
         self.mu_y = self.sd_y = None
 
     def features(self, gui: torch.Tensor, hist: torch.Tensor) -> torch.Tensor:
-        """gui [n,4] factors, hist [n,8] rates (oldest first) -> [n,12] standardised log features."""
+        """gui [n,4] factors, hist [n, HISTORY + context] rates (own history oldest first, then the
+        member means) -> standardised log features."""
         x = torch.cat([torch.log(gui.to(self.dev).float()), torch.log(hist.to(self.dev).float() + self.eps)], dim=1)
         if self.mu_x is not None:
             x = (x - self.mu_x) / self.sd_x

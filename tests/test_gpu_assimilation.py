@@ -5,7 +5,7 @@ import torch
 
 from digital_twin_brain_b200 import synthetic
 from digital_twin_brain_b200.assimilation import DAConfig, EnsembleDA, SurrogateDA, collect_windows, log_torch
-from digital_twin_brain_b200.surrogate import RateSurrogate
+from digital_twin_brain_b200.surrogate import HISTORY, RateSurrogate
 
 pytestmark = pytest.mark.gpu
 
@@ -44,7 +44,7 @@ def test_member_hp_changes_its_own_rate():
 def test_surrogate_da_runs_with_judges_and_fallback():
     cfg = DAConfig(n_members=12, steps_per_window=300, seed=3)
     g, h, t = collect_windows(TEMPLATE, cfg, windows=10)
-    assert g.shape[0] == h.shape[0] == t.shape[0] == 2 * 12 * TEMPLATE.R and h.shape[1] == 8
+    assert g.shape[0] == h.shape[0] == t.shape[0] == 2 * 12 * TEMPLATE.R and h.shape[1] == 8 + 2
     sur = RateSurrogate(seed=0)
     sur.fit(g, h, t, epochs=5)
     sda = SurrogateDA(TEMPLATE, cfg, sur, n_judge=4, threshold=0.0)     # always falls back
@@ -65,7 +65,7 @@ def test_surrogate_da_runs_with_judges_and_fallback():
 def test_surrogate_adapt_lowers_loss_on_new_windows():
     torch.manual_seed(0)
     g = torch.rand(2000, 4) + 0.5
-    h = torch.rand(2000, 8) * 0.01 + 1e-3
+    h = torch.rand(2000, 10) * 0.01 + 1e-3
     t = h.mean(1) * g[:, 0]
     sur = RateSurrogate(seed=1)
     sur.fit(g[:1000], h[:1000], t[:1000] * 0.5, epochs=5)     # trained on a shifted relation
@@ -89,5 +89,5 @@ def test_surrogate_beats_persistence_on_simulated_windows():
     eps = 1e-6
     pred = sur.predict(g[te], h[te]).cpu()
     err_net = float(torch.sqrt(torch.mean((torch.log(pred + eps) - torch.log(t[te] + eps)) ** 2)))
-    err_persist = float(torch.sqrt(torch.mean((torch.log(h[te][:, -1] + eps) - torch.log(t[te] + eps)) ** 2)))
+    err_persist = float(torch.sqrt(torch.mean((torch.log(h[te][:, HISTORY - 1] + eps) - torch.log(t[te] + eps)) ** 2)))
     assert err_net < 0.9 * err_persist, (err_net, err_persist)

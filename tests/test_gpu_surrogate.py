@@ -44,7 +44,7 @@ def test_rate_surrogate_learns_rate_map():
     gui = rng.uniform(0.5, 1.5, (n, 4)).astype(np.float32)
     hist = rng.uniform(0.0005, 0.01, (n, 8)).astype(np.float32)
     target = (0.6 * hist[:, -1] * gui[:, 0] / gui[:, 2] + 0.002 * gui[:, 1]).astype(np.float32)
-    s = RateSurrogate(seed=2)
+    s = RateSurrogate(seed=2, context=0)
     s.fit(torch.from_numpy(gui), torch.from_numpy(hist), torch.from_numpy(target), epochs=40, lr=2e-3)
     pred = s.predict(torch.from_numpy(gui), torch.from_numpy(hist)).cpu().numpy()
     err_net = np.sqrt(np.mean((pred - target) ** 2))
