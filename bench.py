@@ -39,9 +39,9 @@ METRIC = "synaptic events/s & sim-s/wall-s at 2B syn; DA window time surrogate v
 UNIT = "events/s"
 # ncu DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, one pass each) of the whole-brain
 # workload itself (profiles/whole_brain_dram_traffic.md): k_scatter<0> 1.303 GB per launch for
-# 2.346e7 events, staged update 1.108 GB per launch for 2.345e7 neurons
+# 2.346e7 events, staged update 1.014 GB per launch for 2.345e7 neurons
 SCATTER_DRAM_BYTES_PER_EVENT = (943.26e6 + 360.44e6) / 23462598
-UPDATE_DRAM_BYTES_PER_NEURON = (688.37e6 + 419.80e6) / 23448955
+UPDATE_DRAM_BYTES_PER_NEURON = (595.12e6 + 418.77e6) / 23448955
 
 
 def parse():

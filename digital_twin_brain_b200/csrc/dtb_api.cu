@@ -371,6 +371,30 @@ static int upload_class_tables(dtb_block* b)
     return DTB_OK;
 }
 
+// Per-tile class ids: the class of a 128-neuron tile whose neurons all share one (the
+// update then reads no per-neuron class id for it), else kMixedTile.
+static int upload_tile_classes(dtb_block* b, const std::vector<uint32_t>& cls)
+{
+    DevState& s = b->ds;
+    const int64_t nt = (b->N + kWarpNeurons - 1) / kWarpNeurons;
+    if (nt <= 0) return DTB_OK;
+    std::vector<uint32_t> tc((size_t)nt);
+    for (int64_t t = 0; t < nt; ++t) {
+        const int64_t n0 = t * kWarpNeurons, n1 = std::min<int64_t>(b->N, n0 + kWarpNeurons);
+        uint32_t c = cls[(size_t)n0];
+        for (int64_t n = n0 + 1; n < n1; ++n)
+            if (cls[(size_t)n] != c) { c = kMixedTile; break; }
+        tc[(size_t)t] = c;
+    }
+    if (!s.tile_cls) {
+        uint32_t* d = nullptr;
+        RET(dalloc(b, &d, (size_t)nt));
+        s.tile_cls = d;
+    }
+    CK(cudaMemcpy(const_cast<uint32_t*>(s.tile_cls), tc.data(), sizeof(uint32_t) * (size_t)nt, cudaMemcpyHostToDevice));
+    return DTB_OK;
+}
+
 // Class table, per-neuron class ids, subblock tables and initial V.
 static int upload_classes(dtb_block* b, const std::vector<uint32_t>& cls, bool init_v)
 {
@@ -380,6 +404,7 @@ static int upload_classes(dtb_block* b, const std::vector<uint32_t>& cls, bool i
     RET(dalloc(b, &dcls, (size_t)b->N));
     CK(cudaMemcpy(dcls, cls.data(), sizeof(uint32_t) * (size_t)b->N, cudaMemcpyHostToDevice));
     s.cls = dcls;
+    RET(upload_tile_classes(b, cls));
     if (init_v) {
         // models/block.py:56: V = ones * (V_th + V_reset) / 2
         std::vector<float> v0((size_t)b->N);
@@ -1778,6 +1803,7 @@ int dtb_block_update_property(dtb_block* b, const float* property, const float* 
     RET(build_classes(b, b->N, property, decay, cls));
     RET(upload_class_tables(b));
     CK(cudaMemcpy(const_cast<uint32_t*>(s.cls), cls.data(), sizeof(uint32_t) * (size_t)b->N, cudaMemcpyHostToDevice));
+    RET(upload_tile_classes(b, cls));
     if (!s.st_spk) RET(ensure_stats(b, 256));
     if (b->bold_R == 0) RET(rebuild_groups(b, nullptr));
     b->class_prop_base.clear();

@@ -27,6 +27,7 @@ constexpr int kGatherStream = 4;       // k_step streams its tile's pull entries
 constexpr int kStreamWarpBytes = 129 * 8 + 8 + 128 * 16;   // row pointers (+pad) and row sums per warp
 constexpr int kMaskWords = 4;          // position-mask words per kind: in-degree up to 128
 constexpr int kMaskList = 256;         // marked entries a warp gathers together per tile
+constexpr uint32_t kMixedTile = 0xffffffffu;   // tile_cls of a tile whose neurons have different classes
 constexpr int kStepThreads = 256;      // 8 warps, 1024 neurons per CTA
 
 // One deduplicated row of the 22-column property matrix
@@ -94,6 +95,8 @@ struct DevState {
     float* tlast;
     float* isyn_override;       // [N] used once after update_property
     const uint32_t* cls;
+    const uint32_t* tile_cls;   // [ceil(N/128)] the class every neuron of a 128-neuron tile shares, else
+                                // kMixedTile (nullable: every tile then reads its per-neuron ids)
     const ParamClass* pc;
     const float4* gnrn;         // [N] per-neuron factors of g_ui (gamma-distributed properties; nullable)
     const int64_t* member_start;  // [M] first neuron of every ensemble member (nullable)

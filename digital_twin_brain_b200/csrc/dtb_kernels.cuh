@@ -362,16 +362,18 @@ __device__ __forceinline__ void stage_issue(uint32_t dst, const void* src, uint3
                  :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
-// Lane 0: the five copies of tile `base` into buffer `buf` (16-byte aligned, whole tile).
+// Lane 0: the copies of tile `base` into buffer `buf` (16-byte aligned, whole tile); the
+// class ids only for a tile whose neurons have different classes.
 __device__ __forceinline__ void stage_tile(const DevState& s, int64_t base, unsigned char* buf, uint32_t mbar)
 {
+    const bool mixed = !s.tile_cls || __ldg(s.tile_cls + base / kWarpNeurons) == kMixedTile;
+    const uint32_t bytes = (uint32_t)kStageBytes - (mixed ? 0u : (uint32_t)kWarpNeurons * 4u);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier generic reads of buf first
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"((uint32_t)kStageBytes)
-                 : "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(bytes) : "memory");
     const uint32_t d = smem_u32(buf);
     stage_issue(d, s.V + base, kWarpNeurons * 4, mbar);
     stage_issue(d + kWarpNeurons * 4, s.tlast + base, kWarpNeurons * 4, mbar);
-    stage_issue(d + kWarpNeurons * 8, s.cls + base, kWarpNeurons * 4, mbar);
+    if (mixed) stage_issue(d + kWarpNeurons * 8, s.cls + base, kWarpNeurons * 4, mbar);
     stage_issue(d + kWarpNeurons * 12, s.J2 + base, kWarpNeurons * 8, mbar);
     stage_issue(d + kWarpNeurons * 20, s.J2 + s.j_ps + base, kWarpNeurons * 8, mbar);
 }
@@ -721,6 +723,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         float v_in[4], tl_in[4];
         float4 J_in[4];
         uint32_t c_in[4];
+        const uint32_t tcls = s.tile_cls ? __ldg(s.tile_cls + tile) : kMixedTile;   // the tile's class, or kMixedTile
+        const bool mixed = tcls == kMixedTile;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int64_t n = base + j * 32 + lane;
@@ -734,14 +738,14 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                         const int k = j * 32 + lane;
                         reinterpret_cast<float*>(stage_buf)[k] = __ldcs(s.V + n);
                         reinterpret_cast<float*>(stage_buf + kWarpNeurons * 4)[k] = __ldcs(s.tlast + n);
-                        reinterpret_cast<uint32_t*>(stage_buf + kWarpNeurons * 8)[k] = __ldcs(s.cls + n);
+                        if (mixed) reinterpret_cast<uint32_t*>(stage_buf + kWarpNeurons * 8)[k] = __ldcs(s.cls + n);
                         reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 12)[k] = __ldcs(s.J2 + n);
                         reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 20)[k] = __ldcs(s.J2 + s.j_ps + n);
                     }
                 } else {
                     v_in[j] = __ldcs(s.V + n);
                     tl_in[j] = __ldcs(s.tlast + n);
-                    c_in[j] = __ldcs(s.cls + n);
+                    c_in[j] = mixed ? __ldcs(s.cls + n) : tcls;
                     if (!GATHER) J_in[j] = load_J(s, n);
                 }
             }
@@ -749,7 +753,9 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         if (STAGED) {
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                c_in[j] = valid[j] ? reinterpret_cast<const uint32_t*>(stage_buf + kWarpNeurons * 8)[j * 32 + lane] : 0u;
+                c_in[j] = !valid[j] ? 0u
+                          : mixed   ? reinterpret_cast<const uint32_t*>(stage_buf + kWarpNeurons * 8)[j * 32 + lane]
+                                    : tcls;
         }
         // Noise words: counter {tile*32 + lane, stream, step}; inside an ensemble the
         // tile and stream are the member's own (members start on 128-neuron tiles),
