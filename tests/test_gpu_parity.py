@@ -261,6 +261,28 @@ def test_scale_property_by_subblock_matches_oracle():
     assert np.array_equal(net.get(FIELD_V), ob.V)
 
 
+def test_update_property_across_tile_classes_matches_oracle():
+    """Property updates that change which 128-neuron tiles share one parameter class (two
+    classes -> per-neuron g_ui, every tile mixed -> two classes again): the update follows
+    the new classes, spikes and V bit-identical to the oracle."""
+    spec = synthetic.single_block(3000, 60, name="n3k_tiles")
+    net = Network.from_spec(spec, device=0, class_decay=class_decay_like_reference(spec))
+    ob = _oracle_for(spec)
+    base = spec.property()
+    mixed = base.copy()
+    mixed[:, 10:14] *= np.random.default_rng(5).uniform(0.8, 1.25, (spec.N, 4)).astype(np.float32)
+    for prop in (None, mixed, base):
+        if prop is not None:
+            dec = decay_like_reference(prop, spec.dt)
+            net.update_property(prop, np.ascontiguousarray(dec.T))
+            ob.update_property(prop, dec)
+        for _ in range(80):
+            s, _, _ = net.run(1, mode="pull")
+            so, _ = ob.run(0.01)
+            assert np.array_equal(s[0], so)
+        assert np.array_equal(net.get(FIELD_V), ob.V)
+
+
 def test_update_conn_weight_matches_oracle():
     spec = synthetic.single_block(2000, 40, name="n2k_w")
     net = Network.from_spec(spec, device=0, class_decay=class_decay_like_reference(spec))
