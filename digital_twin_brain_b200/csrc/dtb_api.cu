@@ -163,7 +163,7 @@ struct dtb_block {
     int chunk = 32;
     int scatter_wpw = 32;         // bitmask words per warp in the push scatter
     int scatter_variant = 0;      // 0: registers unbounded, 1: budgeted for 6 resident CTAs per SM
-    int step_variant = 0;         // 0: 2 resident CTAs/SM register budget, 1: 3
+    int step_variant = 0;         // 0: 2 resident CTAs/SM register budget, 1: 3; 2..4: staged, 2..4 CTAs/SM
     // ordered push (bit-exact pull through per-neuron slots)
     bool has_qpos = false;
     int pull_method = 0;          // 0: auto, 1: row gather, 2: ordered push (slots), 3: (masks), 4: streamed gather
@@ -628,6 +628,7 @@ static void launch_step(dtb_block* b, const DevState& s)
     if constexpr (G == 0) {
         if (b->step_variant == 2 && staged_layout(s)) { launch_step_staged<U, F, 2>(b, s); return; }
         if (b->step_variant == 3 && staged_layout(s)) { launch_step_staged<U, F, 3>(b, s); return; }
+        if (b->step_variant == 4 && staged_layout(s)) { launch_step_staged<U, F, 4>(b, s); return; }
     }
     if (b->step_variant == 1) launch_step_m<G, U, F, 3>(b, s);
     else launch_step_m<G, U, F, 2>(b, s);
@@ -1545,7 +1546,7 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         break;
     case DTB_TUNE_USE_GRAPHS: b->use_graphs = value != 0; break;
     case DTB_TUNE_STEP_VARIANT:
-        if (value < 0 || value > 3) return fail(DTB_ERR_ARG, "step variant must be 0..3");
+        if (value < 0 || value > 4) return fail(DTB_ERR_ARG, "step variant must be 0..4");
         b->step_variant = (int)value;
         break;
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
@@ -1580,7 +1581,7 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
         const int mode = b->has_push ? DTB_MODE_PUSH : DTB_MODE_PULL;
         float best_u = 1e30f;
         int best_v = 0;
-        for (int v = 0; v < 4; ++v) {
+        for (int v = 0; v < 5; ++v) {
             if (v >= 2 && !staged_layout(b->ds)) continue;
             b->step_variant = v;
             float o[4];

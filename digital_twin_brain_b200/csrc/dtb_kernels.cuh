@@ -344,10 +344,12 @@ __global__ void k_samples(DevState s)
 
 // ------------------------------------------------------------ staged state loads
 // Bulk asynchronous copies (cp.async.bulk, the TMA engine; no multicast) of a
-// tile's V, t_last, class ids and both J planes into shared memory, issued by
-// lane 0 one tile ahead, so that the loads of tile k+1 are in flight while tile
-// k computes.  Completion is counted on a per-warp, per-buffer mbarrier.
-constexpr int kStageBytes = kWarpNeurons * (4 + 4 + 4 + 8 + 8);   // 3584 per tile buffer
+// tile's V, t_last and both J planes into shared memory, issued by lane 0 one
+// tile ahead, so that the loads of tile k+1 are in flight while tile k computes
+// (class ids come from the per-tile table, or, for a tile of mixed classes, from
+// global memory).  Completion is counted on a per-warp, per-buffer mbarrier.
+// 3 KB per buffer: eight warps' double buffers (48 KB) fit four CTAs per SM.
+constexpr int kStageBytes = kWarpNeurons * (4 + 4 + 8 + 8);       // 3072 per tile buffer
 constexpr int kStagedSmem = (kStepThreads / 32) * 2 * kStageBytes;
 constexpr uint32_t kErrStageTimeout = 1u;                        // Ctl::err bit
 
@@ -362,20 +364,18 @@ __device__ __forceinline__ void stage_issue(uint32_t dst, const void* src, uint3
                  :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
-// Lane 0: the copies of tile `base` into buffer `buf` (16-byte aligned, whole tile); the
-// class ids only for a tile whose neurons have different classes.
+// Lane 0: the four copies of tile `base` into buffer `buf` (16-byte aligned, whole tile):
+// V at 0, t_last at 512, J plane 0 at 1024, J plane 1 at 2048.
 __device__ __forceinline__ void stage_tile(const DevState& s, int64_t base, unsigned char* buf, uint32_t mbar)
 {
-    const bool mixed = !s.tile_cls || __ldg(s.tile_cls + base / kWarpNeurons) == kMixedTile;
-    const uint32_t bytes = (uint32_t)kStageBytes - (mixed ? 0u : (uint32_t)kWarpNeurons * 4u);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier generic reads of buf first
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(bytes) : "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"((uint32_t)kStageBytes)
+                 : "memory");
     const uint32_t d = smem_u32(buf);
     stage_issue(d, s.V + base, kWarpNeurons * 4, mbar);
     stage_issue(d + kWarpNeurons * 4, s.tlast + base, kWarpNeurons * 4, mbar);
-    if (mixed) stage_issue(d + kWarpNeurons * 8, s.cls + base, kWarpNeurons * 4, mbar);
-    stage_issue(d + kWarpNeurons * 12, s.J2 + base, kWarpNeurons * 8, mbar);
-    stage_issue(d + kWarpNeurons * 20, s.J2 + s.j_ps + base, kWarpNeurons * 8, mbar);
+    stage_issue(d + kWarpNeurons * 8, s.J2 + base, kWarpNeurons * 8, mbar);
+    stage_issue(d + kWarpNeurons * 16, s.J2 + s.j_ps + base, kWarpNeurons * 8, mbar);
 }
 
 // Bounded wait for a buffer's copies; false after the limit (the caller then loads from global).
@@ -738,9 +738,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                         const int k = j * 32 + lane;
                         reinterpret_cast<float*>(stage_buf)[k] = __ldcs(s.V + n);
                         reinterpret_cast<float*>(stage_buf + kWarpNeurons * 4)[k] = __ldcs(s.tlast + n);
-                        if (mixed) reinterpret_cast<uint32_t*>(stage_buf + kWarpNeurons * 8)[k] = __ldcs(s.cls + n);
-                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 12)[k] = __ldcs(s.J2 + n);
-                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 20)[k] = __ldcs(s.J2 + s.j_ps + n);
+                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 8)[k] = __ldcs(s.J2 + n);
+                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 16)[k] = __ldcs(s.J2 + s.j_ps + n);
                     }
                 } else {
                     v_in[j] = __ldcs(s.V + n);
@@ -754,7 +753,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 c_in[j] = !valid[j] ? 0u
-                          : mixed   ? reinterpret_cast<const uint32_t*>(stage_buf + kWarpNeurons * 8)[j * 32 + lane]
+                          : mixed   ? __ldcs(s.cls + base + j * 32 + lane)
                                     : tcls;
         }
         // Noise words: counter {tile*32 + lane, stream, step}; inside an ensemble the
@@ -792,8 +791,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 const int k = j * 32 + lane;
                 v = reinterpret_cast<const float*>(stage_buf)[k];
                 tl = reinterpret_cast<const float*>(stage_buf + kWarpNeurons * 4)[k];
-                const float2 a = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 12)[k];
-                const float2 b2 = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 20)[k];
+                const float2 a = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 8)[k];
+                const float2 b2 = reinterpret_cast<const float2*>(stage_buf + kWarpNeurons * 16)[k];
                 J = make_float4(a.x, a.y, b2.x, b2.y);
             } else {
                 v = v_in[j];

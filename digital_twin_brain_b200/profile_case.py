@@ -26,7 +26,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=80)
     ap.add_argument("--mode", default="push", choices=["push", "pull"])
     ap.add_argument("--scatter-words", type=int, default=0)
-    ap.add_argument("--step-variant", type=int, default=0, help="0/1: register budgets, 2/3: staged state loads")
+    ap.add_argument("--step-variant", type=int, default=0, help="0/1: register budgets, 2/3/4: staged state loads (2, 3, 4 CTAs per SM)")
     ap.add_argument("--j-cache", type=int, default=0, help="1: the update's J stores keep their L2 lines")
     a = ap.parse_args()
     spec = synthetic.whole_brain(K=a.K, scale=a.scale, name="profile_case")

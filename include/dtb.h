@@ -214,10 +214,10 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          DTB_MODE_AUTO pulls instead of pushing
  * DTB_TUNE_USE_GRAPHS      capture chunks in CUDA graphs (0/1)
  * DTB_TUNE_STEP_VARIANT    update kernel: 0 = registers for two resident
- *                          CTAs per SM (no spills), 1 = three, 2 and 3 =
- *                          two and three with the state of the next tile
- *                          bulk-copied to shared memory while the current one
- *                          computes
+ *                          CTAs per SM (no spills), 1 = three, 2, 3 and 4 =
+ *                          two, three and four with the state of the next
+ *                          tile bulk-copied to shared memory while the
+ *                          current one computes
  * DTB_TUNE_PULL_METHOD     how DTB_MODE_PULL propagates (bit-identical every
  *                          way): 1 = every postsynaptic row gathers its firing
  *                          inputs; 2 = ordered push: firing rows scatter into

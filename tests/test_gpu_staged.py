@@ -11,7 +11,7 @@ from digital_twin_brain_b200._lib import (FIELD_ACTIVE, FIELD_I_SYN, FIELD_J, FI
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("variant", [2, 3])
+@pytest.mark.parametrize("variant", [2, 3, 4])
 @pytest.mark.parametrize("N", [3002, 3001, 128 * 40], ids=["partial_tile", "odd_n", "whole_tiles"])
 def test_staged_update_equals_plain(N, variant):
     spec = synthetic.single_block(N, 60, name=f"staged_{N}")
