@@ -75,3 +75,26 @@ def test_synthetic_specs():
     s2 = synthetic.config_whole_brain()
     assert s2.R == 90 and 1.5e7 < s2.N < 3e7 and abs(s2.S - 100 * s2.N) == 0
     assert np.allclose(s2.cum[:, -1], 1.0) and (np.diff(s2.cum, axis=1) >= 0).all()
+
+
+def declared_constants():
+    """Every `DTB_NAME = value` enumerator of include/dtb.h."""
+    src = open(os.path.join(ROOT, "include", "dtb.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return {k: int(v) for k, v in re.findall(r"\b(DTB_[A-Z0-9_]+)\s*=\s*(\d+)", src)}
+
+
+def test_python_binding_constants_match_the_header():
+    c = declared_constants()
+    assert c["DTB_HOST"] == _lib.DTB_HOST and c["DTB_DEVICE"] == _lib.DTB_DEVICE
+    for mode in ("AUTO", "PUSH", "PULL"):
+        assert c[f"DTB_MODE_{mode}"] == getattr(_lib, f"MODE_{mode}")
+    fields = {k[len("DTB_FIELD_"):]: v for k, v in c.items() if k.startswith("DTB_FIELD_")}
+    tunes = {k[len("DTB_TUNE_"):]: v for k, v in c.items() if k.startswith("DTB_TUNE_")}
+    assert fields and tunes
+    for name, value in fields.items():
+        assert getattr(_lib, f"FIELD_{name}") == value, name
+    for name, value in tunes.items():
+        assert getattr(_lib, f"TUNE_{name}") == value, name
+    errors = {v for k, v in c.items() if k.startswith("DTB_ERR_")} | {c["DTB_OK"]}
+    assert errors == set(_lib.STATUS)
