@@ -261,7 +261,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     N, S = spec.N, spec.S
     evs = kt["events_per_step"]
     nact = evs / spec.K
-    upd_bytes = N * (4 + 16 + 4 + 4) + N * (4 + 16) + 2 * N / 8          # V,J,t_last,class r; V,J w; 2 bitmasks
+    # V, J, t_last read, one class id per 128-neuron tile; V, J written; two bitmasks
+    upd_bytes = N * (4 + 16 + 4 + 4 / 128) + N * (4 + 16) + 2 * N / 8
     prop_bytes = N / 8 + 16 * nact + 12 * evs                              # bitmask, row pointers, (post, w) of rows
     ordered = mode == "pull" and net.get_tuning(TUNE_PULL_METHOD) != 1 and kt["propagate_ms"] > 0 and \
         nact / N <= 0.1
