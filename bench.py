@@ -70,14 +70,30 @@ class ClockSampler:
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
+        self.gpu = self.smi_id(gpu_index)
         self.proc = None
         self.lines = []
+
+    @staticmethod
+    def smi_id(dev: int) -> str:
+        """nvidia-smi's name for CUDA device `dev`: its UUID when nvidia-smi answers to it (CUDA's
+        device order need not be nvidia-smi's index order), else the index."""
+        try:
+            import torch
+            u = str(torch.cuda.get_device_properties(dev).uuid)
+            u = u if u.startswith("GPU-") else "GPU-" + u
+            r = subprocess.run(["nvidia-smi", "--query-gpu=uuid", "--format=csv,noheader", "-i", u],
+                               capture_output=True, text=True, timeout=20)
+            if r.returncode == 0 and r.stdout.strip().lower() == u.lower():
+                return u
+        except Exception:
+            pass
+        return str(dev)
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                          "-i", self.gpu, "-lms", "200"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -253,6 +269,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         net.run(1, noise_rate=args.noise, mode=mode, out="host")
     t_e2e = time.perf_counter() - t0
     ev_e2e = net.get(10) - ev_a
+    # whole job at N replicas: the events of all ranks over the slowest rank's time
+    e2e_ms, ev_e2e = combine_over_ranks(1000.0 * t_e2e, float(ev_e2e), world, f"cuda:{dev}")
+    t_e2e = e2e_ms / 1000.0
     e2e_value = ev_e2e / t_e2e
     h2d = 16                                  # run parameters (base step, noise rate, isolated)
     d2h = 2 * 4 * net.n_sub + 4               # spike sums + mean V per subblock + propagated count
