@@ -168,9 +168,17 @@ struct dtb_block {
     bool has_qpos = false;
     int pull_method = 0;          // 0: auto, 1: row gather, 2: ordered push (slots), 3: (masks), 4: streamed gather
     double slot_threshold = 0.1;
-    // graphs: one chunk graph per propagation method (push, pull rows, pull slots)
-    cudaGraphExec_t graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    int graph_len[6] = {0, 0, 0, 0, 0, 0};
+    // binned push (DTB_TUNE_PUSH_METHOD)
+    int push_method = 1;          // 0: binned when its bins fit, 1: float2 atomics into J, 2: binned
+    int bin_shift_req = 0;        // 0: chosen from N
+    int bin_cap_per_neuron = 8;   // bin entries per neuron of a bin
+    int bin_words = 64;           // bitmask words per scatter round
+    int bin_scatter_per_sm = 0;   // resident scatter CTAs per SM (from the occupancy calculator)
+    bool bins_pending = false;    // the bins hold events not yet folded into J
+    bool bins_failed = false;     // the bins could not be allocated (auto pushes with atomics)
+    // graphs: one chunk graph per propagation method (push, pull rows, pull slots, ..., binned push)
+    cudaGraphExec_t graph[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    int graph_len[7] = {0, 0, 0, 0, 0, 0, 0};
     bool use_graphs = true;
     // attached BOLD
     int bold_R = 0;
@@ -622,9 +630,36 @@ static void launch_step_staged(dtb_block* b, const DevState& s)
 
 static bool staged_layout(const DevState& s) { return s.j_es == 1 && s.j_ps >= s.N && (s.j_ps % 2) == 0; }
 
+// Update that first folds the binned push events of its chunks (one chunk = one bin of
+// 2^bin_shift neurons, its sums in 16 << bin_shift bytes of shared memory): each CTA
+// takes an equal run of chunks.
+template <bool U, bool F, int M>
+static void launch_step_bins(dtb_block* b, const DevState& s)
+{
+    static int per_sm[kBinMaxShift + 1] = {0};
+    const int B = s.bin_shift;
+    const size_t smem = (size_t)16 << B;
+    if (!per_sm[B]) {
+        cudaFuncSetAttribute(k_step<kGatherBins, U, F, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             16 << kBinMaxShift);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[B], k_step<kGatherBins, U, F, M>, kStepThreads, smem);
+        if (per_sm[B] < 1) per_sm[B] = 1;
+    }
+    const int64_t nchunks = (b->N + ((int64_t)1 << B) - 1) >> B;
+    const int64_t maxb = (int64_t)std::max(1, b->n_sm) * per_sm[B];
+    const int64_t cpc = std::max<int64_t>(1, (nchunks + maxb - 1) / maxb);
+    const unsigned grid = (unsigned)std::max<int64_t>(1, (nchunks + cpc - 1) / cpc);
+    k_step<kGatherBins, U, F, M><<<grid, kStepThreads, smem, b->stream>>>(s, (int)cpc);
+}
+
 template <int G, bool U, bool F>
 static void launch_step(dtb_block* b, const DevState& s)
 {
+    if constexpr (G == kGatherBins) {
+        if (b->step_variant == 1 || b->step_variant >= 3) launch_step_bins<U, F, 3>(b, s);
+        else launch_step_bins<U, F, 2>(b, s);
+        return;
+    }
     if constexpr (G == 0) {
         if (b->step_variant == 2 && staged_layout(s)) { launch_step_staged<U, F, 2>(b, s); return; }
         if (b->step_variant == 3 && staged_layout(s)) { launch_step_staged<U, F, 3>(b, s); return; }
@@ -664,13 +699,15 @@ static int launch_update(dtb_block* b, const DevState& s, int gather, bool force
         forced = true;
     }
     if (forced) {
-        if (gather == kGatherRows) launch_step<kGatherRows, true, true>(b, s);
+        if (gather == kGatherBins) launch_step<kGatherBins, true, true>(b, s);
+        else if (gather == kGatherRows) launch_step<kGatherRows, true, true>(b, s);
         else if (gather == kGatherSlots) launch_step<kGatherSlots, true, true>(b, s);
         else if (gather == kGatherMasks) launch_step<kGatherMasks, true, true>(b, s);
         else if (gather == kGatherStream) launch_step<kGatherStream, true, true>(b, s);
         else launch_step<0, true, true>(b, s);
     } else {
-        if (gather == kGatherRows) launch_step<kGatherRows, true, false>(b, s);
+        if (gather == kGatherBins) launch_step<kGatherBins, true, false>(b, s);
+        else if (gather == kGatherRows) launch_step<kGatherRows, true, false>(b, s);
         else if (gather == kGatherSlots) launch_step<kGatherSlots, true, false>(b, s);
         else if (gather == kGatherMasks) launch_step<kGatherMasks, true, false>(b, s);
         else if (gather == kGatherStream) launch_step<kGatherStream, true, false>(b, s);
@@ -716,11 +753,130 @@ static void drop_graphs(dtb_block* b)
     for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
 }
 
+// ------------------------------------------------------------ binned push
+// Bin geometry: 2^B neurons per bin (the update's chunk), B >= 10 (one tile per warp of
+// the update CTA), at least 11 from 8M neurons, raised until the scatter's shared
+// counter table leaves room for two scatter CTAs per SM (n_bins <= 20000), at most
+// kBinMaxShift (the update's 16 << B bytes of sums).
+static int bin_shift_for(const dtb_block* b)
+{
+    if (b->bin_shift_req) return b->bin_shift_req;
+    int B = b->N >= (int64_t)8 << 20 ? 11 : kBinMinShift;
+    while (B < kBinMaxShift && ((b->N + ((int64_t)1 << B) - 1) >> B) > 20000) ++B;
+    return B;
+}
+
+// Bitmask words per scatter round: the round's synapses must stay below 2^31.
+static int bin_words_for(const dtb_block* b)
+{
+    const int64_t lim = ((int64_t)1 << 31) - 1;
+    int w = b->bin_words;
+    while (w > 1 && (int64_t)w * 32 * std::max<int64_t>(1, b->max_out) > lim) w >>= 1;
+    return w;
+}
+
+static bool bins_possible(const dtb_block* b)
+{
+    if (!b->has_push || b->N <= 0) return false;
+    const int B = bin_shift_for(b);
+    if (B > kBinMaxShift || ((b->N + ((int64_t)1 << B) - 1) >> B) > kBinMaxBins) return false;
+    return (int64_t)32 * std::max<int64_t>(1, b->max_out) < ((int64_t)1 << 31);
+}
+
+static void free_bins(dtb_block* b)
+{
+    DevState& s = b->ds;
+    dfree(b, s.bin_idx);
+    dfree(b, s.bin_w);
+    dfree(b, s.bin_cnt);
+    s.n_bins = 0;
+    s.bin_cap = 0;
+    b->bins_pending = false;
+}
+
+static int ensure_bins(dtb_block* b)
+{
+    DevState& s = b->ds;
+    if (s.bin_cnt) return DTB_OK;
+    if (!bins_possible(b)) return fail(DTB_ERR_STATE, "binned push not possible for this network");
+    const int B = bin_shift_for(b);
+    const int64_t n_bins = (b->N + ((int64_t)1 << B) - 1) >> B;
+    int64_t cap = (int64_t)b->bin_cap_per_neuron << B;
+    cap = std::min<int64_t>(cap, (int64_t)0xffffffffLL / n_bins);
+    const size_t entries = (size_t)n_bins * (size_t)cap;
+    uint16_t* bi = nullptr; float2* bw = nullptr; uint32_t* bc = nullptr;
+    int rc = dalloc(b, &bi, entries);
+    if (rc == DTB_OK) rc = dalloc(b, &bw, entries);
+    if (rc == DTB_OK) rc = dalloc(b, &bc, (size_t)n_bins);
+    if (rc != DTB_OK) {
+        dfree(b, bi); dfree(b, bw); dfree(b, bc);
+        b->bins_failed = true;
+        return rc;
+    }
+    CK(cudaMemsetAsync(bc, 0, sizeof(uint32_t) * (size_t)n_bins, b->stream));
+    s.bin_idx = bi; s.bin_w = bw; s.bin_cnt = bc;
+    s.n_bins = n_bins;
+    s.bin_cap = (uint32_t)cap;
+    s.bin_shift = B;
+    const size_t smem = bin_smem_layout(n_bins).total;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        CK(cudaFuncSetAttribute(k_bin_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_set = smem;
+    }
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_scatter, kBinThreads, smem));
+    b->bin_scatter_per_sm = std::max(1, per_sm);
+    b->bins_pending = false;
+    drop_graphs(b);
+    return DTB_OK;
+}
+
+static bool use_bins(dtb_block* b)
+{
+    if (b->push_method == 1 || !b->has_push) return false;
+    if (b->push_method == 0 && (b->bins_failed || !bins_possible(b))) return false;
+    return true;
+}
+
+static int launch_bin_scatter(dtb_block* b, const DevState& s)
+{
+    const int wpr = bin_words_for(b);
+    const int64_t rounds = (s.n_words + wpr - 1) / wpr;
+    if (rounds <= 0) return DTB_OK;
+    const unsigned grid = (unsigned)std::min<int64_t>(rounds, (int64_t)std::max(1, b->n_sm) * b->bin_scatter_per_sm);
+    k_bin_scatter<<<grid, kBinThreads, bin_smem_layout(s.n_bins).total, b->stream>>>(s, wpr);
+    CK(cudaGetLastError());
+    b->launches++;
+    return DTB_OK;
+}
+
+// Folds events still waiting in the bins into J (before anything else reads J).
+static int flush_bins(dtb_block* b)
+{
+    if (!b->bins_pending) return DTB_OK;
+    b->bins_pending = false;
+    launch_step_bins<false, false, 2>(b, b->ds);
+    CK(cudaGetLastError());
+    b->launches++;
+    return DTB_OK;
+}
+
+// Drops events still waiting in the bins (J is about to be overwritten).
+static int discard_bins(dtb_block* b)
+{
+    if (!b->bins_pending) return DTB_OK;
+    b->bins_pending = false;
+    CK(cudaMemsetAsync(b->ds.bin_cnt, 0, sizeof(uint32_t) * (size_t)b->ds.n_bins, b->stream));
+    return DTB_OK;
+}
+
 // Internal propagation methods: DTB_MODE_PUSH, DTB_MODE_PULL (row gather) and
 // the ordered push that DTB_MODE_PULL resolves to while activity is low.
 constexpr int kModeSlots = 3;
 constexpr int kModeMasks = 4;
 constexpr int kModeStream = 5;
+constexpr int kModeBinned = 6;
 
 static int ensure_slots(dtb_block* b)
 {
@@ -761,6 +917,11 @@ static int enqueue_steps(dtb_block* b, int n, int mode)
             RET(launch_update(b, s, 0, false));
             RET(launch_scatter(b, s));
         }
+    } else if (mode == kModeBinned) {
+        for (int k = 0; k < n; ++k) {
+            RET(launch_update(b, s, kGatherBins, false));
+            RET(launch_bin_scatter(b, s));
+        }
     } else if (mode == kModeSlots || mode == kModeMasks) {
         const int g = mode == kModeSlots ? kGatherSlots : kGatherMasks;
         const int how = mode == kModeSlots ? kScatterSlots : kScatterMasks;
@@ -780,7 +941,20 @@ static int enqueue_steps(dtb_block* b, int n, int mode)
     return DTB_OK;
 }
 
+static int enqueue_chunk_inner(dtb_block* b, int n, int mode);
+
+// The binned push leaves its last step's events in the bins; any other method first
+// folds them into J.
 static int enqueue_chunk(dtb_block* b, int n, int mode)
+{
+    if (n <= 0) return DTB_OK;
+    if (mode != kModeBinned) RET(flush_bins(b));
+    RET(enqueue_chunk_inner(b, n, mode));
+    if (mode == kModeBinned) b->bins_pending = true;
+    return DTB_OK;
+}
+
+static int enqueue_chunk_inner(dtb_block* b, int n, int mode)
 {
     if (!b->use_graphs || n != b->chunk || b->stream == nullptr) return enqueue_steps(b, n, mode);
     cudaGraphExec_t& ge = b->graph[mode];
@@ -818,6 +992,7 @@ static int choose_mode(dtb_block* b, int mode)
 // positions and activity is low enough that rows rarely overflow their slots.
 static int resolve_method(dtb_block* b, int m)
 {
+    if (m == DTB_MODE_PUSH) return (use_bins(b) && ensure_bins(b) == DTB_OK) ? kModeBinned : DTB_MODE_PUSH;
     if (m != DTB_MODE_PULL || b->pull_method == 1) return m;
     if (b->pull_method == 4 || !b->has_qpos || !b->has_push) return kModeStream;
     if (b->pull_method == 2) return kModeSlots;
@@ -1464,7 +1639,21 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
     auto rec = [&](int i) { return cudaEventRecord(ev[(size_t)i], b->stream); };
     int rc = DTB_OK;
     int done_steps = 0;
-    if (m == DTB_MODE_PUSH || m == kModeSlots || m == kModeMasks) {
+    if (m != kModeBinned) rc = flush_bins(b);
+    if (rc != DTB_OK) {
+        for (auto& x : ev) cudaEventDestroy(x);
+        return rc;
+    }
+    if (m == kModeBinned) {
+        for (int st = 0; st < n_steps && rc == DTB_OK && k + 6 <= n_ev; ++st) {
+            rec(k); rc = launch_update(b, b->ds, kGatherBins, false); rec(k + 1);
+            kind.push_back(0); k += 2;
+            if (rc != DTB_OK) break;
+            rec(k); rc = launch_bin_scatter(b, b->ds); rec(k + 1); kind.push_back(1); k += 2;
+            done_steps++;
+        }
+        if (done_steps) b->bins_pending = true;
+    } else if (m == DTB_MODE_PUSH || m == kModeSlots || m == kModeMasks) {
         const bool ord = m != DTB_MODE_PUSH;
         const int g = m == kModeSlots ? kGatherSlots : kGatherMasks;
         const int how = m == kModeSlots ? kScatterSlots : (m == kModeMasks ? kScatterMasks : kScatterJ);
@@ -1549,6 +1738,30 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         if (value < 0 || value > 4) return fail(DTB_ERR_ARG, "step variant must be 0..4");
         b->step_variant = (int)value;
         break;
+    case DTB_TUNE_PUSH_METHOD:
+        if (value < 0 || value > 2) return fail(DTB_ERR_ARG, "push method must be 0 (auto), 1 (atomics) or 2 (binned)");
+        if (value == 2 && !bins_possible(b)) return fail(DTB_ERR_STATE, "binned push not possible for this network");
+        if (value == 2) { b->bins_failed = false; RET(ensure_bins(b)); }
+        b->push_method = (int)value;
+        break;
+    case DTB_TUNE_BIN_WORDS:
+        if (value < 1 || value > kBinMaxWords) return fail(DTB_ERR_ARG, "bin scatter words per round must be 1..%d", kBinMaxWords);
+        b->bin_words = (int)value;
+        break;
+    case DTB_TUNE_BIN_CAPACITY:
+    case DTB_TUNE_BIN_SHIFT: {
+        if (key == DTB_TUNE_BIN_CAPACITY && (value < 1 || value > 1024))
+            return fail(DTB_ERR_ARG, "bin capacity must be 1..1024 entries per neuron");
+        if (key == DTB_TUNE_BIN_SHIFT && value != 0 && (value < kBinMinShift || value > kBinMaxShift))
+            return fail(DTB_ERR_ARG, "bin shift must be 0 (auto) or %d..%d", kBinMinShift, kBinMaxShift);
+        RET(flush_bins(b));   // the events waiting in the old bins go to J first
+        CK(cudaStreamSynchronize(b->stream));
+        free_bins(b);
+        b->bins_failed = false;
+        if (key == DTB_TUNE_BIN_CAPACITY) b->bin_cap_per_neuron = (int)value;
+        else b->bin_shift_req = (int)value;
+        break;
+    }
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
     }
     drop_graphs(b);
@@ -1567,6 +1780,10 @@ int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value)
     case DTB_TUNE_PULL_METHOD: *value = b->pull_method; break;
     case DTB_TUNE_J_CACHE: *value = b->ds.j_keep; break;
     case DTB_TUNE_SCATTER_VARIANT: *value = b->scatter_variant; break;
+    case DTB_TUNE_PUSH_METHOD: *value = b->push_method; break;
+    case DTB_TUNE_BIN_WORDS: *value = b->bin_words; break;
+    case DTB_TUNE_BIN_CAPACITY: *value = b->bin_cap_per_neuron; break;
+    case DTB_TUNE_BIN_SHIFT: *value = b->ds.bin_cnt ? b->ds.bin_shift : bin_shift_for(b); break;
     default: return fail(DTB_ERR_ARG, "unknown tuning key %d", key);
     }
     return DTB_OK;
@@ -1577,6 +1794,8 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
     if (!b || n_steps < 2) return fail(DTB_ERR_ARG, "bad argument");
     float best_ms = 1e30f, push_ms = 0.0f, pull_ms = 0.0f, ev = 0.0f;
     int best_w = b->scatter_wpw;
+    const int pm0 = b->push_method;
+    if (b->has_push) b->push_method = 1;   // atomic push first
     {   // register budget of the update kernel
         const int mode = b->has_push ? DTB_MODE_PUSH : DTB_MODE_PULL;
         float best_u = 1e30f;
@@ -1610,6 +1829,31 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
             RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PUSH, o));
             if (o[2] < best_ms) { best_ms = o[2]; ev = o[3]; }
             else b->ds.j_keep = keep;
+        }
+        // binned push: update register budget x scatter round size, kept when faster
+        b->push_method = pm0;
+        if (pm0 != 1 && bins_possible(b) && ensure_bins(b) == DTB_OK) {
+            const int atomic_v = b->step_variant, atomic_words = b->bin_words;
+            float best_b = 1e30f, ev_b = 0.0f;
+            int bv = 0, bw = atomic_words;
+            b->push_method = 2;
+            for (int v = 0; v < 2; ++v)
+                for (int w : {16, 32, 64}) {
+                    b->step_variant = v;
+                    b->bin_words = w;
+                    float o[4];
+                    RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PUSH, o));
+                    if (o[2] < best_b) { best_b = o[2]; bv = v; bw = w; ev_b = o[3]; }
+                }
+            if (best_b < best_ms) {
+                best_ms = best_b; ev = ev_b;
+                b->step_variant = bv; b->bin_words = bw;
+            } else {
+                b->push_method = 1;
+                b->step_variant = atomic_v; b->bin_words = atomic_words;
+            }
+        } else if (pm0 == 0) {
+            b->push_method = 1;
         }
         push_ms = best_ms;
     }
@@ -1654,9 +1898,19 @@ int dtb_block_step_forced(dtb_block* b, float noise_rate, int isolated, int mode
     RET(check_src_steps(b, 1));
     RET(set_run_params(b, noise_rate, isolated));
     const int m = choose_mode(b, mode);
-    RET(launch_update(b, s, 0, true));
-    if (m == DTB_MODE_PUSH) RET(launch_scatter(b, s));
-    else RET(launch_gather_only(b, s));
+    const int mm = m == DTB_MODE_PUSH ? resolve_method(b, m) : m;
+    if (mm == kModeBinned) {
+        s.bin_idx = b->ds.bin_idx; s.bin_w = b->ds.bin_w; s.bin_cnt = b->ds.bin_cnt;
+        s.n_bins = b->ds.n_bins; s.bin_cap = b->ds.bin_cap; s.bin_shift = b->ds.bin_shift;
+        RET(launch_update(b, s, kGatherBins, true));
+        RET(launch_bin_scatter(b, s));
+        b->bins_pending = true;
+    } else {
+        RET(flush_bins(b));
+        RET(launch_update(b, s, 0, true));
+        if (m == DTB_MODE_PUSH) RET(launch_scatter(b, s));
+        else RET(launch_gather_only(b, s));
+    }
     b->steps += 1;
     RET(emit_stats(b, 1, 0, sum_out, mean_out, nullptr, where, nullptr));
     CK(cudaStreamSynchronize(b->stream));
@@ -1680,6 +1934,7 @@ int dtb_block_get(dtb_block* b, int field, void* dst, int where)
     case DTB_FIELD_V: return copy_out(b, dst, s.V, sizeof(float) * N, where);
     case DTB_FIELD_T_LAST: return copy_out(b, dst, s.tlast, sizeof(float) * N, where);
     case DTB_FIELD_J: {
+        RET(flush_bins(b));
         void* p; RET(export_buf(&p));
         k_export_J<<<grid_for(N, 256), 256, 0, b->stream>>>(s, (float*)p);
         CK(cudaGetLastError());
@@ -1692,6 +1947,7 @@ int dtb_block_get(dtb_block* b, int field, void* dst, int where)
             if (field == DTB_FIELD_I_SYN) return copy_out(b, dst, s.isyn_override, sizeof(float) * N, where);
             return copy_out(b, dst, b->d_iui_override, sizeof(float) * 4 * N, where);
         }
+        RET(flush_bins(b));
         void* p; RET(export_buf(&p));
         if (field == DTB_FIELD_I_UI) k_export_current<<<grid_for(N, 256), 256, 0, b->stream>>>(s, (float*)p, nullptr);
         else k_export_current<<<grid_for(N, 256), 256, 0, b->stream>>>(s, nullptr, (float*)p);
@@ -1740,6 +1996,22 @@ int dtb_block_get_csr(dtb_block* b, int which, int64_t* rowptr, uint32_t* index,
     return DTB_OK;
 }
 
+int dtb_block_get_csr_entries(dtb_block* b, int which, int64_t first, int64_t count, uint32_t* index, float* weight,
+                              int where)
+{
+    if (!b || (which != 0 && which != 1)) return fail(DTB_ERR_ARG, "bad argument");
+    if ((which == 0 && !b->has_pull) || (which == 1 && !b->has_push)) return fail(DTB_ERR_STATE, "CSR not built");
+    if (first < 0 || count < 0 || first > b->S || count > b->S - first)
+        return fail(DTB_ERR_ARG, "entries [%lld, %lld) outside [0, %lld)", (long long)first, (long long)(first + count),
+                    (long long)b->S);
+    DeviceGuard g(b->device);
+    const uint32_t* c = which ? b->ds.qcol : b->ds.pcol;
+    const float2* w = which ? b->ds.qw : b->ds.pw;
+    if (index && count) RET(copy_out(b, index, c + first, sizeof(uint32_t) * (size_t)count, where));
+    if (weight && count) RET(copy_out(b, weight, w + first, sizeof(float2) * (size_t)count, where));
+    return DTB_OK;
+}
+
 int dtb_block_set(dtb_block* b, int field, const void* src, int where)
 {
     if (!b || !src) return fail(DTB_ERR_ARG, "null argument");
@@ -1751,6 +2023,7 @@ int dtb_block_set(dtb_block* b, int field, const void* src, int where)
     case DTB_FIELD_V: CK(cudaMemcpyAsync(s.V, src, sizeof(float) * N, k, b->stream)); break;
     case DTB_FIELD_T_LAST: CK(cudaMemcpyAsync(s.tlast, src, sizeof(float) * N, k, b->stream)); break;
     case DTB_FIELD_J: {
+        RET(discard_bins(b));
         if (!b->d_export) RET(dalloc(b, &b->d_export, (size_t)N * 4));
         CK(cudaMemcpyAsync(b->d_export, src, sizeof(float) * 4 * N, k, b->stream));
         k_J_from_planar<<<grid_for(N, 256), 256, 0, b->stream>>>(s, b->d_export);
@@ -1784,6 +2057,7 @@ static int keep_current_isyn(dtb_block* b)
 {
     DevState& s = b->ds;
     if (b->override_pending || b->N <= 0) return DTB_OK;
+    RET(flush_bins(b));
     if (!b->d_iui_override) RET(dalloc(b, &b->d_iui_override, (size_t)b->N * 4));
     k_export_current<<<grid_for(b->N, 256), 256, 0, b->stream>>>(s, b->d_iui_override, s.isyn_override);
     CK(cudaGetLastError());
@@ -2060,6 +2334,7 @@ int dtb_block_save(dtb_block* b, const char* path)
     std::vector<float> V((size_t)N), T((size_t)N), I((size_t)N);
     std::vector<float4> J((size_t)N);
     float t = 0.0f;
+    RET(flush_bins(b));
     CK(cudaStreamSynchronize(b->stream));
     CK(cudaMemcpy(V.data(), b->ds.V, 4 * N, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(J.data(), b->ds.J2, 8 * N, cudaMemcpyDeviceToHost));                       // AMPA, NMDA plane
@@ -2104,6 +2379,7 @@ int dtb_block_load(dtb_block* b, const char* path)
     if (ok && ov) ok = std::fread(I.data(), 4, (size_t)N, f) == (size_t)N;
     std::fclose(f);
     if (!ok) return fail(DTB_ERR_FORMAT, "truncated checkpoint %s", path);
+    RET(discard_bins(b));
     CK(cudaStreamSynchronize(b->stream));
     CK(cudaMemcpy(b->ds.V, V.data(), 4 * N, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b->ds.J2, J.data(), 8 * N, cudaMemcpyHostToDevice));

@@ -24,6 +24,10 @@ constexpr int kGatherRows = 1;         // k_step gathers whole pull rows
 constexpr int kGatherSlots = 2;        // k_step sums its ordered-push slots
 constexpr int kGatherMasks = 3;        // k_step sums the pull entries its position masks mark
 constexpr int kGatherStream = 4;       // k_step streams its tile's pull entries, chunk by chunk
+constexpr int kGatherBins = 5;         // k_step folds its chunk's binned push events (CTA-wide, shared memory)
+constexpr int kBinMinShift = 10;       // binned push: 2^bin_shift neurons per bin (= update chunk), 10..13
+constexpr int kBinMaxShift = 13;
+constexpr int kBinMaxBins = 32768;     // bins per network (u16 counters in the scatter's shared table)
 constexpr int kStreamWarpBytes = 129 * 8 + 8 + 128 * 16;   // row pointers (+pad) and row sums per warp
 constexpr int kMaskWords = 4;          // position-mask words per kind: in-degree up to 128
 constexpr int kMaskList = 256;         // marked entries a warp gathers together per tile
@@ -122,6 +126,14 @@ struct DevState {
     uint32_t* slot_cnt;         // [N] contributions written since the neuron last consumed them
     uint4* slots;               // [N][kSlotCap] {pull-row position | kind bit, 0, w.x bits, w.y bits}
     uint32_t* pmask;            // [N][2][kMaskWords] pull-row positions that fired (excitatory, inhibitory)
+    // binned push: the scatter appends every synaptic event {neuron within bin | kind << 15, w} to the bin of
+    // its postsynaptic neuron; the next update folds each bin into its chunk in shared memory
+    uint16_t* bin_idx;          // [n_bins][bin_cap]
+    float2* bin_w;              // [n_bins][bin_cap]
+    uint32_t* bin_cnt;          // [n_bins] events appended (may exceed bin_cap: the rest went to J by atomics)
+    int64_t n_bins;
+    uint32_t bin_cap;           // entries per bin (n_bins * bin_cap < 2^32)
+    int bin_shift;              // 2^bin_shift neurons per bin
     // statistics
     int n_sub;
     uint32_t* sub_spk;          // [n_sub] accumulators (active)

@@ -390,6 +390,50 @@ __device__ __forceinline__ bool stage_wait(uint32_t mbar, uint32_t parity)
     return false;
 }
 
+// ------------------------------------------------------------ binned push: fold
+// CTA-wide: the events the push scatter appended to bin c (one bin = one chunk of
+// 2^bin_shift neurons) are summed into acc[2^bin_shift] (float4 per neuron:
+// AMPA, NMDA, GABAa, GABAb) with shared-memory atomics; the bin's count is reset
+// for the next scatter.  Events beyond the bin's capacity were added to J by the
+// scatter itself.  Every thread of the CTA calls it (three barriers).
+__device__ __forceinline__ void fold_bin(const DevState& s, int64_t c, float4* acc, uint32_t* sh_n)
+{
+    const int chunk_n = 1 << s.bin_shift;
+    __syncthreads();   // every warp is done with the previous chunk's sums
+    for (int i = threadIdx.x; i < chunk_n; i += kStepThreads) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (threadIdx.x == 0) {
+        const uint32_t n = s.bin_cnt[c];
+        *sh_n = n < s.bin_cap ? n : s.bin_cap;
+        if (n) s.bin_cnt[c] = 0u;
+    }
+    __syncthreads();
+    const uint32_t n = *sh_n;
+    const uint16_t* __restrict__ bi = s.bin_idx + c * (int64_t)s.bin_cap;
+    const float2* __restrict__ bw = s.bin_w + c * (int64_t)s.bin_cap;
+    float* af = reinterpret_cast<float*>(acc);
+    constexpr int U = 4;
+    for (uint32_t i0 = threadIdx.x; i0 < n; i0 += kStepThreads * U) {
+        uint32_t x[U];
+        float2 w[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t i = i0 + u * kStepThreads;
+            x[u] = 0u;
+            w[u] = make_float2(0.f, 0.f);
+            if (i < n) { x[u] = __ldcs(bi + i); w[u] = __ldcs(bw + i); }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (i0 + u * kStepThreads < n) {
+                float* a = af + ((x[u] & 0x7fffu) << 2) + ((x[u] >> 15) << 1);
+                atomicAdd(a, w[u].x);
+                atomicAdd(a + 1, w[u].y);
+            }
+        }
+    }
+    __syncthreads();
+}
+
 // ------------------------------------------------------------ step kernel
 // Persistent: the grid is sized to the resident CTAs, and every warp streams a
 // contiguous run of 128-neuron tiles (tiles_per_warp of them).  In a tile a
@@ -420,6 +464,20 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     const int64_t ntiles = (s.N + kWarpNeurons - 1) / kWarpNeurons;
     const int64_t tile0 = warp_id * tiles_per_warp;
     const int64_t tile1 = tile0 + tiles_per_warp < ntiles ? tile0 + tiles_per_warp : ntiles;
+    // kGatherBins: tiles_per_warp is the number of chunks (2^bin_shift neurons, one push
+    // bin each) per CTA.  The CTA folds chunk c's bin into bacc, then warp wid updates
+    // tiles wid*tpw_b .. wid*tpw_b + tpw_b - 1 of the chunk.
+    __shared__ uint32_t sh_bin_n;
+    float4* bacc = reinterpret_cast<float4*>(stage_smem);
+    const int tpw_b = GATHER == kGatherBins ? (1 << (s.bin_shift - 7)) / kWarps : 1;   // bin_shift >= 10
+    const int64_t chunk_tiles = (int64_t)tpw_b * kWarps;
+    const int64_t bc0 = (int64_t)blockIdx.x * tiles_per_warp;
+    int64_t n_iter = tile1 > tile0 ? tile1 - tile0 : 0;
+    if (GATHER == kGatherBins) {
+        const int64_t nchunks = (ntiles + chunk_tiles - 1) / chunk_tiles;
+        const int64_t bc1 = bc0 + tiles_per_warp < nchunks ? bc0 + tiles_per_warp : nchunks;
+        n_iter = bc1 > bc0 ? (bc1 - bc0) * tpw_b : 0;
+    }
 
     // update-phase constants (models/block.py:133-142)
     const Ctl* ctl = s.ctl;
@@ -451,7 +509,17 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         __syncwarp();
     }
 
-    for (int64_t tile = tile0; tile < tile1; ++tile) {
+    for (int64_t iter = 0; iter < n_iter; ++iter) {
+        int64_t tile = tile0 + iter;
+        int64_t bchunk = 0;
+        if (GATHER == kGatherBins) {   // CTA-uniform: every warp runs the same iterations
+            const int64_t ci = iter / tpw_b;
+            const int jj = (int)(iter - ci * tpw_b);
+            bchunk = bc0 + ci;
+            if (jj == 0) fold_bin(s, bchunk, bacc, &sh_bin_n);
+            tile = bchunk * chunk_tiles + (int64_t)wid * tpw_b + jj;
+            if (tile >= ntiles) continue;
+        }
         const int64_t base = tile * kWarpNeurons;
         float4 Jn[4];
         const int it = (int)(tile - tile0);
@@ -678,6 +746,21 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 if (n < s.N) Jn[j] = add4(load_J(s, n), acc[j * 32 + lane]);   // models/block.py:71-73
             }
             __syncwarp();   // the row pointers and sums are rewritten by the next tile
+            if (!UPDATE) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int64_t n = base + j * 32 + lane;
+                    if (n < s.N) store_J(s, n, Jn[j]);
+                }
+                continue;
+            }
+        } else if (GATHER == kGatherBins) {
+            const float4* acc = bacc + (base - bchunk * chunk_tiles * kWarpNeurons);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int64_t n = base + j * 32 + lane;
+                if (n < s.N) Jn[j] = add4(load_J(s, n), acc[j * 32 + lane]);
+            }
             if (!UPDATE) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -1044,6 +1127,229 @@ __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, i
                     if (ok[u])
                         atomicAdd(s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + (int64_t)(c[u] & kIndexMask) * s.j_es, w[u]);
             }
+        }
+    }
+}
+
+// ------------------------------------------------------------ binned push scatter
+// cuda/src/stage/presynaptic_voltage.cpp:152-266 (every synapse of a firing row
+// adds its weight pair to its postsynaptic neuron), with the additions staged:
+// instead of one L2 float atomic per synaptic event, every event is appended to
+// the bin of its postsynaptic neuron (2^bin_shift neurons per bin) and the next
+// update folds each bin in shared memory (fold_bin).
+//
+// A persistent CTA takes rounds of `wpr` bitmask words (grid-strided), lists the
+// round's firing rows and their bounds in shared memory, and walks the
+// concatenated synapses of those rows in slices of kBinSlice events (8 per
+// thread, coalesced index/weight loads).  Per slice: shared-memory atomics on
+// 16-bit per-bin counters rank every event inside its bin; one global atomic per
+// touched bin reserves the slice's run in that bin; the events are placed in a
+// shared staging buffer sorted by bin and written out run by run (coalesced).
+// An event past its bin's capacity goes to J with a float2 atomic instead, so
+// any activity level gives the right sums.
+constexpr int kBinThreads = 256;
+constexpr int kBinEPT = 8;                                  // events per thread and slice
+constexpr int kBinSlice = kBinThreads * kBinEPT;            // 2048
+constexpr int kBinMaxWords = 64;                            // bitmask words per round
+constexpr int kBinMaxRows = kBinMaxWords * 32;              // 2048 rows per round
+constexpr uint32_t kBinSkip = 0xffffffffu;
+
+// Dynamic shared memory of k_bin_scatter (all offsets multiples of 16).
+struct BinSmemLayout {
+    size_t w, e0, off, dst, tg, cnt, tbin, tl, idx, total;
+};
+__host__ __device__ inline BinSmemLayout bin_smem_layout(int64_t n_bins)
+{
+    BinSmemLayout L;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { const size_t at = o; o += (bytes + 15) & ~(size_t)15; return at; };
+    L.w = take(sizeof(float2) * kBinSlice);
+    L.e0 = take(sizeof(int64_t) * kBinMaxRows);
+    L.off = take(sizeof(int32_t) * (kBinMaxRows + 1));
+    L.dst = take(sizeof(uint32_t) * kBinSlice);
+    L.tg = take(sizeof(uint32_t) * kBinSlice);
+    L.cnt = take(sizeof(uint32_t) * (size_t)((n_bins + 1) / 2));
+    L.tbin = take(sizeof(uint16_t) * kBinSlice);
+    L.tl = take(sizeof(uint16_t) * kBinSlice);
+    L.idx = take(sizeof(uint16_t) * kBinSlice);
+    L.total = o;
+    return L;
+}
+
+// Exclusive prefix sum over the CTA (kBinThreads threads); *total gets the sum.
+__device__ __forceinline__ int bin_block_scan(int v, int* sh_warp, int* total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) sh_warp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int x = lane < kBinThreads / 32 ? sh_warp[lane] : 0;
+        int xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) xi += y;
+        }
+        if (lane < kBinThreads / 32) sh_warp[lane] = xi - x;   // exclusive warp offsets
+        if (lane == 31) sh_warp[kBinThreads / 32] = xi;
+    }
+    __syncthreads();
+    const int r = sh_warp[wid] + incl - v;
+    *total = sh_warp[kBinThreads / 32];
+    __syncthreads();   // sh_warp is reused by the next scan
+    return r;
+}
+
+__global__ void __launch_bounds__(kBinThreads, 2) k_bin_scatter(DevState s, int wpr)
+{
+    extern __shared__ __align__(16) unsigned char bsm[];
+    __shared__ int sh_warp[kBinThreads / 32 + 1];
+    __shared__ int sh_nt;
+    const BinSmemLayout L = bin_smem_layout(s.n_bins);
+    float2* st_w = reinterpret_cast<float2*>(bsm + L.w);
+    int64_t* row_e0 = reinterpret_cast<int64_t*>(bsm + L.e0);
+    int32_t* row_off = reinterpret_cast<int32_t*>(bsm + L.off);
+    uint32_t* st_dst = reinterpret_cast<uint32_t*>(bsm + L.dst);
+    uint32_t* row_pre = st_dst;                                   // listing only (before the slices)
+    uint32_t* t_g = reinterpret_cast<uint32_t*>(bsm + L.tg);
+    uint32_t* cnt32 = reinterpret_cast<uint32_t*>(bsm + L.cnt);   // two 16-bit counters per word
+    uint16_t* cnt16 = reinterpret_cast<uint16_t*>(bsm + L.cnt);
+    uint16_t* t_bin = reinterpret_cast<uint16_t*>(bsm + L.tbin);
+    uint16_t* t_l = reinterpret_cast<uint16_t*>(bsm + L.tl);
+    uint16_t* st_idx = reinterpret_cast<uint16_t*>(bsm + L.idx);
+
+    const int tid = threadIdx.x;
+    const unsigned long long steps_done = s.ctl->steps_done;
+    const uint32_t* __restrict__ bits = s.bits[(steps_done - 1ull) & 1ull];
+    const int B = s.bin_shift;
+    const uint32_t lmask = (1u << B) - 1u;
+    const uint32_t cap = s.bin_cap;
+    const int64_t n_rounds = (s.n_words + wpr - 1) / wpr;
+
+    for (int64_t i = tid; i < (s.n_bins + 1) / 2; i += kBinThreads) cnt32[i] = 0u;
+    if (tid == 0) sh_nt = 0;
+    __syncthreads();
+
+    for (int64_t r = blockIdx.x; r < n_rounds; r += gridDim.x) {
+        // ---- the round's firing rows, in neuron order
+        const int64_t w0 = r * wpr;
+        uint32_t word = (tid < wpr && w0 + tid < s.n_words) ? __ldcs(bits + w0 + tid) : 0u;
+        int nrows;
+        int pos = bin_block_scan(__popc(word), sh_warp, &nrows);
+        while (word) {
+            const int b = __ffs(word) - 1;
+            word &= word - 1u;
+            row_pre[pos++] = (uint32_t)((w0 + tid) * 32 + b);
+        }
+        __syncthreads();
+        int len[kBinMaxRows / kBinThreads];
+        int mine = 0;
+#pragma unroll
+        for (int q = 0; q < kBinMaxRows / kBinThreads; ++q) {
+            const int i = tid * (kBinMaxRows / kBinThreads) + q;
+            len[q] = 0;
+            if (i < nrows) {
+                const uint32_t pre = row_pre[i];
+                const int64_t e0 = __ldg(s.qrow + pre);
+                len[q] = (int)(__ldg(s.qrow + pre + 1) - e0);
+                row_e0[i] = e0;
+                mine += len[q];
+            }
+        }
+        int T;
+        int ex = bin_block_scan(mine, sh_warp, &T);
+#pragma unroll
+        for (int q = 0; q < kBinMaxRows / kBinThreads; ++q) {
+            const int i = tid * (kBinMaxRows / kBinThreads) + q;
+            if (i < nrows) { row_off[i] = ex; ex += len[q]; }
+        }
+        if (tid == 0) row_off[nrows] = T;
+        __syncthreads();
+
+        // ---- slices of kBinSlice events
+        for (int v0 = 0; v0 < T; v0 += kBinSlice) {
+            uint32_t c[kBinEPT], rk[kBinEPT];
+            float2 w[kBinEPT];
+#pragma unroll
+            for (int u = 0; u < kBinEPT; ++u) {
+                const int v = v0 + u * kBinThreads + tid;
+                c[u] = kBinSkip;
+                if (v < T) {
+                    int lo = 0, hi = nrows;   // row_off[lo] <= v < row_off[hi]
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) >> 1;
+                        if (row_off[mid] <= v) lo = mid; else hi = mid;
+                    }
+                    const int64_t e = row_e0[lo] + (v - row_off[lo]);
+                    c[u] = __ldcs(s.qcol + e);
+                    w[u] = __ldcs(s.qw + e);
+                }
+            }
+            // rank of every event inside its bin; first event of a bin lists the bin
+#pragma unroll
+            for (int u = 0; u < kBinEPT; ++u) {
+                rk[u] = 0u;
+                if (c[u] != kBinSkip) {
+                    const uint32_t bin = (c[u] & kIndexMask) >> B;
+                    const uint32_t sh = (bin & 1u) << 4;
+                    rk[u] = (atomicAdd(cnt32 + (bin >> 1), 1u << sh) >> sh) & 0xffffu;
+                    if (rk[u] == 0u) t_bin[atomicAdd(&sh_nt, 1)] = (uint16_t)bin;
+                }
+            }
+            __syncthreads();
+            const int nt = sh_nt;
+            // per touched bin (contiguous ranges per thread): staging offset and the run reserved in the bin
+            const int per = (nt + kBinThreads - 1) / kBinThreads;
+            const int k0 = tid * per < nt ? tid * per : nt;
+            const int k1 = k0 + per < nt ? k0 + per : nt;
+            int sum = 0;
+            for (int k = k0; k < k1; ++k) sum += cnt16[t_bin[k]];
+            int tot;
+            int lo = bin_block_scan(sum, sh_warp, &tot);
+            for (int k = k0; k < k1; ++k) {
+                const uint32_t bin = t_bin[k];
+                const uint32_t cn = cnt16[bin];
+                t_l[k] = (uint16_t)lo;
+                lo += (int)cn;
+                t_g[k] = atomicAdd(s.bin_cnt + bin, cn);
+                cnt16[bin] = (uint16_t)k;   // from here on: the bin's touched index
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < kBinEPT; ++u) {
+                if (c[u] == kBinSkip) continue;
+                const uint32_t post = c[u] & kIndexMask;
+                const uint32_t bin = post >> B;
+                const uint32_t k = cnt16[bin];
+                const uint32_t lp = (uint32_t)t_l[k] + rk[u];
+                const uint32_t g = t_g[k] + rk[u];
+                if (g < cap) {
+                    st_dst[lp] = bin * cap + g;
+                    st_w[lp] = w[u];
+                    st_idx[lp] = (uint16_t)((post & lmask) | ((c[u] >> 31) << 15));
+                } else {   // bin full: straight into J
+                    st_dst[lp] = kBinSkip;
+                    atomicAdd(s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + (int64_t)post * s.j_es, w[u]);
+                }
+            }
+            __syncthreads();
+            const int n_slice = T - v0 < kBinSlice ? T - v0 : kBinSlice;
+            for (int i = tid; i < n_slice; i += kBinThreads) {
+                const uint32_t d = st_dst[i];
+                if (d != kBinSkip) {
+                    s.bin_idx[d] = st_idx[i];
+                    s.bin_w[d] = st_w[i];
+                }
+            }
+            for (int k = tid; k < nt; k += kBinThreads) cnt16[t_bin[k]] = 0;
+            if (tid == 0) sh_nt = 0;
+            __syncthreads();
         }
     }
 }

@@ -231,6 +231,28 @@ class Network:
         _lib.call("dtb_block_get_csr", self._h, 0 if which == "pull" else 1, _ptr(rp), _ptr(ix), _ptr(w), DTB_HOST)
         return rp, ix, w
 
+    def get_csr_rowptr(self, which: str = "pull") -> np.ndarray:
+        rp = np.empty(self.N + 1, np.int64)
+        _lib.call("dtb_block_get_csr", self._h, 0 if which == "pull" else 1, _ptr(rp), None, None, DTB_HOST)
+        return rp
+
+    def get_csr_entries(self, which: str, first: int, count: int, device: bool = False, weights: bool = True):
+        """Entries [first, first+count) of a CSR: (index uint32 with bit 31 = GABA pair, weight [count,2]);
+        numpy on the host, or torch CUDA tensors (index as int32 bits) with device=True."""
+        which_i = 0 if which == "pull" else 1
+        if device:
+            dev = torch.device("cuda", self.device)
+            ix = torch.empty(count, dtype=torch.int32, device=dev)
+            w = torch.empty((count, 2), dtype=torch.float32, device=dev) if weights else None
+            _lib.call("dtb_block_get_csr_entries", self._h, which_i, int(first), int(count), _ptr(ix), _ptr(w),
+                      DTB_DEVICE)
+            self.synchronize()
+            return ix, w
+        ix = np.empty(count, np.uint32)
+        w = np.empty((count, 2), np.float32) if weights else None
+        _lib.call("dtb_block_get_csr_entries", self._h, which_i, int(first), int(count), _ptr(ix), _ptr(w), DTB_HOST)
+        return ix, w
+
     def set(self, field: int, value):
         if field == FIELD_T:
             arr = np.asarray([value], np.float32)

@@ -233,15 +233,33 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  * DTB_TUNE_J_CACHE         0 = the update streams J (evict first), 1 = its J
  *                          stores keep normal L2 priority for the scatter
  * DTB_TUNE_SCATTER_VARIANT push scatter registers: 0 = unbounded, 1 = budgeted
- *                          for six resident CTAs per SM */
+ *                          for six resident CTAs per SM
+ * DTB_TUNE_PUSH_METHOD     how DTB_MODE_PUSH adds the weights of firing rows
+ *                          (the order of the float additions differs, the sums
+ *                          agree to rounding): 1 = one float2 atomic into J per
+ *                          synaptic event; 2 = binned: every event is appended
+ *                          to the bin of its postsynaptic neuron (a run of 2^B
+ *                          neurons) and the next update adds each bin to its
+ *                          neurons in shared memory, events past a bin's
+ *                          capacity going to J by atomics; 0 = binned whenever
+ *                          the network allows it (push CSR, at most 2^28
+ *                          neurons) and its bins could be allocated; default 1,
+ *                          dtb_block_autotune keeps the faster of 1 and 2
+ * DTB_TUNE_BIN_WORDS       binned push: bitmask words (32 neurons each) whose
+ *                          firing rows one scatter CTA takes per round (1..64)
+ * DTB_TUNE_BIN_CAPACITY    binned push: bin entries per neuron of the bin
+ *                          (1..1024, default 8; 10 bytes each); reallocates
+ * DTB_TUNE_BIN_SHIFT       binned push: B (10..13), 0 = chosen from N; reallocates */
 enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,
-       DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5, DTB_TUNE_J_CACHE = 6, DTB_TUNE_SCATTER_VARIANT = 7 };
+       DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5, DTB_TUNE_J_CACHE = 6, DTB_TUNE_SCATTER_VARIANT = 7,
+       DTB_TUNE_PUSH_METHOD = 8, DTB_TUNE_BIN_WORDS = 9, DTB_TUNE_BIN_CAPACITY = 10, DTB_TUNE_BIN_SHIFT = 11 };
 int dtb_block_set_tuning(dtb_block* b, int key, int64_t value);
 int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value);
 
-/* Autotuner: times the step kernel's two register budgets, the push scatter at 1, 2, 4, ..., 32 bitmask words per
- * warp and the pull gather on the live network (n_steps each; the
- * simulation advances), keeps the fastest scatter shape and sets the
+/* Autotuner: times the step kernel's register budgets, the atomic push scatter at 1, 2, 4, ..., 32 bitmask words
+ * per warp, the binned push at 16, 32 and 64 words per round (unless DTB_TUNE_PUSH_METHOD is 1) and the pull
+ * gather on the live network (n_steps each; the simulation advances), keeps the fastest push method and shape
+ * (DTB_TUNE_PUSH_METHOD becomes 1 or 2) and sets the
  * AUTO push/pull threshold from the measured costs at the current activity.
  * report (nullable, 6 floats): words per warp, push ms/step, pull ms/step,
  * activity fraction, threshold, step variant. */
@@ -258,6 +276,11 @@ int dtb_block_get(dtb_block* b, int field, void* dst, int where);
  * Any output may be NULL.  The layout of cuda/src/configuration.cpp:783-795
  * (rowptrs, colinds, float2 vals, connkinds) with the kind folded into bit 31. */
 int dtb_block_get_csr(dtb_block* b, int which, int64_t* rowptr, uint32_t* index, float* weight, int where);
+/* Entries [first, first + count) of the same CSR arrays (index[count], weight[count][2], either nullable):
+ * rows of a network too large to copy whole (configuration.cpp reads its tables back by range,
+ * cuda/src/configuration.cpp:214-341). */
+int dtb_block_get_csr_entries(dtb_block* b, int which, int64_t first, int64_t count, uint32_t* index,
+                              float* weight, int where);
 
 /* Overwrite V, J, T_LAST, T or STEP (checkpoint restore, tests). */
 int dtb_block_set(dtb_block* b, int field, const void* src, int where);

@@ -126,11 +126,14 @@ def test_small_blocks_drop_in_bit_exact_vs_reference():
     assert np.float32(b.t.item()) == g["t_final"]
 
 
-def test_push_teacher_forced_within_tolerance():
-    """Push scatter (float atomics, any order) under teacher forcing: V and J within 1e-5 relative."""
+@pytest.mark.parametrize("push_method", [1, 2], ids=["atomic", "binned"])
+def test_push_teacher_forced_within_tolerance(push_method):
+    """Push scatter (float atomics, any order; or binned) under teacher forcing: V and J within 1e-5 relative."""
+    from digital_twin_brain_b200._lib import TUNE_PUSH_METHOD
     g = np.load(os.path.join(GOLDEN, "single_block_2k.npz"))
     spec = synthetic.config_single_block()
     net = Network.from_spec(spec, device=0, build_push=True, class_decay=class_decay_like_reference(spec))
+    net.set_tuning(TUNE_PUSH_METHOD, push_method)
     act_ref = unpack(g["active"], spec.N)
     nact_ref = unpack(g["new_active"], spec.N)
     every = int(g["v_every"])
@@ -180,10 +183,11 @@ def test_autotune_and_tuning_knobs():
 def test_scatter_shapes_agree_with_pull_under_forcing(wpw, variant):
     """One push step from identical state at several launch shapes and register budgets vs the
     exact pull step."""
-    from digital_twin_brain_b200._lib import TUNE_SCATTER_VARIANT, TUNE_SCATTER_WORDS
+    from digital_twin_brain_b200._lib import TUNE_PUSH_METHOD, TUNE_SCATTER_VARIANT, TUNE_SCATTER_WORDS
     spec = synthetic.single_block(8000, 100, name="n8k")
     a = Network.from_spec(spec, device=0)
     b = Network.from_spec(spec, device=0)
+    a.set_tuning(TUNE_PUSH_METHOD, 1)     # the atomic scatter these shapes belong to
     a.set_tuning(TUNE_SCATTER_WORDS, wpw)
     a.set_tuning(TUNE_SCATTER_VARIANT, variant)
     for _ in range(80):
