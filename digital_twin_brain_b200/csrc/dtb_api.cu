@@ -172,7 +172,7 @@ struct dtb_block {
     int push_method = 1;          // 0: binned when its bins fit, 1: float2 atomics into J, 2: binned
     int bin_shift_req = 0;        // 0: chosen from N
     int bin_cap_per_neuron = 8;   // bin entries per neuron of a bin
-    int bin_words = 64;           // bitmask words per scatter round
+    int bin_words = 256;          // bitmask words per scatter round
     int bin_scatter_per_sm = 0;   // resident scatter CTAs per SM (from the occupancy calculator)
     bool bins_pending = false;    // the bins hold events not yet folded into J
     bool bins_failed = false;     // the bins could not be allocated (auto pushes with atomics)
@@ -755,15 +755,13 @@ static void drop_graphs(dtb_block* b)
 
 // ------------------------------------------------------------ binned push
 // Bin geometry: 2^B neurons per bin (the update's chunk), B >= 10 (one tile per warp of
-// the update CTA), at least 11 from 8M neurons, raised until the scatter's shared
-// counter table leaves room for two scatter CTAs per SM (n_bins <= 20000), at most
-// kBinMaxShift (the update's 16 << B bytes of sums).
+// the update CTA), 11 from 8M neurons (the scatter's window of kBinWin bins then spans
+// 2M neurons, more than a region), at most kBinMaxShift (the update's 16 << B bytes of
+// sums in shared memory).
 static int bin_shift_for(const dtb_block* b)
 {
     if (b->bin_shift_req) return b->bin_shift_req;
-    int B = b->N >= (int64_t)8 << 20 ? 11 : kBinMinShift;
-    while (B < kBinMaxShift && ((b->N + ((int64_t)1 << B) - 1) >> B) > 20000) ++B;
-    return B;
+    return b->N >= (int64_t)8 << 20 ? 11 : kBinMinShift;
 }
 
 // Bitmask words per scatter round: the round's synapses must stay below 2^31.
@@ -780,7 +778,7 @@ static bool bins_possible(const dtb_block* b)
     if (!b->has_push || b->N <= 0) return false;
     const int B = bin_shift_for(b);
     if (B > kBinMaxShift || ((b->N + ((int64_t)1 << B) - 1) >> B) > kBinMaxBins) return false;
-    return (int64_t)32 * std::max<int64_t>(1, b->max_out) < ((int64_t)1 << 31);
+    return (int64_t)32 * std::max<int64_t>(1, b->max_out) < ((int64_t)1 << 31);   // one round's synapses
 }
 
 static void free_bins(dtb_block* b)
@@ -818,14 +816,13 @@ static int ensure_bins(dtb_block* b)
     s.n_bins = n_bins;
     s.bin_cap = (uint32_t)cap;
     s.bin_shift = B;
-    const size_t smem = bin_smem_layout(n_bins).total;
-    static size_t smem_set = 0;
-    if (smem > smem_set) {
-        CK(cudaFuncSetAttribute(k_bin_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        smem_set = smem;
+    static bool smem_set = false;
+    if (!smem_set) {
+        CK(cudaFuncSetAttribute(k_bin_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, kBinSmem));
+        smem_set = true;
     }
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_scatter, kBinThreads, smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_scatter, kBinThreads, kBinSmem));
     b->bin_scatter_per_sm = std::max(1, per_sm);
     b->bins_pending = false;
     drop_graphs(b);
@@ -845,7 +842,7 @@ static int launch_bin_scatter(dtb_block* b, const DevState& s)
     const int64_t rounds = (s.n_words + wpr - 1) / wpr;
     if (rounds <= 0) return DTB_OK;
     const unsigned grid = (unsigned)std::min<int64_t>(rounds, (int64_t)std::max(1, b->n_sm) * b->bin_scatter_per_sm);
-    k_bin_scatter<<<grid, kBinThreads, bin_smem_layout(s.n_bins).total, b->stream>>>(s, wpr);
+    k_bin_scatter<<<grid, kBinThreads, kBinSmem, b->stream>>>(s, wpr);
     CK(cudaGetLastError());
     b->launches++;
     return DTB_OK;
@@ -1838,7 +1835,7 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
             int bv = 0, bw = atomic_words;
             b->push_method = 2;
             for (int v = 0; v < 2; ++v)
-                for (int w : {16, 32, 64}) {
+                for (int w : {64, 128, 256}) {
                     b->step_variant = v;
                     b->bin_words = w;
                     float o[4];

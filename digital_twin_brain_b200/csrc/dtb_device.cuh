@@ -27,7 +27,7 @@ constexpr int kGatherStream = 4;       // k_step streams its tile's pull entries
 constexpr int kGatherBins = 5;         // k_step folds its chunk's binned push events (CTA-wide, shared memory)
 constexpr int kBinMinShift = 10;       // binned push: 2^bin_shift neurons per bin (= update chunk), 10..13
 constexpr int kBinMaxShift = 13;
-constexpr int kBinMaxBins = 32768;     // bins per network (u16 counters in the scatter's shared table)
+constexpr int kBinMaxBins = 1 << 22;  // bins per network (u32 entry addresses: bins x capacity < 2^32)
 constexpr int kStreamWarpBytes = 129 * 8 + 8 + 128 * 16;   // row pointers (+pad) and row sums per warp
 constexpr int kMaskWords = 4;          // position-mask words per kind: in-degree up to 128
 constexpr int kMaskList = 256;         // marked entries a warp gathers together per tile

@@ -395,40 +395,46 @@ __device__ __forceinline__ bool stage_wait(uint32_t mbar, uint32_t parity)
 // 2^bin_shift neurons) are summed into acc[2^bin_shift] (float4 per neuron:
 // AMPA, NMDA, GABAa, GABAb) with shared-memory atomics; the bin's count is reset
 // for the next scatter.  Events beyond the bin's capacity were added to J by the
-// scatter itself.  Every thread of the CTA calls it (three barriers).
-__device__ __forceinline__ void fold_bin(const DevState& s, int64_t c, float4* acc, uint32_t* sh_n)
+// scatter itself.  n_raw = the bin's count, read by the caller one chunk ahead;
+// the first entries are loaded before the barrier that frees acc.  Every thread
+// of the CTA calls it (three barriers).
+constexpr int kFoldBatch = 8;   // entries per thread in flight
+
+__device__ __forceinline__ void fold_bin(const DevState& s, int64_t c, float4* acc, uint32_t n_raw)
 {
     const int chunk_n = 1 << s.bin_shift;
-    __syncthreads();   // every warp is done with the previous chunk's sums
-    for (int i = threadIdx.x; i < chunk_n; i += kStepThreads) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (threadIdx.x == 0) {
-        const uint32_t n = s.bin_cnt[c];
-        *sh_n = n < s.bin_cap ? n : s.bin_cap;
-        if (n) s.bin_cnt[c] = 0u;
-    }
-    __syncthreads();
-    const uint32_t n = *sh_n;
+    const uint32_t n = n_raw < s.bin_cap ? n_raw : s.bin_cap;
     const uint16_t* __restrict__ bi = s.bin_idx + c * (int64_t)s.bin_cap;
     const float2* __restrict__ bw = s.bin_w + c * (int64_t)s.bin_cap;
     float* af = reinterpret_cast<float*>(acc);
-    constexpr int U = 4;
-    for (uint32_t i0 = threadIdx.x; i0 < n; i0 += kStepThreads * U) {
-        uint32_t x[U];
-        float2 w[U];
+    uint32_t x[kFoldBatch];
+    float2 w[kFoldBatch];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t i = i0 + u * kStepThreads;
-            x[u] = 0u;
-            w[u] = make_float2(0.f, 0.f);
-            if (i < n) { x[u] = __ldcs(bi + i); w[u] = __ldcs(bw + i); }
-        }
+    for (int u = 0; u < kFoldBatch; ++u) {
+        const uint32_t i = threadIdx.x + u * kStepThreads;
+        x[u] = 0u;
+        w[u] = make_float2(0.f, 0.f);
+        if (i < n) { x[u] = __ldcs(bi + i); w[u] = __ldcs(bw + i); }
+    }
+    __syncthreads();   // every warp is done with the previous chunk's sums
+    for (int i = threadIdx.x; i < chunk_n; i += kStepThreads) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (threadIdx.x == 0 && n_raw) s.bin_cnt[c] = 0u;
+    __syncthreads();
+    for (uint32_t i0 = 0;; i0 += kStepThreads * kFoldBatch) {
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (i0 + u * kStepThreads < n) {
+        for (int u = 0; u < kFoldBatch; ++u) {
+            if (i0 + threadIdx.x + u * kStepThreads < n) {
                 float* a = af + ((x[u] & 0x7fffu) << 2) + ((x[u] >> 15) << 1);
                 atomicAdd(a, w[u].x);
                 atomicAdd(a + 1, w[u].y);
             }
+        }
+        const uint32_t i1 = i0 + kStepThreads * kFoldBatch;
+        if (i1 >= n) break;
+#pragma unroll
+        for (int u = 0; u < kFoldBatch; ++u) {
+            const uint32_t i = i1 + threadIdx.x + u * kStepThreads;
+            if (i < n) { x[u] = __ldcs(bi + i); w[u] = __ldcs(bw + i); }
         }
     }
     __syncthreads();
@@ -467,16 +473,18 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     // kGatherBins: tiles_per_warp is the number of chunks (2^bin_shift neurons, one push
     // bin each) per CTA.  The CTA folds chunk c's bin into bacc, then warp wid updates
     // tiles wid*tpw_b .. wid*tpw_b + tpw_b - 1 of the chunk.
-    __shared__ uint32_t sh_bin_n;
     float4* bacc = reinterpret_cast<float4*>(stage_smem);
     const int tpw_b = GATHER == kGatherBins ? (1 << (s.bin_shift - 7)) / kWarps : 1;   // bin_shift >= 10
     const int64_t chunk_tiles = (int64_t)tpw_b * kWarps;
     const int64_t bc0 = (int64_t)blockIdx.x * tiles_per_warp;
     int64_t n_iter = tile1 > tile0 ? tile1 - tile0 : 0;
+    int64_t bc1 = bc0;
+    uint32_t bin_next = 0u;   // count of the next chunk's bin, read one chunk ahead
     if (GATHER == kGatherBins) {
         const int64_t nchunks = (ntiles + chunk_tiles - 1) / chunk_tiles;
-        const int64_t bc1 = bc0 + tiles_per_warp < nchunks ? bc0 + tiles_per_warp : nchunks;
+        bc1 = bc0 + tiles_per_warp < nchunks ? bc0 + tiles_per_warp : nchunks;
         n_iter = bc1 > bc0 ? (bc1 - bc0) * tpw_b : 0;
+        if (bc0 < bc1) bin_next = __ldcg(s.bin_cnt + bc0);
     }
 
     // update-phase constants (models/block.py:133-142)
@@ -516,7 +524,11 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             const int64_t ci = iter / tpw_b;
             const int jj = (int)(iter - ci * tpw_b);
             bchunk = bc0 + ci;
-            if (jj == 0) fold_bin(s, bchunk, bacc, &sh_bin_n);
+            if (jj == 0) {
+                const uint32_t n_raw = bin_next;
+                if (bchunk + 1 < bc1) bin_next = __ldcg(s.bin_cnt + bchunk + 1);
+                fold_bin(s, bchunk, bacc, n_raw);
+            }
             tile = bchunk * chunk_tiles + (int64_t)wid * tpw_b + jj;
             if (tile >= ntiles) continue;
         }
@@ -1134,47 +1146,38 @@ __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, i
 // ------------------------------------------------------------ binned push scatter
 // cuda/src/stage/presynaptic_voltage.cpp:152-266 (every synapse of a firing row
 // adds its weight pair to its postsynaptic neuron), with the additions staged:
-// instead of one L2 float atomic per synaptic event, every event is appended to
-// the bin of its postsynaptic neuron (2^bin_shift neurons per bin) and the next
+// instead of one L2 float atomic per synaptic event, events are appended to the
+// bin of their postsynaptic neuron (2^bin_shift neurons per bin) and the next
 // update folds each bin in shared memory (fold_bin).
 //
 // A persistent CTA takes rounds of `wpr` bitmask words (grid-strided), lists the
 // round's firing rows and their bounds in shared memory, and walks the
 // concatenated synapses of those rows in slices of kBinSlice events (8 per
-// thread, coalesced index/weight loads).  Per slice: shared-memory atomics on
-// 16-bit per-bin counters rank every event inside its bin; one global atomic per
-// touched bin reserves the slice's run in that bin; the events are placed in a
-// shared staging buffer sorted by bin and written out run by run (coalesced).
-// An event past its bin's capacity goes to J with a float2 atomic instead, so
-// any activity level gives the right sums.
+// thread, coalesced index/weight loads).  Bins within a window of kBinWin bins
+// around the round's own neurons (the neuron's region and its neighbours: most
+// synapses stay inside the region) are staged: shared-memory atomics rank every
+// event inside its bin, a CTA-wide scan of the window's counts gives each bin its
+// run in a shared staging buffer, one global atomic per bin reserves the run in
+// the bin, and the runs are written out coalesced.  Events outside the window, or
+// past their bin's capacity, go to J with a float2 atomic.
 constexpr int kBinThreads = 256;
 constexpr int kBinEPT = 8;                                  // events per thread and slice
 constexpr int kBinSlice = kBinThreads * kBinEPT;            // 2048
-constexpr int kBinMaxWords = 64;                            // bitmask words per round
-constexpr int kBinMaxRows = kBinMaxWords * 32;              // 2048 rows per round
+constexpr int kBinMaxWords = 256;                           // bitmask words per round (one per thread)
+constexpr int kBinMaxRows = 2048;                           // firing rows listed at once (a sub-round)
+constexpr int kBinWin = 1024;                               // bins staged per round
+constexpr int kBinWinPerThread = kBinWin / kBinThreads;
 constexpr uint32_t kBinSkip = 0xffffffffu;
 
-// Dynamic shared memory of k_bin_scatter (all offsets multiples of 16).
-struct BinSmemLayout {
-    size_t w, e0, off, dst, tg, cnt, tbin, tl, idx, total;
-};
-__host__ __device__ inline BinSmemLayout bin_smem_layout(int64_t n_bins)
-{
-    BinSmemLayout L;
-    size_t o = 0;
-    auto take = [&](size_t bytes) { const size_t at = o; o += (bytes + 15) & ~(size_t)15; return at; };
-    L.w = take(sizeof(float2) * kBinSlice);
-    L.e0 = take(sizeof(int64_t) * kBinMaxRows);
-    L.off = take(sizeof(int32_t) * (kBinMaxRows + 1));
-    L.dst = take(sizeof(uint32_t) * kBinSlice);
-    L.tg = take(sizeof(uint32_t) * kBinSlice);
-    L.cnt = take(sizeof(uint32_t) * (size_t)((n_bins + 1) / 2));
-    L.tbin = take(sizeof(uint16_t) * kBinSlice);
-    L.tl = take(sizeof(uint16_t) * kBinSlice);
-    L.idx = take(sizeof(uint16_t) * kBinSlice);
-    L.total = o;
-    return L;
-}
+// Dynamic shared memory of k_bin_scatter (offsets multiples of 16).
+constexpr int kBinOffW = 0;                                               // float2 [kBinSlice]
+constexpr int kBinOffE0 = kBinOffW + 8 * kBinSlice;                       // u32 [kBinMaxRows], rel. to the round's first row
+constexpr int kBinOffRow = kBinOffE0 + 4 * kBinMaxRows;                   // i32 [kBinMaxRows + 1]
+constexpr int kBinOffDst = kBinOffRow + ((4 * (kBinMaxRows + 1) + 15) & ~15);   // u32 [kBinSlice]
+constexpr int kBinOffCnt = kBinOffDst + 4 * kBinSlice;                    // u32 [kBinWin] counts, then run offsets
+constexpr int kBinOffG = kBinOffCnt + 4 * kBinWin;                        // u32 [kBinWin] run position in the bin
+constexpr int kBinOffIdx = kBinOffG + 4 * kBinWin;                        // u16 [kBinSlice]
+constexpr int kBinSmem = kBinOffIdx + 2 * kBinSlice;                      // 53264 bytes: four CTAs per SM
 
 // Exclusive prefix sum over the CTA (kBinThreads threads); *total gets the sum.
 __device__ __forceinline__ int bin_block_scan(int v, int* sh_warp, int* total)
@@ -1206,23 +1209,18 @@ __device__ __forceinline__ int bin_block_scan(int v, int* sh_warp, int* total)
     return r;
 }
 
-__global__ void __launch_bounds__(kBinThreads, 2) k_bin_scatter(DevState s, int wpr)
+__global__ void __launch_bounds__(kBinThreads, 4) k_bin_scatter(DevState s, int wpr)
 {
     extern __shared__ __align__(16) unsigned char bsm[];
     __shared__ int sh_warp[kBinThreads / 32 + 1];
-    __shared__ int sh_nt;
-    const BinSmemLayout L = bin_smem_layout(s.n_bins);
-    float2* st_w = reinterpret_cast<float2*>(bsm + L.w);
-    int64_t* row_e0 = reinterpret_cast<int64_t*>(bsm + L.e0);
-    int32_t* row_off = reinterpret_cast<int32_t*>(bsm + L.off);
-    uint32_t* st_dst = reinterpret_cast<uint32_t*>(bsm + L.dst);
-    uint32_t* row_pre = st_dst;                                   // listing only (before the slices)
-    uint32_t* t_g = reinterpret_cast<uint32_t*>(bsm + L.tg);
-    uint32_t* cnt32 = reinterpret_cast<uint32_t*>(bsm + L.cnt);   // two 16-bit counters per word
-    uint16_t* cnt16 = reinterpret_cast<uint16_t*>(bsm + L.cnt);
-    uint16_t* t_bin = reinterpret_cast<uint16_t*>(bsm + L.tbin);
-    uint16_t* t_l = reinterpret_cast<uint16_t*>(bsm + L.tl);
-    uint16_t* st_idx = reinterpret_cast<uint16_t*>(bsm + L.idx);
+    float2* st_w = reinterpret_cast<float2*>(bsm + kBinOffW);
+    uint32_t* row_e0 = reinterpret_cast<uint32_t*>(bsm + kBinOffE0);
+    int32_t* row_off = reinterpret_cast<int32_t*>(bsm + kBinOffRow);
+    uint32_t* st_dst = reinterpret_cast<uint32_t*>(bsm + kBinOffDst);
+    uint32_t* row_pre = st_dst;                                    // listing only (before the slices)
+    uint32_t* w_cnt = reinterpret_cast<uint32_t*>(bsm + kBinOffCnt);
+    uint32_t* w_g = reinterpret_cast<uint32_t*>(bsm + kBinOffG);
+    uint16_t* st_idx = reinterpret_cast<uint16_t*>(bsm + kBinOffIdx);
 
     const int tid = threadIdx.x;
     const unsigned long long steps_done = s.ctl->steps_done;
@@ -1232,22 +1230,42 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_scatter(DevState s, int 
     const uint32_t cap = s.bin_cap;
     const int64_t n_rounds = (s.n_words + wpr - 1) / wpr;
 
-    for (int64_t i = tid; i < (s.n_bins + 1) / 2; i += kBinThreads) cnt32[i] = 0u;
-    if (tid == 0) sh_nt = 0;
+#pragma unroll
+    for (int q = 0; q < kBinWinPerThread; ++q) w_cnt[tid * kBinWinPerThread + q] = 0u;
     __syncthreads();
 
     for (int64_t r = blockIdx.x; r < n_rounds; r += gridDim.x) {
-        // ---- the round's firing rows, in neuron order
-        const int64_t w0 = r * wpr;
-        uint32_t word = (tid < wpr && w0 + tid < s.n_words) ? __ldcs(bits + w0 + tid) : 0u;
-        int nrows;
-        int pos = bin_block_scan(__popc(word), sh_warp, &nrows);
-        while (word) {
-            const int b = __ffs(word) - 1;
-            word &= word - 1u;
-            row_pre[pos++] = (uint32_t)((w0 + tid) * 32 + b);
+        // ---- the round's firing rows in neuron order, listed in sub-rounds of at most
+        //      kBinMaxRows rows (a prefix of the remaining words: at most 32 rows per word);
+        //      the window of staged bins around them
+        const int64_t rw0 = r * wpr;
+        const uint32_t word_all = (tid < wpr && rw0 + tid < s.n_words) ? __ldcs(bits + rw0 + tid) : 0u;
+        for (int wstart = 0; wstart < wpr;) {
+        const int64_t w0 = rw0 + wstart;
+        const int64_t n0 = w0 * 32 < s.N ? w0 * 32 : s.N;
+        int64_t wb = (n0 >> B) - kBinWin / 2;
+        if (wb > s.n_bins - kBinWin) wb = s.n_bins - kBinWin;
+        if (wb < 0) wb = 0;
+        const int64_t e_base = __ldg(s.qrow + n0);
+        const bool mine_w = tid >= wstart && tid < wpr;
+        const int cw = mine_w ? __popc(word_all) : 0;
+        int all_rows;
+        const int excl = bin_block_scan(cw, sh_warp, &all_rows);
+        const bool take = mine_w && excl + cw <= kBinMaxRows;
+        const int wend = wstart + __syncthreads_count(take);
+        if (take) {
+            uint32_t word = word_all;
+            int pos = excl;
+            while (word) {
+                const int b = __ffs(word) - 1;
+                word &= word - 1u;
+                row_pre[pos++] = (uint32_t)((rw0 + tid) * 32 + b);
+            }
         }
+        (void)all_rows;
+        if (take && tid == wend - 1) sh_warp[kBinThreads / 32] = excl + cw;   // rows of this sub-round
         __syncthreads();
+        const int nrows = sh_warp[kBinThreads / 32];
         int len[kBinMaxRows / kBinThreads];
         int mine = 0;
 #pragma unroll
@@ -1258,7 +1276,7 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_scatter(DevState s, int 
                 const uint32_t pre = row_pre[i];
                 const int64_t e0 = __ldg(s.qrow + pre);
                 len[q] = (int)(__ldg(s.qrow + pre + 1) - e0);
-                row_e0[i] = e0;
+                row_e0[i] = (uint32_t)(e0 - e_base);
                 mine += len[q];
             }
         }
@@ -1286,39 +1304,42 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_scatter(DevState s, int 
                         const int mid = (lo + hi) >> 1;
                         if (row_off[mid] <= v) lo = mid; else hi = mid;
                     }
-                    const int64_t e = row_e0[lo] + (v - row_off[lo]);
+                    const int64_t e = e_base + (int64_t)row_e0[lo] + (v - row_off[lo]);
                     c[u] = __ldcs(s.qcol + e);
                     w[u] = __ldcs(s.qw + e);
                 }
             }
-            // rank of every event inside its bin; first event of a bin lists the bin
+            // rank every event inside its window bin; events outside the window go to J now
 #pragma unroll
             for (int u = 0; u < kBinEPT; ++u) {
                 rk[u] = 0u;
-                if (c[u] != kBinSkip) {
-                    const uint32_t bin = (c[u] & kIndexMask) >> B;
-                    const uint32_t sh = (bin & 1u) << 4;
-                    rk[u] = (atomicAdd(cnt32 + (bin >> 1), 1u << sh) >> sh) & 0xffffu;
-                    if (rk[u] == 0u) t_bin[atomicAdd(&sh_nt, 1)] = (uint16_t)bin;
+                if (c[u] == kBinSkip) continue;
+                const uint32_t post = c[u] & kIndexMask;
+                const int64_t wi = (int64_t)(post >> B) - wb;
+                if (wi >= 0 && wi < kBinWin) {
+                    rk[u] = atomicAdd(w_cnt + wi, 1u);
+                } else {
+                    atomicAdd(s.J2 + (int64_t)(c[u] >> 31) * s.j_ps + (int64_t)post * s.j_es, w[u]);
+                    c[u] = kBinSkip;
                 }
             }
             __syncthreads();
-            const int nt = sh_nt;
-            // per touched bin (contiguous ranges per thread): staging offset and the run reserved in the bin
-            const int per = (nt + kBinThreads - 1) / kBinThreads;
-            const int k0 = tid * per < nt ? tid * per : nt;
-            const int k1 = k0 + per < nt ? k0 + per : nt;
+            // window bins: run offsets in the staging buffer (scan) and runs reserved in the bins
+            uint32_t cn[kBinWinPerThread];
             int sum = 0;
-            for (int k = k0; k < k1; ++k) sum += cnt16[t_bin[k]];
+#pragma unroll
+            for (int q = 0; q < kBinWinPerThread; ++q) { cn[q] = w_cnt[tid * kBinWinPerThread + q]; sum += (int)cn[q]; }
             int tot;
             int lo = bin_block_scan(sum, sh_warp, &tot);
-            for (int k = k0; k < k1; ++k) {
-                const uint32_t bin = t_bin[k];
-                const uint32_t cn = cnt16[bin];
-                t_l[k] = (uint16_t)lo;
-                lo += (int)cn;
-                t_g[k] = atomicAdd(s.bin_cnt + bin, cn);
-                cnt16[bin] = (uint16_t)k;   // from here on: the bin's touched index
+            uint32_t g[kBinWinPerThread];
+#pragma unroll
+            for (int q = 0; q < kBinWinPerThread; ++q)
+                g[q] = cn[q] ? atomicAdd(s.bin_cnt + wb + tid * kBinWinPerThread + q, cn[q]) : 0u;
+#pragma unroll
+            for (int q = 0; q < kBinWinPerThread; ++q) {
+                w_cnt[tid * kBinWinPerThread + q] = (uint32_t)lo;
+                w_g[tid * kBinWinPerThread + q] = g[q];
+                lo += (int)cn[q];
             }
             __syncthreads();
 #pragma unroll
@@ -1326,11 +1347,11 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_scatter(DevState s, int 
                 if (c[u] == kBinSkip) continue;
                 const uint32_t post = c[u] & kIndexMask;
                 const uint32_t bin = post >> B;
-                const uint32_t k = cnt16[bin];
-                const uint32_t lp = (uint32_t)t_l[k] + rk[u];
-                const uint32_t g = t_g[k] + rk[u];
-                if (g < cap) {
-                    st_dst[lp] = bin * cap + g;
+                const int wi = (int)((int64_t)bin - wb);
+                const uint32_t lp = w_cnt[wi] + rk[u];
+                const uint32_t gp = w_g[wi] + rk[u];
+                if (gp < cap) {
+                    st_dst[lp] = bin * cap + gp;
                     st_w[lp] = w[u];
                     st_idx[lp] = (uint16_t)((post & lmask) | ((c[u] >> 31) << 15));
                 } else {   // bin full: straight into J
@@ -1339,17 +1360,18 @@ __global__ void __launch_bounds__(kBinThreads, 2) k_bin_scatter(DevState s, int 
                 }
             }
             __syncthreads();
-            const int n_slice = T - v0 < kBinSlice ? T - v0 : kBinSlice;
-            for (int i = tid; i < n_slice; i += kBinThreads) {
+            for (int i = tid; i < tot; i += kBinThreads) {
                 const uint32_t d = st_dst[i];
                 if (d != kBinSkip) {
                     s.bin_idx[d] = st_idx[i];
                     s.bin_w[d] = st_w[i];
                 }
             }
-            for (int k = tid; k < nt; k += kBinThreads) cnt16[t_bin[k]] = 0;
-            if (tid == 0) sh_nt = 0;
+#pragma unroll
+            for (int q = 0; q < kBinWinPerThread; ++q) w_cnt[tid * kBinWinPerThread + q] = 0u;
             __syncthreads();
+        }
+        wstart = wend;
         }
     }
 }

@@ -246,10 +246,10 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          neurons) and its bins could be allocated; default 1,
  *                          dtb_block_autotune keeps the faster of 1 and 2
  * DTB_TUNE_BIN_WORDS       binned push: bitmask words (32 neurons each) whose
- *                          firing rows one scatter CTA takes per round (1..64)
+ *                          firing rows one scatter CTA takes per round (1..256)
  * DTB_TUNE_BIN_CAPACITY    binned push: bin entries per neuron of the bin
  *                          (1..1024, default 8; 10 bytes each); reallocates
- * DTB_TUNE_BIN_SHIFT       binned push: B (10..13), 0 = chosen from N; reallocates */
+ * DTB_TUNE_BIN_SHIFT       binned push: B (10..13), 0 = chosen from N (11 from 8M neurons, else 10); reallocates */
 enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,
        DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5, DTB_TUNE_J_CACHE = 6, DTB_TUNE_SCATTER_VARIANT = 7,
        DTB_TUNE_PUSH_METHOD = 8, DTB_TUNE_BIN_WORDS = 9, DTB_TUNE_BIN_CAPACITY = 10, DTB_TUNE_BIN_SHIFT = 11 };
@@ -257,7 +257,7 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value);
 int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value);
 
 /* Autotuner: times the step kernel's register budgets, the atomic push scatter at 1, 2, 4, ..., 32 bitmask words
- * per warp, the binned push at 16, 32 and 64 words per round (unless DTB_TUNE_PUSH_METHOD is 1) and the pull
+ * per warp, the binned push at 64, 128 and 256 words per round (unless DTB_TUNE_PUSH_METHOD is 1) and the pull
  * gather on the live network (n_steps each; the simulation advances), keeps the fastest push method and shape
  * (DTB_TUNE_PUSH_METHOD becomes 1 or 2) and sets the
  * AUTO push/pull threshold from the measured costs at the current activity.

@@ -35,7 +35,7 @@ def _binned(spec, tune=None):
     return net
 
 
-@pytest.mark.parametrize("words", [1, 16, 64])
+@pytest.mark.parametrize("words", [1, 64, 256])
 @pytest.mark.parametrize("shift", [10, 11, 13])
 def test_binned_step_equals_pull_step_from_same_state(shift, words):
     """One binned push step from identical state vs the exact pull step, 60 times (past the
