@@ -246,6 +246,14 @@ static int ensure_pinned(dtb_block* b, size_t bytes)
 
 static inline unsigned grid_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+// ctl->events <- the sum of the per-warp event counters (before the host reads it).
+static int sum_events(dtb_block* b)
+{
+    k_sum_events<<<1, kEvParts, 0, b->stream>>>(b->ds.ev_part, b->ds.ctl);
+    CK(cudaGetLastError());
+    return DTB_OK;
+}
+
 static int copy_out(dtb_block* b, void* dst, const void* dsrc, size_t bytes, int where)
 {
     if (bytes == 0) return DTB_OK;
@@ -327,6 +335,7 @@ static int alloc_state(dtb_block* b)
     for (int p = 0; p < 2; ++p) RET(dalloc(b, &s.bits[p], (size_t)s.n_words));
     RET(dalloc(b, &s.abits, (size_t)s.n_words));
     RET(dalloc(b, &s.ctl, 1));
+    RET(dalloc(b, &s.ev_part, kEvParts));
     RET(dalloc(b, &s.unmapped_nact, 1));
     RET(dalloc(b, &b->d_err, 4));
     CK(cudaMemsetAsync(s.J2, 0, sizeof(float2) * 2 * (size_t)jps, b->stream));
@@ -334,6 +343,7 @@ static int alloc_state(dtb_block* b)
     for (int p = 0; p < 2; ++p) CK(cudaMemsetAsync(s.bits[p], 0, sizeof(uint32_t) * (size_t)s.n_words, b->stream));
     CK(cudaMemsetAsync(s.abits, 0, sizeof(uint32_t) * (size_t)s.n_words, b->stream));
     CK(cudaMemsetAsync(s.ctl, 0, sizeof(Ctl), b->stream));
+    CK(cudaMemsetAsync(s.ev_part, 0, sizeof(unsigned long long) * kEvParts, b->stream));
     CK(cudaMemsetAsync(s.unmapped_nact, 0, sizeof(uint32_t), b->stream));
     s.seed = b->seed;
     s.stream_id = b->stream_id;
@@ -1626,6 +1636,7 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
     RET(ensure_stats(b, (uint32_t)n_steps));
     RET(set_run_params(b, noise_rate, isolated));
     unsigned long long ev0 = 0, ev1 = 0;
+    RET(sum_events(b));
     CK(cudaStreamSynchronize(b->stream));
     CK(cudaMemcpy(&ev0, &b->ds.ctl->events, 8, cudaMemcpyDeviceToHost));
     const int n_ev = 4 * n_steps + 4;
@@ -1688,6 +1699,8 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
     for (auto& x : ev) cudaEventDestroy(x);
     if (rc != DTB_OK) return rc;
     if (e != cudaSuccess) return fail(DTB_ERR_CUDA, "event timing: %s", cudaGetErrorString(e));
+    RET(sum_events(b));
+    CK(cudaStreamSynchronize(b->stream));
     CK(cudaMemcpy(&ev1, &b->ds.ctl->events, 8, cudaMemcpyDeviceToHost));
     out_ms[0] = cnt[0] ? (float)(sum[0] / cnt[0]) : 0.0f;
     out_ms[1] = cnt[1] ? (float)(sum[1] / cnt[1]) : 0.0f;
@@ -1966,7 +1979,9 @@ int dtb_block_get(dtb_block* b, int field, void* dst, int where)
         if (where == DTB_HOST) { std::memcpy(dst, &b->steps, sizeof(uint64_t)); return DTB_OK; }
         return copy_out(b, dst, &s.ctl->steps_done, sizeof(uint64_t), where);
     }
-    case DTB_FIELD_EVENTS: return copy_out(b, dst, &s.ctl->events, sizeof(unsigned long long), where);
+    case DTB_FIELD_EVENTS:
+        RET(sum_events(b));
+        return copy_out(b, dst, &s.ctl->events, sizeof(unsigned long long), where);
     case DTB_FIELD_WINDOW_SPIKES:
         return copy_out(b, dst, s.win_spk, sizeof(unsigned long long) * (size_t)b->n_sub, where);
     case DTB_FIELD_G_FACTOR:

@@ -33,6 +33,7 @@ constexpr int kMaskWords = 4;          // position-mask words per kind: in-degre
 constexpr int kMaskList = 256;         // marked entries a warp gathers together per tile
 constexpr uint32_t kMixedTile = 0xffffffffu;   // tile_cls of a tile whose neurons have different classes
 constexpr int kStepThreads = 256;      // 8 warps, 1024 neurons per CTA
+constexpr int kEvParts = 1024;         // event counters: many warps add at once, one address would serialise
 
 // One deduplicated row of the 22-column property matrix
 // (generation/make_block.py:394-432) with the derived constants the step uses.
@@ -156,6 +157,8 @@ struct DevState {
     float* st_mean;             // [stats_cap][n_sub]
     uint32_t* st_nact;          // [stats_cap]
     Ctl* ctl;
+    unsigned long long* ev_part;   // [kEvParts] synaptic event counters (summed into ctl->events on demand;
+                                   // nullable: then the kernels add to ctl->events)
     uint64_t seed;
     uint32_t stream_id;
     float dt;

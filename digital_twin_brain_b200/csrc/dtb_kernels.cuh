@@ -85,6 +85,14 @@ __device__ __forceinline__ void store_J(const DevState& s, int64_t n, float4 J)
     }
 }
 
+// Synaptic events propagated by a warp or CTA, into one of kEvParts counters.
+__device__ __forceinline__ void add_events(const DevState& s, unsigned long long ev, uint32_t key)
+{
+    if (!ev) return;
+    if (s.ev_part) atomicAdd(s.ev_part + (key & (kEvParts - 1)), ev);
+    else atomicAdd(&s.ctl->events, ev);
+}
+
 __device__ __forceinline__ bool test_bit(const uint32_t* __restrict__ bits, int64_t n)
 {
     return (__ldg(bits + (n >> 5)) >> (n & 31)) & 1u;
@@ -751,7 +759,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 }
             }
             __syncwarp();
-            if (!s.qrow) acc_ev += events;
+            acc_ev += events;   // synaptic events of the step gathered
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int64_t n = base + j * 32 + lane;
@@ -794,7 +802,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                     if (lane == r) sum[j] = a;
                 }
             }
-            if (!s.qrow) acc_ev += events;   // no push rows to count from in the update
+            acc_ev += events;   // synaptic events of the step gathered
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int64_t n = base + j * 32 + lane;
@@ -877,7 +885,6 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         int mysub0 = -1;
         bool lane_uni = true;               // all of this lane's valid neurons in mysub0
         double vsum_lane = 0.0;
-        uint32_t ev_lane = 0;
         auto neuron = [&](int j, const ParamClass& p) {
             const int64_t n = base + j * 32 + lane;
             float v, tl;
@@ -914,8 +921,6 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             __stcs(s.V + n, vmin);
             store_J(s, n, mul4(J, p.decay));
             if (a) s.tlast[n] = t;
-            // synaptic events of this step: out-degree of every propagating neuron
-            if (na && s.qrow) ev_lane += (uint32_t)(__ldg(s.qrow + n + 1) - __ldg(s.qrow + n));
             act_m |= (uint32_t)a << j;
             nav_m |= (uint32_t)na << j;
             if (j == 0) mysub0 = p.sub;
@@ -940,7 +945,6 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             for (int j = 0; j < 4; ++j)
                 if (valid[j]) neuron(j, load_class(s.pc, c_in[j]));
         }
-        acc_ev += (unsigned long long)__reduce_add_sync(0xffffffffu, ev_lane);
 
         uint32_t cnt_spk = 0, cnt_nact = 0;
 #pragma unroll
@@ -1008,7 +1012,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             cs += sh_spk[w]; cn += sh_nact[w]; cv += sh_vsum[w];
         }
         if (cur >= 0) { atomicAdd(s.sub_spk + cur, cs); atomicAdd(s.sub_nact + cur, cn); atomicAdd(s.sub_vsum + cur, cv); }
-        if (ev) atomicAdd(&s.ctl->events, ev);
+        add_events(s, ev, blockIdx.x);
         if (UPDATE) {
             __threadfence();   // the CTA's statistics before its done-count
             const unsigned prev = atomicAdd(&s.ctl->done, 1u);
@@ -1034,7 +1038,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
 // read with evict-first hints so it does not push the J lines out of L2; a
 // small `wpw` keeps the rows scattered at any moment inside a narrow window
 // of neurons, whose intra-region targets then share L2-resident J lines.  No
-// CTA-wide barrier: the events are counted by the update kernel.
+// CTA-wide barrier; the synaptic events (row lengths) are counted per warp.
 constexpr int kScatterThreads = 256;
 constexpr int kScatterMaxWords = 32;
 
@@ -1071,6 +1075,7 @@ __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, i
         rows[pos++] = (uint32_t)((w0 + lane) * 32 + b);
     }
     __syncwarp();
+    unsigned long long warp_events = 0;
     for (int r0 = 0; r0 < total; r0 += 32) {
         const bool has = r0 + lane < total;
         int64_t e0 = 0, len = 0;
@@ -1087,6 +1092,7 @@ __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, i
             if (lane >= o) off += y;
         }
         const int64_t T = __shfl_sync(0xffffffffu, off, 31);
+        warp_events += (unsigned long long)T;
         const int64_t start = off - len;           // exclusive offset of this lane's row
         for (int64_t v0 = 0; v0 < T; v0 += 32 * kScatterUnroll) {
             uint32_t c[kScatterUnroll];
@@ -1141,6 +1147,7 @@ __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, i
             }
         }
     }
+    if (lane == 0) add_events(s, warp_events, (uint32_t)warp_global);
 }
 
 // ------------------------------------------------------------ binned push scatter
@@ -1229,6 +1236,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_scatter(DevState s, int 
     const uint32_t lmask = (1u << B) - 1u;
     const uint32_t cap = s.bin_cap;
     const int64_t n_rounds = (s.n_words + wpr - 1) / wpr;
+    unsigned long long cta_events = 0;
 
 #pragma unroll
     for (int q = 0; q < kBinWinPerThread; ++q) w_cnt[tid * kBinWinPerThread + q] = 0u;
@@ -1288,6 +1296,7 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_scatter(DevState s, int 
             if (i < nrows) { row_off[i] = ex; ex += len[q]; }
         }
         if (tid == 0) row_off[nrows] = T;
+        cta_events += (unsigned long long)T;
         __syncthreads();
 
         // ---- slices of kBinSlice events
@@ -1374,9 +1383,27 @@ __global__ void __launch_bounds__(kBinThreads, 4) k_bin_scatter(DevState s, int 
         wstart = wend;
         }
     }
+    if (tid == 0) add_events(s, cta_events, blockIdx.x);
 }
 
 // ------------------------------------------------------------ exports
+
+// ctl->events = the sum of the event counters (one CTA of kEvParts threads).
+__global__ void __launch_bounds__(kEvParts) k_sum_events(const unsigned long long* __restrict__ part, Ctl* ctl)
+{
+    __shared__ unsigned long long sh[kEvParts / 32];
+    unsigned long long v = part[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = sh[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) ctl->events = v;
+    }
+}
 
 __global__ void k_export_J(const DevState s, float* __restrict__ out)
 {

@@ -130,3 +130,26 @@ def test_autotune_chooses_a_push_method():
     pm = net.get_tuning(TUNE_PUSH_METHOD)
     assert pm in (ATOMIC, BINNED) and r["push_ms"] > 0
     net.run(10, mode="push")
+
+
+@pytest.mark.parametrize("how", ["atomic", "binned", "rows", "slots", "masks", "stream"])
+def test_synaptic_event_count_every_method(how):
+    """FIELD_EVENTS advances by the out-degree sum of every neuron that propagated (spike | noise),
+    whichever kernel propagates (the scatters count the rows they push, the gathers the entries
+    they add)."""
+    from digital_twin_brain_b200._lib import FIELD_EVENTS, FIELD_NEW_ACTIVE, TUNE_PULL_METHOD
+    spec = synthetic.whole_brain(R=3, mean_size=2000, sigma=0.3, K=40, gen_seed=6, name="wb3_ev")
+    net = Network.from_spec(spec, device=0)
+    mode = "push" if how in ("atomic", "binned") else "pull"
+    if how == "binned":
+        net.set_tuning(TUNE_PUSH_METHOD, BINNED)
+    elif mode == "pull":
+        net.set_tuning(TUNE_PULL_METHOD, {"rows": 1, "slots": 2, "masks": 3, "stream": 4}[how])
+    qrp = net.get_csr_rowptr("push")
+    outdeg = np.diff(qrp)
+    for n in (1, 3, 40):
+        for _ in range(n):
+            e0 = net.get(FIELD_EVENTS)
+            net.run(1, noise_rate=0.03, mode=mode)
+            na = net.get(FIELD_NEW_ACTIVE).astype(bool)
+            assert net.get(FIELD_EVENTS) - e0 == int(outdeg[na].sum())
