@@ -18,6 +18,14 @@ an independent replica (the path does not shard across GPUs).
 --impl reference times the reference's algorithm on the host cores (the CPU
 oracle restating models/block.py, OpenMP) on a bounded sample of the same
 workload and prints the same line with "impl": "reference".
+
+Other workloads (--config): one_region (N=1e6, K=100; --noise sweeps the pull/push
+crossover), single_block (N=2000), ensemble (64 members of U[5e4,4e5] neurons with
+per-member g_ui, one BOLD region each) and profile_case (the whole-brain structure
+at scale 0.45 with K=20: a few GB on the device, the case the ncu captures use).
+The default whole-brain run also runs the data-assimilation comparison (surrogate-
+served vs all-simulator ensemble, digital_twin_brain_b200/da_bench.py) at a
+reduced region size and reports it under "da".
 """
 from __future__ import annotations
 
@@ -37,9 +45,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "synaptic events/s & sim-s/wall-s at 2B syn; DA window time surrogate vs plain"
 UNIT = "events/s"
-# ncu DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, one pass each) of the whole-brain
-# workload itself (profiles/whole_brain_dram_traffic.md): k_scatter<0> 1.303 GB per launch for
-# 2.346e7 events, staged update 1.014 GB per launch for 2.345e7 neurons
+# DRAM traffic per unit processed, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum)
+# of single launches: the atomic push scatter per synaptic event and the staged update per neuron.
+# The line's roofline.traffic scales these to the launch it reports and says so.
 SCATTER_DRAM_BYTES_PER_EVENT = (943.26e6 + 360.44e6) / 23462598
 UPDATE_DRAM_BYTES_PER_NEURON = (595.12e6 + 418.77e6) / 23448955
 
@@ -52,18 +60,32 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="tune", choices=["tune", "auto", "push", "pull"])
     ap.add_argument("--scale", type=float, default=1.0, help="whole-brain size scale (1.0 = ~2.2e9 synapses)")
-    ap.add_argument("--config", default="whole_brain", choices=["whole_brain", "one_region", "single_block"],
+    ap.add_argument("--config", default="whole_brain",
+                    choices=["whole_brain", "one_region", "single_block", "ensemble", "profile_case"],
                     help="whole_brain: 90 regions ~2.2e9 synapses (the headline); one_region: N=1e6, K=100; "
-                         "single_block: N=2000, K=100")
+                         "single_block: N=2000, K=100; ensemble: 64 members N~U[5e4,4e5], per-member g_ui; "
+                         "profile_case: whole-brain structure x0.45, K=20 (ncu captures)")
     ap.add_argument("--noise", type=float, default=0.01)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=400)
+    ap.add_argument("--graphs", type=int, default=1, help="0: one launch per kernel (profilers)")
+    ap.add_argument("--push-method", type=int, default=-1, help="1 atomics, 2 binned (-1: autotuned / default)")
+    ap.add_argument("--pull-method", type=int, default=-1, help="1 rows, 2 slots, 3 masks, 4 streamed (-1: auto)")
+    ap.add_argument("--step-variant", type=int, default=-1, help="update kernel variant 0..4 (-1: autotuned)")
+    ap.add_argument("--scatter-words", type=int, default=0, help="atomic scatter bitmask words per warp (0: tuned)")
+    ap.add_argument("--da", type=int, default=-1,
+                    help="1: run the data-assimilation comparison (default: on for the whole-brain line)")
+    ap.add_argument("--da-region-size", type=float, default=250)
+    ap.add_argument("--da-windows", type=int, default=24)
+    ap.add_argument("--da-members", type=int, default=128)
+    ap.add_argument("--da-train-windows", type=int, default=20)
     return ap.parse_args()
 
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms, from the kernel timing through
+    the timed region to the end-to-end run."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -93,7 +115,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-i", self.gpu, "-lms", "200"], stdout=subprocess.PIPE,
+                                          "-i", self.gpu, "-lms", "50"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -199,93 +221,52 @@ def run_reference(args, rank: int, world: int):
 
 
 # ---------------------------------------------------------------- our arm
-def run_ours(args, rank: int, world: int, local_rank: int):
-    import torch
-    import torch.distributed as dist
-    from digital_twin_brain_b200 import Network, synthetic
-    from digital_twin_brain_b200._lib import TUNE_PULL_METHOD
-
-    dev = local_rank
-    torch.cuda.set_device(dev)
+def build_spec(args, rank: int):
+    from digital_twin_brain_b200 import synthetic
     if args.config == "one_region":
         spec = synthetic.config_one_region(args.noise)
     elif args.config == "single_block":
         spec = synthetic.config_single_block()
+    elif args.config == "ensemble":
+        spec = synthetic.config_ensemble(scale=args.scale)
+    elif args.config == "profile_case":
+        spec = synthetic.whole_brain(K=20, scale=0.45, name="profile_case_wb90_x0.45_K20")
     else:
         spec = synthetic.config_whole_brain(args.scale) if args.scale != 1.0 else synthetic.config_whole_brain()
     spec.seed = 1000 + rank              # independent replica noise per rank
     spec.extra["noise"] = args.noise
-    t_build = time.perf_counter()
-    net = Network.from_spec(spec, device=dev, build_push=True)
-    net.attach_bold(spec.sub_to_region(), spec.R, delta_t=spec.dt / 1000.0)
-    stream = torch.cuda.Stream(device=dev)
-    net.set_stream(stream)
-    torch.cuda.synchronize(dev)
-    t_build = time.perf_counter() - t_build
-    info = net.info()
+    return spec
 
-    # warm-up (also passes the initial refractory period) and method choice
-    W = max(args.warmup, 3)
-    net.run(W, noise_rate=args.noise, mode="auto", out=None)
-    tune = {}
-    if args.mode == "tune":
-        tune = net.autotune(32, noise_rate=args.noise)
-        mode = "push" if tune["push_ms"] <= tune["pull_ms"] else "pull"
-    else:
-        mode = args.mode
-    kt = net.time_kernels(64, noise_rate=args.noise, mode=mode)
-    torch.cuda.synchronize(dev)
 
-    # ---- timed region: exactly K steps on the device
-    K = args.steps
-    ev0 = net.get(10)  # FIELD_EVENTS
-    l0 = net.info().kernel_launches
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    with ClockSampler(dev) as clk:
-        start.record(stream)
-        net.run(K, noise_rate=args.noise, mode=mode, out=None)
-        end.record(stream)
-        torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
-    ms = start.elapsed_time(end)
-    events = net.get(10) - ev0
-    launches = net.info().kernel_launches - l0
-    ms_max, events_all = combine_over_ranks(ms, float(events), world, f"cuda:{dev}")
-    value = events_all / (ms_max / 1000.0)
-    sim_ratio = K * spec.dt / 1000.0 / (ms_max / 1000.0)
+def describe(spec, args) -> str:
+    N, S = spec.N, spec.S
+    if args.config == "ensemble":
+        sizes = spec.extra["member_sizes"]
+        return (f"{spec.name}: {len(sizes)} members of N~U[5e4,4e5] x{args.scale} ({min(sizes)}..{max(sizes)}), "
+                f"N={N}, S={S}, K={spec.K}, per-member g_ui x U[0.5,1.5], dt=0.1 ms, noise p={args.noise}, "
+                f"fp32 weights, BOLD per member")
+    if args.config in ("one_region", "single_block"):
+        return f"{spec.name}: one region, N={N}, S={S}, K={spec.K}, 80/20 E/I, dt=0.1 ms, noise p={args.noise}, fp32 weights"
+    sc = " x0.45" if args.config == "profile_case" else (f" x{args.scale}" if args.scale != 1.0 else "")
+    return (f"{spec.name}: {spec.R} regions lognormal(ln 2.2e5, 0.5){sc}, N={N}, S={S}, K={spec.K}, "
+            f"80% intra-region, dt=0.1 ms, noise p={args.noise}, fp32 weights, BOLD per region")
 
-    # ---- end to end through the public API: per step, host->device run parameters and the
-    #      per-subblock results (spike sums, mean V, propagated count) back to host memory
-    E = min(args.e2e_steps, K)
-    ev_a = net.get(10)
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    for _ in range(E):
-        net.run(1, noise_rate=args.noise, mode=mode, out="host")
-    t_e2e = time.perf_counter() - t0
-    ev_e2e = net.get(10) - ev_a
-    # whole job at N replicas: the events of all ranks over the slowest rank's time
-    e2e_ms, ev_e2e = combine_over_ranks(1000.0 * t_e2e, float(ev_e2e), world, f"cuda:{dev}")
-    t_e2e = e2e_ms / 1000.0
-    e2e_value = ev_e2e / t_e2e
-    h2d = 16                                  # run parameters (base step, noise rate, isolated)
-    d2h = 2 * 4 * net.n_sub + 4               # spike sums + mean V per subblock + propagated count
 
-    # ---- roofline of the dominant kernel
+def roofline_of(spec, kt, mode, push_method, pull_method, peaks):
+    """Algorithmic bytes of every kernel of the step (per launch) and the dominant kernel's roofline."""
     N, S = spec.N, spec.S
     evs = kt["events_per_step"]
     nact = evs / spec.K
     # V, J, t_last read, one class id per 128-neuron tile; V, J written; two bitmasks
     upd_bytes = N * (4 + 16 + 4 + 4 / 128) + N * (4 + 16) + 2 * N / 8
     prop_bytes = N / 8 + 16 * nact + 12 * evs                              # bitmask, row pointers, (post, w) of rows
-    ordered = mode == "pull" and net.get_tuning(TUNE_PULL_METHOD) != 1 and kt["propagate_ms"] > 0 and \
-        nact / N <= 0.1
-    if mode == "push":
+    ordered = mode == "pull" and pull_method != 1 and kt["propagate_ms"] > 0 and nact / N <= 0.1
+    if mode == "push" and push_method == 2:
+        # binned: the scatter also writes every event into its bin (u16 index + weight pair), the
+        # update reads them back
+        kernels = {"update+fold": (kt["update_ms"], upd_bytes + 10 * evs),
+                   "binned scatter": (kt["propagate_ms"], prop_bytes + 10 * evs)}
+    elif mode == "push":
         kernels = {"update": (kt["update_ms"], upd_bytes), "scatter": (kt["propagate_ms"], prop_bytes)}
     elif ordered:
         # ordered push: + pull-row positions, slot writes; the update reads counts and slots
@@ -296,72 +277,221 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         kernels = {"gather+update": (kt["update_ms"], fused)}
     dom = max(kernels, key=lambda k: kernels[k][0])
     d_ms, d_bytes = kernels[dom]
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = d_bytes / (d_ms * 1e-3) / 1e9 if d_ms > 0 else 0.0
+    traffic, tsrc = None, None
+    if dom == "scatter":
+        traffic = SCATTER_DRAM_BYTES_PER_EVENT * evs
+        tsrc = "ncu DRAM bytes per synaptic event of the atomic scatter, scaled to this launch's events"
+    elif dom == "update":
+        traffic = UPDATE_DRAM_BYTES_PER_NEURON * N
+        tsrc = "ncu DRAM bytes per neuron of the staged update, scaled to this launch's neurons"
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "traffic_source": tsrc, "kernel": dom, "algorithmic_bytes_per_launch": d_bytes,
+                "launch_ms": d_ms,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
+    per_kernel = {k: {"ms": v[0], "bytes": v[1], "gbs": v[1] / (v[0] * 1e-3) / 1e9 if v[0] > 0 else 0.0,
+                      "frac": (v[1] / (v[0] * 1e-3) / 1e9) / peak if v[0] > 0 else 0.0} for k, v in kernels.items()}
+    # the step against the reference layout's byte model: N*44 + S_touched*13 + N/8 per step
+    model_bytes = N * 44 + evs * 13 + N / 8
+    step = {"bytes_per_step_model": model_bytes, "ms": kt["step_ms"],
+            "achieved_gbs": model_bytes / (kt["step_ms"] * 1e-3) / 1e9 if kt["step_ms"] else 0,
+            "frac": (model_bytes / (kt["step_ms"] * 1e-3) / 1e9) / peak if kt["step_ms"] else 0,
+            "kernels": per_kernel}
+    return roofline, step
+
+
+def atomic_probe(dev, N, evs, window):
+    """float2 atomics per second on this GPU into J-sized targets (bench-only helper library)."""
+    import ctypes
+    from digital_twin_brain_b200 import build as B
+    try:
+        L = ctypes.CDLL(B.build_probe())
+        fn = L.dtb_bench_atomic_rate
+        fn.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(ctypes.c_float)]
+        fn.restype = ctypes.c_int
+        ms = ctypes.c_float()
+        if fn(dev, int(N), int(max(evs, 1)), int(max(1, window)), ctypes.byref(ms)) != 0:
+            return None
+        return ms.value
+    except Exception:
+        return None
+
+
+def run_da(args, dev):
+    """The data-assimilation comparison (metric part 3) at a reduced region size."""
+    from digital_twin_brain_b200 import da_bench
+    argv = ["--members", str(args.da_members), "--judges", str(max(1, args.da_members // 8)),
+            "--region-size", str(args.da_region_size), "--windows", str(args.da_windows),
+            "--train-windows", str(args.da_train_windows), "--plain-seeds", "1", "--skip", "4"]
+    r = da_bench.main(argv, quiet=True)
+    keys = ("members", "judges", "regions", "region_size", "neurons_per_member", "windows", "steps_per_window",
+            "plain_window_s", "surrogate_window_s", "speedup", "plain_total_s", "surrogate_total_s", "speedup_total",
+            "surrogate_served_window_s", "speedup_served_windows", "fallbacks", "plain_rmse", "surrogate_rmse",
+            "rmse_ratio", "plain_gui_rel_err", "surrogate_gui_rel_err", "train_windows", "train_samples",
+            "train_collect_s", "train_s", "heldout_logrmse_net", "heldout_logrmse_persistence", "total_s")
+    out = {k: r[k] for k in keys if k in r}
+    out["note"] = ("surrogate_total_s includes its burn-in window; train_collect_s (simulating the training "
+                   "windows) and train_s are outside both totals")
+    return out
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import torch.distributed as dist
+    from digital_twin_brain_b200 import Network
+    from digital_twin_brain_b200._lib import (TUNE_PULL_METHOD, TUNE_PUSH_METHOD, TUNE_SCATTER_WORDS,
+                                              TUNE_STEP_VARIANT, TUNE_USE_GRAPHS)
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    spec = build_spec(args, rank)
+    t_build = time.perf_counter()
+    net = Network.from_spec(spec, device=dev, build_push=True)
+    bold_regions = spec.R
+    net.attach_bold(spec.sub_to_region(), bold_regions, delta_t=spec.dt / 1000.0)
+    stream = torch.cuda.Stream(device=dev)
+    net.set_stream(stream)
+    torch.cuda.synchronize(dev)
+    t_build = time.perf_counter() - t_build
+    info = net.info()
+    if not args.graphs:
+        net.set_tuning(TUNE_USE_GRAPHS, 0)
+
+    # warm-up (also passes the initial refractory period) and method choice
+    W = max(args.warmup, 3)
+    net.run(W, noise_rate=args.noise, mode="auto", out=None)
+    tune = {}
+    if args.mode == "tune":
+        tune = net.autotune(32, noise_rate=args.noise)
+        mode = "push" if tune["push_ms"] <= tune["pull_ms"] else "pull"
+    else:
+        mode = args.mode
+    if args.push_method >= 0:
+        net.set_tuning(TUNE_PUSH_METHOD, args.push_method)
+    if args.pull_method >= 0:
+        net.set_tuning(TUNE_PULL_METHOD, args.pull_method)
+    if args.step_variant >= 0:
+        net.set_tuning(TUNE_STEP_VARIANT, args.step_variant)
+    if args.scatter_words > 0:
+        net.set_tuning(TUNE_SCATTER_WORDS, args.scatter_words)
+    push_method = net.get_tuning(TUNE_PUSH_METHOD)
+    pull_method = net.get_tuning(TUNE_PULL_METHOD)
+    torch.cuda.synchronize(dev)
+
+    clk = ClockSampler(dev)
+    clk.__enter__()
+    try:
+        kt = net.time_kernels(64, noise_rate=args.noise, mode=mode)
+        torch.cuda.synchronize(dev)
+
+        # ---- timed region: exactly K steps on the device
+        K = args.steps
+        ev0 = net.get(10)  # FIELD_EVENTS
+        l0 = net.info().kernel_launches
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        start.record(stream)
+        net.run(K, noise_rate=args.noise, mode=mode, out=None)
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        ms = start.elapsed_time(end)
+        events = net.get(10) - ev0
+        launches = net.info().kernel_launches - l0
+        ms_max, events_all = combine_over_ranks(ms, float(events), world, f"cuda:{dev}")
+        value = events_all / (ms_max / 1000.0)
+        sim_ratio = K * spec.dt / 1000.0 / (ms_max / 1000.0)
+
+        # ---- end to end through the public API: per step, host->device run parameters and the
+        #      per-subblock results (spike sums, mean V, propagated count) back to host memory
+        E = min(args.e2e_steps, K)
+        e2e = None
+        if E > 0:
+            ev_a = net.get(10)
+            torch.cuda.synchronize(dev)
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            for _ in range(E):
+                net.run(1, noise_rate=args.noise, mode=mode, out="host")
+            t_e2e = time.perf_counter() - t0
+            ev_e2e = net.get(10) - ev_a
+            # whole job at N replicas: the events of all ranks over the slowest rank's time
+            e2e_ms, ev_e2e = combine_over_ranks(1000.0 * t_e2e, float(ev_e2e), world, f"cuda:{dev}")
+            t_e2e = e2e_ms / 1000.0
+            h2d = 16                                  # run parameters (base step, noise rate, isolated)
+            d2h = 2 * 4 * net.n_sub + 4               # spike sums + mean V per subblock + propagated count
+            e2e = {"value": ev_e2e / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "steps": E, "ms_per_step": 1000.0 * t_e2e / E,
+                   "api": "Network.run(1, out='host') per step (ctypes -> dtb_block_run, DTB_HOST)"}
+    finally:
+        clk.__exit__()
+
+    # ---- roofline of the dominant kernel and of the step
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = d_bytes / (d_ms * 1e-3) / 1e9 if d_ms > 0 else 0.0
-    step_bytes = sum(b for _, b in kernels.values())
-    # DRAM bytes per launch measured by ncu on this workload, per unit processed (events, neurons)
-    traffic = None
-    if dom == "scatter":
-        traffic = SCATTER_DRAM_BYTES_PER_EVENT * evs
-    elif dom == "update":
-        traffic = UPDATE_DRAM_BYTES_PER_NEURON * N
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": dom, "algorithmic_bytes_per_launch": d_bytes, "launch_ms": d_ms,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s"}
+    roofline, step_roofline = roofline_of(spec, kt, mode, push_method, pull_method, peaks)
 
-    # the push scatter's own ceiling: float2 atomics per second on this GPU, measured live with the
-    # same count into J-sized targets, destinations inside region-sized windows
+    # the atomic push scatter's own ceiling: float2 atomics per second on this GPU, measured live with
+    # the same count into J-sized targets, destinations inside region-sized windows
     atomic = None
-    if mode == "push" and kt["propagate_ms"] > 0:
-        import ctypes
-        from digital_twin_brain_b200 import _lib
-        pm = ctypes.c_float()
-        _lib.call("dtb_measure_atomic_rate", dev, int(N), int(max(evs, 1)), int(max(1, N // spec.R)),
-                  ctypes.byref(pm))
-        peak_ops = evs / (pm.value * 1e-3) / 1e9
-        got_ops = evs / (kt["propagate_ms"] * 1e-3) / 1e9
-        atomic = {"bound": "l2_atomics", "achieved": got_ops, "peak": peak_ops, "unit": "G float2 atomics/s",
-                  "frac": got_ops / peak_ops, "kernel": "scatter",
-                  "probe": f"dtb_measure_atomic_rate(N={N}, ops={int(evs)}, window={N // spec.R})"}
+    evs = kt["events_per_step"]
+    if mode == "push" and push_method != 2 and kt["propagate_ms"] > 0 and args.config != "profile_case":
+        probe_ms = atomic_probe(dev, spec.N, evs, spec.N // spec.R)
+        if probe_ms:
+            peak_ops = evs / (probe_ms * 1e-3) / 1e9
+            got_ops = evs / (kt["propagate_ms"] * 1e-3) / 1e9
+            atomic = {"bound": "l2_atomics", "achieved": got_ops, "peak": peak_ops, "unit": "G float2 atomics/s",
+                      "frac": got_ops / peak_ops, "kernel": "scatter",
+                      "probe": f"dtb_bench_atomic_rate(N={spec.N}, ops={int(evs)}, window={spec.N // spec.R})"}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config in ("whole_brain",):
         r = cpu_sample(scale=1 / 64, noise=args.noise, seconds=15.0, max_steps=10_000)
         cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]}
 
+    da = None
+    run_da_now = args.da == 1 or (args.da < 0 and args.config == "whole_brain" and args.scale == 1.0)
+    if rank == 0 and world == 1 and run_da_now:
+        net.close()
+        net = None
+        torch.cuda.empty_cache()
+        da = run_da(args, dev)
+
     if rank == 0:
-        clocks = clk.summary()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
                 "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
-                "config": {"workload": (f"{spec.name}: {spec.R} regions"
-                                        + (f" lognormal(ln 2.2e5, 0.5) x{args.scale}" if args.config == "whole_brain" else "")
-                                        + f", N={N}, S={S}, K={spec.K}, 80% intra-region, dt=0.1 ms, "
-                                        f"noise p={args.noise}, fp32 weights, BOLD per region"),
-                           "method": mode, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                           "l2": "inputs larger than L2 (state ~1 GB, synapses ~27 GB per CSR)"},
+                "config": {"workload": describe(spec, args),
+                           "method": mode + (("/binned" if push_method == 2 else "/atomic") if mode == "push" else ""),
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                           "l2": "inputs larger than L2 (state ~1 GB, synapses ~27 GB per CSR)"
+                                 if args.config == "whole_brain" else "inputs larger than L2"},
                 "value_metric": "synaptic events/s", "sim_s_per_wall_s": sim_ratio,
                 "events_per_step": events_all / world / K, "firing": {
-                    "propagated_per_step": evs / spec.K, "propagated_frac": evs / spec.K / N},
+                    "propagated_per_step": evs / spec.K, "propagated_frac": evs / spec.K / spec.N},
                 "kernel_ms": kt, "tune": tune, "build_s": t_build, "device_gb": info.device_bytes / 1e9,
                 "gpu_launches": int(launches),
                 "roofline": roofline,
                 "atomic_roofline": atomic,
-                "step_roofline": {"bytes_per_step": step_bytes, "ms": kt["step_ms"],
-                                  "achieved_gbs": step_bytes / (kt["step_ms"] * 1e-3) / 1e9 if kt["step_ms"] else 0},
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "steps": E, "ms_per_step": 1000.0 * t_e2e / E,
-                        "api": "Network.run(1, out='host') per step (ctypes -> dtb_block_run, DTB_HOST)"},
-                "clocks": clocks}
+                "step_roofline": step_roofline,
+                "e2e": e2e,
+                "clocks": clk.summary()}
         if cpu:
             line["cpu_baseline"] = cpu
+        if da:
+            line["da"] = da
         print(json.dumps(line))
-    net.close()
+    if net is not None:
+        net.close()
 
 
 def main():

@@ -23,7 +23,8 @@ FIELD_V, FIELD_J, FIELD_I_UI, FIELD_I_SYN, FIELD_T_LAST, FIELD_ACTIVE, FIELD_NEW
     FIELD_SUB_COUNT, FIELD_EVENTS, FIELD_WINDOW_SPIKES, FIELD_G_FACTOR = range(13)
 
 TUNE_SCATTER_WORDS, TUNE_CHUNK, TUNE_PULL_THRESHOLD_PPM, TUNE_USE_GRAPHS, TUNE_STEP_VARIANT, TUNE_PULL_METHOD, \
-    TUNE_J_CACHE, TUNE_SCATTER_VARIANT, TUNE_PUSH_METHOD, TUNE_BIN_WORDS, TUNE_BIN_CAPACITY, TUNE_BIN_SHIFT = range(12)
+    TUNE_J_CACHE, TUNE_SCATTER_VARIANT, TUNE_PUSH_METHOD, TUNE_BIN_WORDS, TUNE_BIN_CAPACITY, TUNE_BIN_SHIFT, \
+    TUNE_STAGE_WAIT_LIMIT = range(13)
 
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "out of memory", 4: "I/O error", 5: "format error",
           6: "invalid state", 7: "limit exceeded"}
@@ -82,7 +83,6 @@ _SIGS = {
     "dtb_block_scale_property_by_subblock": [c_vp, c_int, c_vp, c_vp, c_vp],
     "dtb_block_gamma_property_by_subblock": [c_vp, c_int, c_vp, c_vp, c_vp, c_vp],
     "dtb_block_set_input_spikes": [c_vp, c_i64, c_vp, c_i64, c_vp],
-    "dtb_measure_atomic_rate": [c_int, c_i64, c_i64, c_i64, c_vp],
     "dtb_block_update_conn_weight": [c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
     "dtb_block_save": [c_vp, c_char_p],
     "dtb_block_load": [c_vp, c_char_p],

@@ -16,6 +16,9 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libdtb.so")
+# bench.py's measurement helper (float2 atomic rate), kept out of libdtb.so
+PROBE_LIB = os.path.join(PKG, "libdtb_bench_probe.so")
+PROBE_SOURCES = ["bench_probe.cu"]
 
 SOURCES = ["dtb_api.cu", "dtb_prealloc.cu", "dtb_mlp.cu", "dtb_io.cpp"]
 HEADERS = ["dtb_device.cuh", "dtb_kernels.cuh", "dtb_io.h"]
@@ -46,6 +49,7 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    build_probe(force)
     if not force and not _stale():
         return LIB
     cmd = [nvcc()] + NVCC_FLAGS + ["-I", INCLUDE, "-I", CSRC, "-o", LIB + ".tmp"]
@@ -56,6 +60,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
     subprocess.check_call(cmd)
     os.replace(LIB + ".tmp", LIB)
     return LIB
+
+
+def build_probe(force: bool = False) -> str:
+    """libdtb_bench_probe.so: the float2 atomic-rate probe bench.py reports beside the push scatter."""
+    srcs = [os.path.join(CSRC, f) for f in PROBE_SOURCES]
+    if not force and os.path.exists(PROBE_LIB) and all(os.path.getmtime(f) <= os.path.getmtime(PROBE_LIB)
+                                                        for f in srcs + [__file__]):
+        return PROBE_LIB
+    subprocess.check_call([nvcc()] + NVCC_FLAGS + ["-o", PROBE_LIB + ".tmp"] + srcs)
+    os.replace(PROBE_LIB + ".tmp", PROBE_LIB)
+    return PROBE_LIB
 
 
 if __name__ == "__main__":

@@ -317,6 +317,19 @@ static int build_classes(dtb_block* b, int64_t N, const float* property, const f
     return DTB_OK;
 }
 
+// ------------------------------------------------------------ input checks
+// A NaN in a property row would turn into NaN membrane potentials (models/block.py
+// computes with it unchecked); the library refuses such rows up front.  Infinite
+// values stay allowed (V_th = +inf marks neurons that never fire).
+static int check_property(int64_t N, const float* property, const char* what)
+{
+    for (int64_t i = 0; i < N; ++i)
+        for (int c = 0; c < DTB_NPROP; ++c)
+            if (std::isnan(property[i * DTB_NPROP + c]))
+                return fail(DTB_ERR_ARG, "%s: property row %lld column %d is NaN", what, (long long)i, c);
+    return DTB_OK;
+}
+
 // ------------------------------------------------------------ state setup
 static int alloc_state(dtb_block* b)
 {
@@ -348,6 +361,7 @@ static int alloc_state(dtb_block* b)
     s.seed = b->seed;
     s.stream_id = b->stream_id;
     s.dt = b->dt;
+    s.stage_wait_limit = 1u << 20;
     s.forced_active = nullptr;
     s.forced_new = nullptr;
     return DTB_OK;
@@ -1048,7 +1062,13 @@ static int emit_stats(dtb_block* b, int rows, int64_t row0, float* sum_out, floa
         uint32_t* herr = reinterpret_cast<uint32_t*>(p + ((2 * bs + bn + 7) & ~(size_t)7));
         CK(cudaMemcpyAsync(herr, &b->ds.ctl->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream));
         CK(cudaStreamSynchronize(b->stream));
-        if (*herr & kErrStageTimeout) return fail(DTB_ERR_CUDA, "a staged state copy did not complete in time");
+        if (*herr) {   // reported once: the flags are cleared
+            CK(cudaMemsetAsync(&b->ds.ctl->err, 0, sizeof(uint32_t), b->stream));
+            CK(cudaStreamSynchronize(b->stream));
+            if (*herr & (kErrStageTimeout | kErrStageDrain))
+                return fail(DTB_ERR_CUDA, "a staged state copy did not complete in time%s (the update loaded that "
+                            "state from global memory instead)", (*herr & kErrStageDrain) ? " and had not landed at exit" : "");
+        }
         if (where == DTB_HOST) {
             if (sum_out && bs) std::memcpy(sum_out + row0 * ns, p, bs);
             if (mean_out && bs) std::memcpy(mean_out + row0 * ns, p + bs, bs);
@@ -1186,6 +1206,7 @@ int dtb_block_create(const dtb_block_desc* d, dtb_block** out)
     if (d->n_synapses < 0) return fail(DTB_ERR_ARG, "n_synapses < 0");
     if (d->n_synapses > 0 && (!d->post || !d->pre || !d->kind || !d->weight)) return fail(DTB_ERR_ARG, "synapse arrays are null");
     const int64_t N = d->n_neurons, S = d->n_synapses;
+    RET(check_property(N, d->property, "dtb_block_create"));
     for (int64_t e = 0; e < S; ++e) {
         if (d->post[e] >= (uint64_t)N || d->pre[e] >= (uint64_t)N)
             return fail(DTB_ERR_ARG, "synapse %lld references neuron out of range (post %u, pre %u, N %lld)", (long long)e,
@@ -1453,6 +1474,7 @@ int dtb_block_create_from_npz(const char* dir, float dt, uint64_t seed, uint32_t
     }
     const int64_t N = bases.back(), S = syn.back();
     if (N <= 0 || N > (int64_t)kIndexMask) return fail(DTB_ERR_LIMIT, "n_neurons must be in [1, 2^31-1]");
+    RET(check_property(N, prop.data(), "dtb_block_create_from_npz"));
     dtb_block* b = new dtb_block();
     DeviceGuard guard(device < 0 ? 0 : device);
     int rc = create_common(b, device, dt, seed, stream_id);
@@ -1572,7 +1594,12 @@ int dtb_block_synchronize(dtb_block* b)
     CK(cudaStreamSynchronize(b->stream));
     uint32_t err = 0;
     CK(cudaMemcpy(&err, &b->ds.ctl->err, sizeof(err), cudaMemcpyDeviceToHost));
-    if (err & kErrStageTimeout) return fail(DTB_ERR_CUDA, "a staged state copy did not complete in time");
+    if (err) {
+        CK(cudaMemset(&b->ds.ctl->err, 0, sizeof(uint32_t)));
+        if (err & (kErrStageTimeout | kErrStageDrain))
+            return fail(DTB_ERR_CUDA, "a staged state copy did not complete in time (the update loaded that state "
+                        "from global memory instead)");
+    }
     return DTB_OK;
 }
 
@@ -1748,6 +1775,10 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         if (value < 0 || value > 4) return fail(DTB_ERR_ARG, "step variant must be 0..4");
         b->step_variant = (int)value;
         break;
+    case DTB_TUNE_STAGE_WAIT_LIMIT:
+        if (value < 0 || value > 0x7fffffffLL) return fail(DTB_ERR_ARG, "stage wait limit must be 0..2^31-1");
+        b->ds.stage_wait_limit = (uint32_t)value;
+        break;
     case DTB_TUNE_PUSH_METHOD:
         if (value < 0 || value > 2) return fail(DTB_ERR_ARG, "push method must be 0 (auto), 1 (atomics) or 2 (binned)");
         if (value == 2 && !bins_possible(b)) return fail(DTB_ERR_STATE, "binned push not possible for this network");
@@ -1791,6 +1822,7 @@ int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value)
     case DTB_TUNE_J_CACHE: *value = b->ds.j_keep; break;
     case DTB_TUNE_SCATTER_VARIANT: *value = b->scatter_variant; break;
     case DTB_TUNE_PUSH_METHOD: *value = b->push_method; break;
+    case DTB_TUNE_STAGE_WAIT_LIMIT: *value = b->ds.stage_wait_limit; break;
     case DTB_TUNE_BIN_WORDS: *value = b->bin_words; break;
     case DTB_TUNE_BIN_CAPACITY: *value = b->bin_cap_per_neuron; break;
     case DTB_TUNE_BIN_SHIFT: *value = b->ds.bin_cnt ? b->ds.bin_shift : bin_shift_for(b); break;
@@ -2083,6 +2115,7 @@ static int keep_current_isyn(dtb_block* b)
 int dtb_block_update_property(dtb_block* b, const float* property, const float* decay)
 {
     if (!b || !property) return fail(DTB_ERR_ARG, "null argument");
+    RET(check_property(b->N, property, "dtb_block_update_property"));
     DeviceGuard g(b->device);
     DevState& s = b->ds;
     RET(keep_current_isyn(b));   // keep the current synaptic current (computed with the old parameters)
@@ -2264,40 +2297,6 @@ int dtb_block_set_input_spikes(dtb_block* b, int64_t n_src, const uint32_t* neur
     s.forced_active = dv;
     s.forced_mask = dm;
     drop_graphs(b);
-    return DTB_OK;
-}
-
-int dtb_measure_atomic_rate(int device, int64_t n_targets, int64_t n_ops, int64_t window, float* ms_out)
-{
-    if (!ms_out || n_targets < 1 || n_targets > (int64_t)kIndexMask || n_ops < 1 || window < 1)
-        return fail(DTB_ERR_ARG, "bad argument");
-    DeviceGuard g(device);
-    int sms = 148;
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    uint32_t* idx = nullptr; float2* J = nullptr;
-    cudaEvent_t a = nullptr, z = nullptr;
-    cudaError_t e = cudaMalloc(&idx, sizeof(uint32_t) * (size_t)n_ops);
-    if (e == cudaSuccess) e = cudaMalloc(&J, sizeof(float2) * (size_t)n_targets);
-    if (e == cudaSuccess) e = cudaMemset(J, 0, sizeof(float2) * (size_t)n_targets);
-    if (e == cudaSuccess) e = cudaEventCreate(&a);
-    if (e == cudaSuccess) e = cudaEventCreate(&z);
-    if (e == cudaSuccess) {
-        k_probe_fill<<<grid_for(n_ops, 256), 256>>>(idx, n_ops, (uint32_t)n_targets,
-                                                    (uint32_t)std::min<int64_t>(window, n_targets), 12345u);
-        for (int w = 0; w < 2; ++w) k_probe_red<<<sms * 16, 256>>>(idx, n_ops, J);
-        cudaEventRecord(a);
-        for (int r = 0; r < 10; ++r) k_probe_red<<<sms * 16, 256>>>(idx, n_ops, J);
-        cudaEventRecord(z);
-        e = cudaEventSynchronize(z);
-        float ms = 0.0f;
-        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, z);
-        *ms_out = ms / 10.0f;
-    }
-    if (a) cudaEventDestroy(a);
-    if (z) cudaEventDestroy(z);
-    cudaFree(idx);
-    cudaFree(J);
-    if (e != cudaSuccess) return fail(DTB_ERR_CUDA, "atomic-rate probe: %s", cudaGetErrorString(e));
     return DTB_OK;
 }
 

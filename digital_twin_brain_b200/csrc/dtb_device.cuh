@@ -157,6 +157,7 @@ struct DevState {
     float* st_mean;             // [stats_cap][n_sub]
     uint32_t* st_nact;          // [stats_cap]
     Ctl* ctl;
+    uint32_t stage_wait_limit;     // polls of a staged copy's mbarrier before the update gives up on it
     unsigned long long* ev_part;   // [kEvParts] synaptic event counters (summed into ctl->events on demand;
                                    // nullable: then the kernels add to ctl->events)
     uint64_t seed;

@@ -137,6 +137,7 @@ bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std
     for (uint64_t e = 0; e < n_entries; ++e) {
         if (p + 46 > (uint64_t)fsize || rd32(b + p) != 0x02014b50u) { err = "bad central directory: " + path; return false; }
         const int method = rd16(b + p + 10);
+        const uint32_t crc_expect = rd32(b + p + 16);
         uint64_t csize = rd32(b + p + 20), usize = rd32(b + p + 24);
         const int nlen = rd16(b + p + 28), xlen = rd16(b + p + 30), clen = rd16(b + p + 32);
         uint64_t loff = rd32(b + p + 42);
@@ -176,6 +177,16 @@ bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std
         } else {
             err = "unsupported zip compression method in " + name;
             return false;
+        }
+        if (blen != usize) { err = "member size differs from its directory entry: " + name; return false; }
+        {   // CRC-32 of the member's uncompressed bytes against its central-directory entry
+            uLong crc = crc32(0L, Z_NULL, 0);
+            for (size_t at = 0; at < blen;) {
+                const size_t n = std::min<size_t>(blen - at, (size_t)1 << 30);
+                crc = crc32(crc, reinterpret_cast<const Bytef*>(buf + at), (uInt)n);
+                at += n;
+            }
+            if ((uint32_t)crc != crc_expect) { err = "CRC-32 mismatch (corrupt member): " + name; return false; }
         }
         std::string key = name;
         if (key.size() > 4 && key.compare(key.size() - 4, 4, ".npy") == 0) key = key.substr(0, key.size() - 4);

@@ -359,7 +359,8 @@ __global__ void k_samples(DevState s)
 // 3 KB per buffer: eight warps' double buffers (48 KB) fit four CTAs per SM.
 constexpr int kStageBytes = kWarpNeurons * (4 + 4 + 8 + 8);       // 3072 per tile buffer
 constexpr int kStagedSmem = (kStepThreads / 32) * 2 * kStageBytes;
-constexpr uint32_t kErrStageTimeout = 1u;                        // Ctl::err bit
+constexpr uint32_t kErrStageTimeout = 1u;                        // Ctl::err bit: a staged copy was given up on
+constexpr uint32_t kErrStageDrain = 2u;                          // Ctl::err bit: ... and had not landed at exit
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -386,10 +387,11 @@ __device__ __forceinline__ void stage_tile(const DevState& s, int64_t base, unsi
     stage_issue(d + kWarpNeurons * 16, s.J2 + s.j_ps + base, kWarpNeurons * 8, mbar);
 }
 
-// Bounded wait for a buffer's copies; false after the limit (the caller then loads from global).
-__device__ __forceinline__ bool stage_wait(uint32_t mbar, uint32_t parity)
+// Bounded wait for a buffer's copies: at most `limit` polls; false after the limit (the
+// caller then loads from global).  limit 0 gives up at once (tests of the fallback).
+__device__ __forceinline__ bool stage_wait(uint32_t mbar, uint32_t parity, uint32_t limit)
 {
-    for (uint32_t it = 0; it < (1u << 20); ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t ok;
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
@@ -514,6 +516,9 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     // STAGED: whole tiles are copied one ahead into two per-warp buffers (the second J
     // plane must start on 16 bytes: the host stages only split planes with an even stride)
     unsigned char* my_stage = stage_smem + (size_t)wid * 2 * kStageBytes;
+    bool stage_off = false;      // a copy was given up on: no more copies from this warp
+    int bad_sb = 0;              // ... the buffer it targets and the phase it belongs to
+    uint32_t bad_parity = 0;
     if (STAGED) {
         if (lane == 0) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&stage_bar[wid][0])) : "memory");
@@ -544,17 +549,28 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         float4 Jn[4];
         const int it = (int)(tile - tile0);
         const int sb = it & 1;
-        bool staged = false;   // this tile's state is in my_stage[sb]
+        bool staged = false;   // this tile's state is in stage_buf
+        unsigned char* stage_buf = my_stage + sb * kStageBytes;
         if (STAGED) {
-            if (lane == 0 && tile + 1 < tile1 && (tile + 2) * kWarpNeurons <= s.N)
+            if (!stage_off && base + kWarpNeurons <= s.N) {
+                const bool ok = stage_wait(smem_u32(&stage_bar[wid][sb]), (uint32_t)((it >> 1) & 1),
+                                           s.stage_wait_limit);
+                staged = __all_sync(0xffffffffu, ok);
+                if (!staged) {
+                    // copy given up on: flag it, issue no further copies, and keep off its
+                    // buffer (the copy may still land there) until the drain at exit
+                    if (lane == 0) atomicOr(&s.ctl->err, kErrStageTimeout);
+                    stage_off = true;
+                    bad_sb = sb;
+                    bad_parity = (uint32_t)((it >> 1) & 1);
+                }
+            }
+            if (stage_off && sb == bad_sb) stage_buf = my_stage + (sb ^ 1) * kStageBytes;
+            // the next tile's copy, into the buffer the previous tile has finished with
+            if (!stage_off && lane == 0 && tile + 1 < tile1 && (tile + 2) * kWarpNeurons <= s.N)
                 stage_tile(s, base + kWarpNeurons, my_stage + (sb ^ 1) * kStageBytes,
                            smem_u32(&stage_bar[wid][sb ^ 1]));
-            if (base + kWarpNeurons <= s.N) {
-                staged = stage_wait(smem_u32(&stage_bar[wid][sb]), (uint32_t)((it >> 1) & 1));
-                if (!staged && lane == 0) atomicOr(&s.ctl->err, kErrStageTimeout);
-            }
         }
-        unsigned char* stage_buf = my_stage + sb * kStageBytes;
         if (GATHER == kGatherMasks) {
             // The warp lists every marked pull entry of its 128 neurons (a lane's entries
             // contiguous, neuron by neuron, excitatory then inhibitory, ascending position),
@@ -936,6 +952,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         for (int j = 0; j < 4; ++j)
             if (valid[j]) same = same && (c_in[j] == c0);
         if (__all_sync(0xffffffffu, same)) {
+            // one class for the warp's tile, loaded once into registers (a per-warp shared
+            // copy read field by field measured slower: 0.230 against 0.224 ms)
             const ParamClass p = load_class(s.pc, c0);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
@@ -943,7 +961,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         } else {
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-                if (valid[j]) neuron(j, load_class(s.pc, c_in[j]));
+                if (valid[j]) neuron(j, s.pc[c_in[j]]);   // fields read from the (L1-cached) table as used
         }
 
         uint32_t cnt_spk = 0, cnt_nact = 0;
@@ -992,6 +1010,12 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         if (STAGED) __syncwarp();   // every lane is done with the buffer before lane 0 refills it
     }
     if (flushed) __threadfence();
+    if (STAGED && stage_off) {
+        // a copy given up on must land before this CTA's shared memory is released
+        if (lane == 0 && !stage_wait(smem_u32(&stage_bar[wid][bad_sb]), bad_parity, 1u << 22))
+            atomicOr(&s.ctl->err, kErrStageDrain);
+        __syncwarp();
+    }
 
     // ---- CTA merge: one barrier, one set of atomics, one done-count per CTA
     if (lane == 0) { sh_sub[wid] = cur_sub; sh_spk[wid] = acc_spk; sh_nact[wid] = acc_nact; sh_vsum[wid] = acc_v; sh_ev[wid] = acc_ev; }
@@ -1938,27 +1962,6 @@ __global__ void k_fill4(float4* p, int64_t n, float4 val)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = val;
-}
-
-// ------------------------------------------------------------ atomic-rate probe
-// The push scatter's ceiling: float2 atomics at n_ops targets drawn inside a
-// window of `window` neurons that moves with the op index (a region's
-// intra-region synapses), or anywhere in [0, n) when window >= n.
-__global__ void k_probe_fill(uint32_t* idx, int64_t n_ops, uint32_t n, uint32_t window, uint32_t seed)
-{
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_ops) return;
-    uint32_t x = (uint32_t)i * 2654435761u ^ seed;
-    x ^= x >> 13; x *= 0x5bd1e995u; x ^= x >> 15;
-    const uint32_t w = window < n ? window : n;
-    const uint32_t start = (uint32_t)(((uint64_t)(i / 100) * 100u) % n);
-    idx[i] = (uint32_t)(((uint64_t)start + (x % w)) % n);
-}
-
-__global__ void k_probe_red(const uint32_t* __restrict__ idx, int64_t n_ops, float2* J)
-{
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_ops; i += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(J + __ldcs(idx + i), make_float2(1.0f, 0.5f));
 }
 
 }  // namespace dtb

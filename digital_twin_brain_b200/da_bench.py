@@ -30,7 +30,9 @@ from .assimilation import DAConfig, EnsembleDA, SurrogateDA, collect_windows, ju
 from .surrogate import HISTORY, RateSurrogate
 
 
-def main(argv=None):
+def main(argv=None, quiet: bool = False) -> dict:
+    """Runs the comparison with command-line style arguments; returns the result dict
+    (and prints it as one JSON line unless quiet)."""
     ap = argparse.ArgumentParser()
     ap.add_argument("--members", type=int, default=128)
     ap.add_argument("--judges", type=int, default=16)
@@ -170,10 +172,12 @@ def main(argv=None):
     out["plain_rmse_seed_spread"] = float(np.max(plain_rmse) / np.min(plain_rmse) - 1.0) if len(plain_rmse) > 1 else None
     out["total_s"] = time.perf_counter() - t_all
     line = json.dumps(out)
-    print(line)
+    if not quiet:
+        print(line)
     if a.out:
         with open(a.out, "w") as f:
             f.write(line + "\n")
+    return out
 
 
 if __name__ == "__main__":

@@ -227,3 +227,26 @@ def config_one_region(noise_rate: float = 0.01) -> NetworkSpec:
 def config_whole_brain(scale: float = 1.0) -> NetworkSpec:
     """90 regions, log-normal(ln 2.2e5, 0.5) sizes (~2e7 neurons), K=100 (~2e9 synapses)."""
     return whole_brain(90, 2.2e5, 0.5, 100, scale=scale, name="whole_brain_90" + ("" if scale == 1.0 else f"_x{scale}"))
+
+
+def ensemble_members(n_members: int = 64, n_min: int = 50_000, n_max: int = 400_000, K: int = 100,
+                     seed: int = 0, scale: float = 1.0):
+    """Members of the batched-ensemble workload: neuron counts U[n_min, n_max] (times `scale`),
+    one 80/20 block each with its own generator seed, and per-member g_ui factors U[0.5, 1.5]
+    for the four receptors (data_assimilation/DataAssimilation.py:97 concatenates members; the
+    per-member factors are cuda/python/dist_blockwrapper_pytorch.py:446-458 scalings)."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(n_min, n_max + 1, n_members)
+    sizes = np.maximum(np.round(sizes * scale), 2 * K + 2).astype(np.int64)
+    g_scale = rng.uniform(0.5, 1.5, (n_members, 4)).astype(np.float32)
+    members = [single_block(int(n), K, gen_seed=seed * 1000 + m, name=f"member{m}") for m, n in enumerate(sizes)]
+    return members, g_scale
+
+
+def config_ensemble(n_members: int = 64, scale: float = 1.0, seed: int = 0) -> NetworkSpec:
+    """64 members, N ~ U[5e4, 4e5] each (~1.4e7 neurons, ~1.4e9 synapses in all), K=100,
+    per-member g_ui U[0.5, 1.5] x the single-block values, one BOLD region per member."""
+    members, g_scale = ensemble_members(n_members, seed=seed, scale=scale)
+    spec = ensemble(members, g_scale=g_scale, name=f"ensemble_{n_members}" + ("" if scale == 1.0 else f"_x{scale}"))
+    spec.extra["g_scale"] = g_scale
+    return spec

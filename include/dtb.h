@@ -249,10 +249,17 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          firing rows one scatter CTA takes per round (1..256)
  * DTB_TUNE_BIN_CAPACITY    binned push: bin entries per neuron of the bin
  *                          (1..1024, default 8; 10 bytes each); reallocates
- * DTB_TUNE_BIN_SHIFT       binned push: B (10..13), 0 = chosen from N (11 from 8M neurons, else 10); reallocates */
+ * DTB_TUNE_BIN_SHIFT       binned push: B (10..13), 0 = chosen from N (11 from 8M neurons, else 10); reallocates
+ * DTB_TUNE_STAGE_WAIT_LIMIT polls of a staged copy's completion barrier before the
+ *                          update gives up on it (default 2^20; 0 gives up at once, for
+ *                          tests): the update then loads that state from global memory,
+ *                          stops staging for the rest of the launch and the next call that
+ *                          reads results returns DTB_ERR_CUDA (the flag is cleared once
+ *                          reported; the results themselves are exact) */
 enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,
        DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5, DTB_TUNE_J_CACHE = 6, DTB_TUNE_SCATTER_VARIANT = 7,
-       DTB_TUNE_PUSH_METHOD = 8, DTB_TUNE_BIN_WORDS = 9, DTB_TUNE_BIN_CAPACITY = 10, DTB_TUNE_BIN_SHIFT = 11 };
+       DTB_TUNE_PUSH_METHOD = 8, DTB_TUNE_BIN_WORDS = 9, DTB_TUNE_BIN_CAPACITY = 10, DTB_TUNE_BIN_SHIFT = 11,
+       DTB_TUNE_STAGE_WAIT_LIMIT = 12 };
 int dtb_block_set_tuning(dtb_block* b, int key, int64_t value);
 int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value);
 
@@ -320,14 +327,6 @@ int dtb_block_gamma_property_by_subblock(dtb_block* b, int n, const int32_t* sub
  * removes the inputs. */
 int dtb_block_set_input_spikes(dtb_block* b, int64_t n_src, const uint32_t* neurons, int64_t T,
                                const uint8_t* spikes);
-
-/* Measurement helper, no counterpart in the reference: the rate of float2
- * atomic additions (the push scatter's per-synapse operation) on `device`,
- * n_ops of them into n_targets float2 targets, each target drawn inside a
- * window of `window` consecutive targets that moves with the operation index
- * (window >= n_targets: anywhere).  ms_out = milliseconds for the n_ops.
- * Allocates and frees its own device buffers. */
-int dtb_measure_atomic_rate(int device, int64_t n_targets, int64_t n_ops, int64_t window, float* ms_out);
 
 /* models/block.py:172-177 block.update_conn_weight: set the channel weight
  * of existing synapses (channel[i], post[i], pre[i]) to value[i]. */
@@ -466,11 +465,22 @@ typedef struct {
  * every GPU that loads the library holds until the process exits; hence the
  * limits DTB_PREALLOC_MAX_NEURONS and DTB_PREALLOC_MAX_SUBBLOCKS, beyond which
  * the call returns DTB_ERR_LIMIT (bad pointers or dt: DTB_ERR_ARG; a failed
- * launch: DTB_ERR_CUDA; this call reports by status code only).  The first call on a device looks up the
- * array's device address (with that device current); make that first call
- * before any stream capture.  All calls share the array and every call
+ * launch: DTB_ERR_CUDA; this call reports by status code only; a CUDA error left
+ * pending on the calling thread by earlier, unrelated work is reported through
+ * this call as DTB_ERR_CUDA too).  The first call on a device is the warm-up:
+ * it looks up the array's device address (with that device current) and, under
+ * CUDA's lazy module loading (the default), that lookup loads the kernels and
+ * the array, which can allocate and synchronise once.  Make that first call
+ * before entering a loop that must not allocate and before any stream capture,
+ * or set CUDA_MODULE_LOADING=EAGER.  All calls share the array and every call
  * re-initialises what it uses, but calls whose work overlaps on the GPU (two
  * streams, two host threads) race on it: serialise them.
+ *
+ * Preconditions the call does not check (the kernels index with these values;
+ * an array that breaks them makes the kernels read outside the arrays): every
+ * (index[e] & 0x7fffffff) < n_neurons; rowptr non-decreasing with rowptr[0] = 0
+ * and rowptr[n_neurons] = the number of synapses; every cls[n] below the number
+ * of rows of `classes`; every class's subblock below n_subblocks or -1.
  *
  * t is block.t before the step and step the number of steps already taken
  * (the noise counter); after the call block.t is float32(t + dt).  sum_out /

@@ -106,3 +106,24 @@ def test_set_bold_state_roundtrip():
         v = np.linspace(0.5, 1.5, e.R)
         net.set_bold(f, v)
         assert np.array_equal(net.get_bold(f), v)
+
+
+def test_ensemble_workload_members_equal_standalone():
+    """The batched-ensemble workload (64 members of N~U[5e4,4e5] at 2 % size, per-member g_ui
+    factors U[0.5,1.5]): members picked across the ensemble equal themselves simulated alone,
+    bit for bit in pull mode."""
+    e = synthetic.config_ensemble(scale=0.02)
+    members, g = synthetic.ensemble_members(scale=0.02)
+    ens = Network.from_spec(e, device=0)
+    s_e, m_e, _ = ens.run(120, mode="pull")
+    Ve = ens.get(FIELD_V)
+    for m in (0, 31, 63):
+        alone = _scaled(members[m], g[m])
+        alone.stream_id = m
+        net = Network.from_spec(alone, device=0)
+        s_a, m_a, _ = net.run(120, mode="pull")
+        ms = int(e.members["member_start"][m])
+        r0 = synthetic.member_region_index(e, m, 0)
+        assert np.array_equal(s_e[:, 2 * r0:2 * r0 + 2], s_a), f"member {m}: spike counts differ"
+        assert np.array_equal(m_e[:, 2 * r0:2 * r0 + 2], m_a)
+        assert np.array_equal(Ve[ms:ms + members[m].N], net.get(FIELD_V)), f"member {m}: V differs"

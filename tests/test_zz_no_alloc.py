@@ -9,11 +9,15 @@ memory is a fixed static device array inside libdtb.so.
 
 The test builds the same network twice — once as a library-owned handle
 (dtb_block_create_synthetic + dtb_block_run in pull mode, the existing entry
-point) and once as plain caller-owned device tensors — and checks that two
-calls in a row of the allocation-free entry point give the same V, J, t_last
-and per-subblock results, bit for bit (the pull path's tolerance is zero).
-It also checks that sizes beyond the fixed scratch are rejected.  The file is
-named to be collected last.
+point) and once as plain caller-owned device tensors — and checks that calls in
+a row of the allocation-free entry point give the same V, J, t_last and
+per-subblock results, bit for bit (the pull path's tolerance is zero): the first
+two calls, and then enough calls (100) that the neurons leave the 5 ms (50-step)
+refractory window every neuron starts in, so threshold crossings, t_last and
+spike propagation are compared too.  Variants: isolated steps, no statistics
+outputs (the scratch's spare rows), no subblocks.  The device's free memory must
+not change across the calls after the first.  It also checks that sizes beyond
+the fixed scratch are rejected.  The file is named to be collected last.
 """
 import ctypes
 
@@ -75,7 +79,8 @@ def step_fn():
     return fn
 
 
-def test_preallocated_step_matches_library_owned_run_twice():
+@pytest.mark.parametrize("case", ["plain", "isolated", "no_outputs", "no_subblocks"])
+def test_preallocated_step_matches_library_owned_run(case):
     spec = synthetic.single_block(20000, 100, name="prealloc_20k")
     cdec = per_class_decay(spec)
     ref = Network.from_spec(spec, device=0, build_push=False, class_decay=cdec)
@@ -94,30 +99,42 @@ def test_preallocated_step_matches_library_owned_run_twice():
     rp = torch.from_numpy(rowptr).to(dev)
     ix = torch.from_numpy(index.view(np.int32)).to(dev)
     w = torch.from_numpy(weight).to(dev)
-    n_sub = 2 * spec.R
-    sub_count = torch.from_numpy(np.bincount(cls_np, minlength=n_sub).astype(np.int32)).to(dev)
-    sums = torch.empty(n_sub, dtype=torch.float32, device=dev)
-    means = torch.empty(n_sub, dtype=torch.float32, device=dev)
+    n_sub = 0 if case == "no_subblocks" else 2 * spec.R
+    sub_count = torch.from_numpy(np.bincount(cls_np, minlength=2 * spec.R).astype(np.int32)).to(dev)
+    sums = torch.empty(2 * spec.R, dtype=torch.float32, device=dev)
+    means = torch.empty(2 * spec.R, dtype=torch.float32, device=dev)
+    outputs = case in ("plain", "isolated")
     net = PreallocNet(n_neurons=spec.N, n_subblocks=n_sub, device=0, V=V.data_ptr(), J=J.data_ptr(),
                       t_last=t_last.data_ptr(), cls=cls.data_ptr(), classes=classes.data_ptr(),
-                      sub_count=sub_count.data_ptr(), rowptr=rp.data_ptr(), index=ix.data_ptr(), weight=w.data_ptr(), dt=spec.dt,
-                      seed=spec.seed, stream_id=spec.stream_id)
+                      sub_count=sub_count.data_ptr() if n_sub else None, rowptr=rp.data_ptr(), index=ix.data_ptr(),
+                      weight=w.data_ptr(), dt=spec.dt, seed=spec.seed, stream_id=spec.stream_id)
     fn = step_fn()
     stream = torch.cuda.current_stream(dev)
     t = np.float32(0.0)
-    for step in range(2):
-        rc = fn(ctypes.byref(net), float(t), step, 0.01, 0, sums.data_ptr(), means.data_ptr(),
-                ctypes.c_void_p(stream.cuda_stream))
+    iso = case == "isolated"
+    spiked = 0
+    for step in range(100):
+        stream.synchronize()
+        free_before = torch.cuda.mem_get_info(dev)[0]
+        rc = fn(ctypes.byref(net), float(t), step, 0.01, int(iso), sums.data_ptr() if outputs else None,
+                means.data_ptr() if outputs else None, ctypes.c_void_p(stream.cuda_stream))
         assert rc == 0
         stream.synchronize()
+        if step > 0:   # the calls after the first allocate nothing on the device
+            assert torch.cuda.mem_get_info(dev)[0] == free_before
         t = np.float32(t + np.float32(spec.dt))
-        s_ref, m_ref, _ = ref.run(1, noise_rate=0.01, mode="pull")
-        assert np.array_equal(sums.cpu().numpy(), s_ref[0])
-        assert np.array_equal(means.cpu().numpy(), m_ref[0])
-        assert np.array_equal(V.cpu().numpy(), ref.get(FIELD_V)), f"V differs after call {step + 1}"
-        assert np.array_equal(J.cpu().numpy().T, ref.get(FIELD_J)), f"J differs after call {step + 1}"
-        assert np.array_equal(t_last.cpu().numpy(), ref.get(FIELD_T_LAST))
+        s_ref, m_ref, _ = ref.run(1, noise_rate=0.01, isolated=iso, mode="pull")
+        spiked += int(s_ref[0].sum())
+        if outputs:
+            assert np.array_equal(sums.cpu().numpy(), s_ref[0])
+            assert np.array_equal(means.cpu().numpy(), m_ref[0])
+        if step < 2 or step % 10 == 9:
+            assert np.array_equal(V.cpu().numpy(), ref.get(FIELD_V)), f"V differs after call {step + 1}"
+            assert np.array_equal(J.cpu().numpy().T, ref.get(FIELD_J)), f"J differs after call {step + 1}"
+            assert np.array_equal(t_last.cpu().numpy(), ref.get(FIELD_T_LAST))
     assert float(t) == np.float32(ref.get(7))  # block.t advances identically
+    assert spiked > 0                          # threshold crossings after the refractory window
+    assert (t_last.cpu().numpy() > 0).any()
 
 
 def test_preallocated_step_rejects_sizes_beyond_its_scratch():
