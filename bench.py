@@ -75,10 +75,10 @@ def parse():
     ap.add_argument("--scatter-words", type=int, default=0, help="atomic scatter bitmask words per warp (0: tuned)")
     ap.add_argument("--da", type=int, default=-1,
                     help="1: run the data-assimilation comparison (default: on for the whole-brain line)")
-    ap.add_argument("--da-region-size", type=float, default=250)
+    ap.add_argument("--da-region-size", type=float, default=2000)
     ap.add_argument("--da-windows", type=int, default=24)
     ap.add_argument("--da-members", type=int, default=128)
-    ap.add_argument("--da-train-windows", type=int, default=20)
+    ap.add_argument("--da-train-windows", type=int, default=16)
     return ap.parse_args()
 
 
@@ -318,6 +318,42 @@ def atomic_probe(dev, N, evs, window):
         return None
 
 
+def mlp_measure(dev, peaks) -> dict:
+    """The surrogate network's tensor-core kernels (tcgen05, BF16 operands, FP32 accumulation) timed
+    on the DA forecast batch (128 members x 90 regions) and a training minibatch, against the
+    measured dense BF16 peak.  Algorithmic FLOPs count each multiply-add of the network once (the
+    kernels run three BF16 products per FP32 operand to keep FP32 accuracy)."""
+    import torch
+    from digital_twin_brain_b200.surrogate import MLP
+    torch.cuda.set_device(dev)
+    in_dim, H = 14, 256
+    m = MLP(in_dim, H, seed=0, device=dev)
+    g = torch.Generator(device=f"cuda:{dev}").manual_seed(0)
+    out = {}
+    for name, B, fn in (("forward", 128 * 90, "fwd"), ("train_step", 4096, "train")):
+        x = torch.randn(B, in_dim, device=f"cuda:{dev}", generator=g)
+        t = torch.randn(B, device=f"cuda:{dev}", generator=g)
+        run = (lambda: m.forward(x)) if fn == "fwd" else (lambda: m.train_step(x, t, 1e-4))
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            run()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / 20
+        flops = 2.0 * B * (in_dim * H + H * H + H) * (1 if fn == "fwd" else 3)
+        tf = flops / (ms * 1e-3) / 1e12
+        peak = float(peaks.get("bf16_tflops", 1590.0))
+        out[name] = {"rows": B, "ms": ms, "tflops": tf, "peak_tflops": peak, "frac": tf / peak,
+                     "unit": "TFLOP/s", "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)"
+                     if "bf16_tflops" in peaks else "fallback 1590 TFLOP/s"}
+    m.close()
+    return out
+
+
 def run_da(args, dev):
     """The data-assimilation comparison (metric part 3) at a reduced region size."""
     from digital_twin_brain_b200 import da_bench
@@ -465,6 +501,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         net = None
         torch.cuda.empty_cache()
         da = run_da(args, dev)
+        da["mlp"] = mlp_measure(dev, peaks)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,

@@ -401,6 +401,42 @@ class SurrogateDA:
                     fallbacks=self.fallbacks, errors=np.array(self.errors))
 
 
+def collect_da_windows(template: synthetic.NetworkSpec, cfg: DAConfig, bold_obs: torch.Tensor, device: int = 0,
+                       history: int = 8, context: int | None = None):
+    """Training windows for the surrogate from an assimilation run (every member on the
+    simulator, data_assimilation/DataAssimilation.py:402-453) against observations of another
+    hidden truth: the g_ui factors of every window then move as the analysis moves them (large
+    steps in the first windows), which a random walk does not show.  Returns what
+    collect_windows returns, over the windows with a full history."""
+    from .surrogate import CONTEXT
+    context = CONTEXT if context is None else context
+    da = EnsembleDA(template, cfg, device)
+    da.hp_random_initialize()
+    hps, rates = [], []
+    for t in range(bold_obs.shape[0]):
+        da.da_evolve()
+        hps.append(da.hp.reshape(da.M, da.R, da.n_hp).cpu())
+        rates.append(torch.from_numpy(da.window_rates()).float())
+        da.da_filter(bold_obs[t].to(da.dev))
+    hp = torch.stack(hps)
+    rt = torch.stack(rates)
+    g, h, t = [], [], []
+    for w in range(history, len(hps)):
+        g.append(hp[w].reshape(-1, 4))
+        h.append(with_context(rt[w - history:w].permute(1, 2, 0), context))
+        t.append(rt[w].reshape(-1))
+    # the first windows (short histories padded with their earliest rate), where the analysis
+    # moves the parameters most
+    for w in range(1, min(history, len(hps))):
+        hw = rt[:w].permute(1, 2, 0)
+        hw = torch.cat([hw[:, :, :1].repeat(1, 1, history - w), hw], 2)
+        g.append(hp[w].reshape(-1, 4))
+        h.append(with_context(hw, context))
+        t.append(rt[w].reshape(-1))
+    del da
+    return torch.cat(g), torch.cat(h), torch.cat(t)
+
+
 def collect_windows(template: synthetic.NetworkSpec, cfg: DAConfig, windows: int, device: int = 0,
                     history: int = 8, context: int | None = None):
     """Training windows for the surrogate: an ensemble with random-walk g_ui factors (the DA

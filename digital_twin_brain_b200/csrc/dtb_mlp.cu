@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "dtb.h"
@@ -107,6 +108,217 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int64_t K, const TA*
 }
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+
+// ------------------------------------------------------------ tensor-core GEMM (tcgen05)
+// C[M][N] = A[M][K] * B[K][N] on the 5th-generation tensor cores: tcgen05.mma of
+// kind::f16 with BF16 operands from shared memory and the FP32 accumulator in
+// tensor memory (TMEM), issued by one thread; the accumulator is read back with
+// tcgen05.ld by the four warps (warp w owns TMEM lanes 32w..32w+31 = tile rows).
+//
+// Operand precision: an operand already in BF16 (the weights) enters as one
+// term; an FP32 operand (activations, gradients) is split into three BF16 terms
+// hi + mid + lo (each the rounding of what the previous ones leave), and the
+// products of term pairs (i, j) with i + j < 3 are accumulated: BF16 x BF16
+// products are exact in FP32, so the result keeps FP32 accuracy (to a few units
+// of 2^-24 relative per product) while every multiply runs on the tensor cores.
+//
+// Tile: 128 rows (the M = 128 instruction shape, cta_group::1) x n_tile columns
+// (16..128, a multiple of 16), K in chunks of 32 (two K = 16 instructions).
+// Shared-memory operand layout: K-major, no swizzle, 8x16-byte core matrices,
+// core (r, c) of a 128x32 tile at (r * 4 + c) * 128 bytes: leading (K) byte
+// offset 128, stride (8-row) byte offset 512.  gridDim.z splits K; partial tiles
+// are then added to C atomically (C pre-zeroed).
+constexpr int kMmaM = 128;
+constexpr int kMmaKc = 32;                        // K per staged chunk
+constexpr int kMmaThreads = 128;
+constexpr int kMmaTile = kMmaM * kMmaKc * 2;      // bytes of one BF16 term tile (8 KB)
+constexpr int kMmaTmemCols = 128;
+
+struct MmaArgs {
+    int M, N;
+    int64_t K;
+    const void* A; int64_t a_m, a_k; int a_bf16;  // A(m, k) = A[m * a_m + k * a_k]
+    const void* B; int64_t b_k, b_n; int b_bf16;  // B(k, n) = B[k * b_k + n * b_n]
+    float* C; int64_t c_m;                        // C(m, n) = C[m * c_m + n]
+    int64_t k_per_split;
+    const float* bias;                            // epilogue (nullable): Z = acc + bias[n]
+    float* H;                                     // (nullable) H = GELU(Z), same layout as C
+    int n_tile;
+    unsigned* err;                                // set when a completion wait gave up
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (tcgen05): start >> 4, leading byte offset >> 4 at
+// bit 16, stride byte offset >> 4 at bit 32, descriptor version 1 at bit 46, no swizzle.
+__device__ __forceinline__ uint64_t mma_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3fffu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(512 >> 4) << 32) |
+           (1ull << 46);
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator (bit 4), A and B BF16 (bits 7, 10),
+// both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+__device__ __forceinline__ uint32_t mma_idesc(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kMmaM >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mma_wait(uint32_t mbar, uint32_t parity, uint32_t limit)
+{
+    for (uint32_t it = 0; it < limit; ++it) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+template <typename T>
+__device__ __forceinline__ float ld_elem(const T* p, int64_t i) { return load_f(p + i); }
+
+// Split x into nt BF16 terms (nt = 1: plain rounding).
+__device__ __forceinline__ void split_bf16(float x, int nt, __nv_bfloat16* t)
+{
+    float r = x;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (i < nt) {
+            t[i] = __float2bfloat16_rn(r);
+            r = r - __bfloat162float(t[i]);
+        }
+    }
+}
+
+// One 128 x 32 operand tile (rows = M or N of the instruction, K-major) into nt term tiles:
+// thread t stages row t.  get(row, k) returns the FP32 value (0 outside the matrix).
+template <typename Get>
+__device__ __forceinline__ void stage_rows(unsigned char* tiles, int nt, Get get)
+{
+    const int r = threadIdx.x;
+#pragma unroll
+    for (int c = 0; c < kMmaKc / 8; ++c) {          // four core matrices along K
+        __align__(16) __nv_bfloat16 t[3][8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            __nv_bfloat16 s3[3];
+            split_bf16(get(r, c * 8 + e), nt, s3);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) t[i][e] = s3[i];
+        }
+        const int off = ((r >> 3) * (kMmaKc / 8) + c) * 128 + (r & 7) * 16;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if (i < nt) *reinterpret_cast<uint4*>(tiles + i * kMmaTile + off) = *reinterpret_cast<const uint4*>(t[i]);
+    }
+}
+
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(kMmaThreads) k_mma_gemm(MmaArgs g)
+{
+    extern __shared__ __align__(1024) unsigned char mma_smem[];   // A term tiles, then B term tiles
+    __shared__ __align__(8) unsigned long long mbar;
+    __shared__ uint32_t tmem_base;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * kMmaM, n0 = blockIdx.x * g.n_tile;
+    const int64_t k_begin = (int64_t)blockIdx.z * g.k_per_split;
+    const int64_t k_end = k_begin + g.k_per_split < g.K ? k_begin + g.k_per_split : g.K;
+    const int nA = g.a_bf16 ? 1 : 3, nB = g.b_bf16 ? 1 : 3;
+    unsigned char* sA = mma_smem;
+    unsigned char* sB = mma_smem + nA * kMmaTile;
+    const TA* A = static_cast<const TA*>(g.A);
+    const TB* B = static_cast<const TB*>(g.B);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_addr(&tmem_base)), "r"((uint32_t)kMmaTmemCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&mbar)) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const uint32_t idesc = mma_idesc(g.n_tile);
+    const uint32_t mb = smem_addr(&mbar);
+
+    int chunks = 0;
+    bool ok = true;
+    for (int64_t k0 = k_begin; k0 < k_end; k0 += kMmaKc, ++chunks) {
+        if (chunks > 0 && ok) ok = mma_wait(mb, (uint32_t)((chunks - 1) & 1), 1u << 22);   // tiles free again
+        stage_rows(sA, nA, [&](int r, int k) -> float {
+            const int64_t m = m0 + r, kk = k0 + k;
+            return (m < g.M && kk < k_end) ? ld_elem(A, m * g.a_m + kk * g.a_k) : 0.0f;
+        });
+        stage_rows(sB, nB, [&](int r, int k) -> float {
+            const int64_t n = n0 + r, kk = k0 + k;
+            return (r < g.n_tile && n < g.N && kk < k_end) ? ld_elem(B, kk * g.b_k + n * g.b_n) : 0.0f;
+        });
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic stores -> tensor-core reads
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            int issued = 0;
+#pragma unroll
+            for (int s = 0; s < kMmaKc / 16; ++s)
+                for (int i = 0; i < nA; ++i)
+                    for (int j = 0; j < nB; ++j) {
+                        if (i + j >= 3) continue;
+                        const uint64_t ad = mma_desc(smem_addr(sA + i * kMmaTile + s * 256));
+                        const uint64_t bd = mma_desc(smem_addr(sB + j * kMmaTile + s * 256));
+                        const uint32_t acc = (chunks > 0 || issued > 0) ? 1u : 0u;
+                        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                     :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+                        ++issued;
+                    }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(mb) : "memory");
+        }
+    }
+    if (chunks > 0) {
+        if (ok) ok = mma_wait(mb, (uint32_t)((chunks - 1) & 1), 1u << 24);
+        if (!ok) {   // give up: flag it, and make sure the MMAs are done before TMEM is freed
+            if (threadIdx.x == 0 && g.err) atomicOr(g.err, 1u);
+            mma_wait(mb, (uint32_t)((chunks - 1) & 1), 1u << 26);
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // epilogue: warp w reads rows 32w + lane, 16 columns at a time
+        const int64_t m = m0 + warp * 32 + lane;
+        for (int c = 0; c < g.n_tile; c += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                           "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                         : "r"(taddr) : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (ok && m < g.M) {
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const int64_t n = n0 + c + e;
+                    if (c + e >= g.n_tile || n >= g.N) continue;
+                    float z = __uint_as_float(v[e]);
+                    if (gridDim.z > 1) { atomicAdd(g.C + m * g.c_m + n, z); continue; }
+                    if (g.bias) z += g.bias[n];
+                    g.C[m * g.c_m + n] = z;
+                    if (g.H) g.H[m * g.c_m + n] = gelu(z);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"((uint32_t)kMmaTmemCols)
+                     : "memory");
+    }
+}
 __device__ __forceinline__ float gelu_grad(float x)
 {
     // d/dx [x Phi(x)] = Phi(x) + x phi(x)
@@ -202,6 +414,7 @@ struct dtb_mlp {
     float *Z1 = nullptr, *H1 = nullptr, *Z2 = nullptr, *H2 = nullptr, *Y = nullptr;
     float *dY = nullptr, *dH2 = nullptr, *dZ2 = nullptr, *dH1 = nullptr, *dZ1 = nullptr;
     int64_t t = 0;                 // Adam step
+    unsigned* err = nullptr;       // device flag: a tensor-core GEMM gave up waiting for its MMAs
 };
 
 namespace {
@@ -220,6 +433,50 @@ int gemm(dtb_mlp* p, int M, int N, int64_t K, const TA* A, int64_t a_m, int64_t 
     dim3 grid(cdiv(N, TN), cdiv(M, TM), splits);
     k_gemm<TA, TB><<<grid, 256, 0, p->stream>>>(M, N, K, A, a_m, a_k, B, b_k, b_n, C, c_m, kps);
     MCK(cudaGetLastError());
+    return DTB_OK;
+}
+
+// The hidden layers' GEMMs on the tensor cores (k_mma_gemm): C = A B (+ bias, GELU when H).
+template <typename TA, typename TB>
+int mma_gemm(dtb_mlp* p, int M, int N, int64_t K, const TA* A, int64_t a_m, int64_t a_k, const TB* B, int64_t b_k,
+             int64_t b_n, float* C, int64_t c_m, bool split, const float* bias = nullptr, float* H = nullptr)
+{
+    MmaArgs g;
+    g.M = M; g.N = N; g.K = K;
+    g.A = A; g.a_m = a_m; g.a_k = a_k; g.a_bf16 = std::is_same<TA, __nv_bfloat16>::value ? 1 : 0;
+    g.B = B; g.b_k = b_k; g.b_n = b_n; g.b_bf16 = std::is_same<TB, __nv_bfloat16>::value ? 1 : 0;
+    g.C = C; g.c_m = c_m;
+    g.bias = bias; g.H = H;
+    g.err = p->err;
+    g.n_tile = N >= 128 ? 128 : ((N + 15) / 16) * 16;
+    const int64_t tiles = (int64_t)cdiv(N, g.n_tile) * cdiv(M, kMmaM);
+    int64_t splits = 1;
+    if (split) {
+        splits = std::min<int64_t>(std::max<int64_t>(1, (2 * 148 + tiles - 1) / tiles), std::max<int64_t>(1, K / 256));
+        MCK(cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * (size_t)c_m, p->stream));
+    }
+    g.k_per_split = ((K + splits - 1) / splits + kMmaKc - 1) / kMmaKc * kMmaKc;
+    splits = (K + g.k_per_split - 1) / g.k_per_split;      // no empty split
+    dim3 grid(cdiv(N, g.n_tile), cdiv(M, kMmaM), (unsigned)splits);
+    const int smem = ((g.a_bf16 ? 1 : 3) + (g.b_bf16 ? 1 : 3)) * kMmaTile;
+    static bool attr = false;
+    if (!attr) {
+        MCK(cudaFuncSetAttribute(k_mma_gemm<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 6 * kMmaTile));
+        attr = true;
+    }
+    k_mma_gemm<TA, TB><<<grid, kMmaThreads, smem, p->stream>>>(g);
+    MCK(cudaGetLastError());
+    return DTB_OK;
+}
+
+int check_err(dtb_mlp* p)
+{
+    unsigned e = 0;
+    MCK(cudaMemcpy(&e, p->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (e) {
+        cudaMemset(p->err, 0, sizeof(unsigned));
+        return mlp_fail(DTB_ERR_CUDA, "a tensor-core GEMM did not complete in time");
+    }
     return DTB_OK;
 }
 
@@ -243,13 +500,13 @@ int forward(dtb_mlp* p, const float* x, int64_t B, float* y)
 {
     const int in = p->in, H = p->H;
     const __nv_bfloat16* wb = p->wb;
-    // Z1 = X W1^T + b1, H1 = GELU(Z1)
-    if (int rc = gemm(p, (int)B, H, in, x, in, 1, wb + p->o_W1, 1, in, p->Z1, H, false)) return rc;
-    k_bias_act<<<cdiv(B * H, 256), 256, 0, p->stream>>>(B, H, p->Z1, p->w + p->o_b1, p->H1, 1);
+    // Z1 = X W1^T + b1, H1 = GELU(Z1) (tensor cores, bias and GELU in the epilogue)
+    if (int rc = mma_gemm(p, (int)B, H, in, x, in, 1, wb + p->o_W1, 1, in, p->Z1, H, false, p->w + p->o_b1, p->H1))
+        return rc;
     // Z2 = H1 W2^T + b2, H2 = GELU(Z2)
-    if (int rc = gemm(p, (int)B, H, H, p->H1, H, 1, wb + p->o_W2, 1, H, p->Z2, H, false)) return rc;
-    k_bias_act<<<cdiv(B * H, 256), 256, 0, p->stream>>>(B, H, p->Z2, p->w + p->o_b2, p->H2, 1);
-    // y = H2 W3^T + b3
+    if (int rc = mma_gemm(p, (int)B, H, H, p->H1, H, 1, wb + p->o_W2, 1, H, p->Z2, H, false, p->w + p->o_b2, p->H2))
+        return rc;
+    // y = H2 W3^T + b3 (one output column: a dot product per row)
     if (int rc = gemm(p, (int)B, 1, H, p->H2, H, 1, wb + p->o_W3, 1, H, y, 1, false)) return rc;
     k_bias_act<<<cdiv(B, 256), 256, 0, p->stream>>>(B, 1, y, p->w + p->o_b3, y, 0);
     MCK(cudaGetLastError());
@@ -269,13 +526,13 @@ int backward(dtb_mlp* p, const float* x, const float* target, int64_t B)
     k_colsum<<<dim3(1, cdiv(B, 256)), 256, 0, p->stream>>>(B, 1, p->dY, p->g + p->o_b3);
     if (int rc = gemm(p, (int)B, H, 1, p->dY, 1, 1, wb + p->o_W3, H, 1, p->dH2, H, false)) return rc;
     k_gelu_bwd<<<cdiv(B * H, 256), 256, 0, p->stream>>>(B * H, p->dH2, p->Z2, p->dZ2);
-    // layer 2: dW2 = dZ2^T H1, db2 = colsum dZ2, dH1 = dZ2 W2
-    if (int rc = gemm(p, H, H, B, p->dZ2, 1, H, p->H1, H, 1, p->g + p->o_W2, H, true)) return rc;
+    // layer 2: dW2 = dZ2^T H1, db2 = colsum dZ2, dH1 = dZ2 W2 (tensor cores)
+    if (int rc = mma_gemm(p, H, H, B, p->dZ2, 1, H, p->H1, H, 1, p->g + p->o_W2, H, true)) return rc;
     k_colsum<<<dim3(cdiv(H, 32), cdiv(B, 256)), 256, 0, p->stream>>>(B, H, p->dZ2, p->g + p->o_b2);
-    if (int rc = gemm(p, (int)B, H, H, p->dZ2, H, 1, wb + p->o_W2, H, 1, p->dH1, H, false)) return rc;
+    if (int rc = mma_gemm(p, (int)B, H, H, p->dZ2, H, 1, wb + p->o_W2, H, 1, p->dH1, H, false)) return rc;
     k_gelu_bwd<<<cdiv(B * H, 256), 256, 0, p->stream>>>(B * H, p->dH1, p->Z1, p->dZ1);
-    // layer 1: dW1 = dZ1^T X, db1 = colsum dZ1
-    if (int rc = gemm(p, H, in, B, p->dZ1, 1, H, x, in, 1, p->g + p->o_W1, in, true)) return rc;
+    // layer 1: dW1 = dZ1^T X, db1 = colsum dZ1 (tensor cores)
+    if (int rc = mma_gemm(p, H, in, B, p->dZ1, 1, H, x, in, 1, p->g + p->o_W1, in, true)) return rc;
     k_colsum<<<dim3(cdiv(H, 32), cdiv(B, 256)), 256, 0, p->stream>>>(B, H, p->dZ1, p->g + p->o_b1);
     MCK(cudaGetLastError());
     return DTB_OK;
@@ -321,6 +578,8 @@ int dtb_mlp_create(int in_dim, int hidden, uint64_t seed, int device, dtb_mlp** 
     if (e == cudaSuccess) e = cudaMalloc(&p->m, sizeof(float) * (size_t)o);
     if (e == cudaSuccess) e = cudaMalloc(&p->v, sizeof(float) * (size_t)o);
     if (e == cudaSuccess) e = cudaMalloc(&p->loss, sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&p->err, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(p->err, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemcpy(p->w, w.data(), sizeof(float) * (size_t)o, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(p->m, 0, sizeof(float) * (size_t)o);
     if (e == cudaSuccess) e = cudaMemset(p->v, 0, sizeof(float) * (size_t)o);
@@ -343,7 +602,7 @@ int dtb_mlp_destroy(dtb_mlp* p)
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(p->device);
-    void* bufs[] = {p->w, p->wb, p->g, p->m, p->v, p->loss, p->Z1, p->H1, p->Z2, p->H2, p->Y,
+    void* bufs[] = {p->w, p->wb, p->g, p->m, p->v, p->loss, p->err, p->Z1, p->H1, p->Z2, p->H2, p->Y,
                     p->dY, p->dH2, p->dZ2, p->dH1, p->dZ1};
     for (void* b : bufs) if (b) cudaFree(b);
     if (prev >= 0) cudaSetDevice(prev);
@@ -371,7 +630,7 @@ int dtb_mlp_get_params(dtb_mlp* p, float* dst, int where)
     MCK(cudaMemcpyAsync(dst, p->w, sizeof(float) * (size_t)p->n_params,
                         where == DTB_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, p->stream));
     MCK(cudaStreamSynchronize(p->stream));
-    return DTB_OK;
+    return check_err(p);
 }
 
 int dtb_mlp_set_params(dtb_mlp* p, const float* src, int where)

@@ -26,8 +26,24 @@ import numpy as np
 import torch
 
 from . import synthetic
-from .assimilation import DAConfig, EnsembleDA, SurrogateDA, collect_windows, judge_error, log_torch
+from .assimilation import (DAConfig, EnsembleDA, SurrogateDA, collect_da_windows, collect_windows, judge_error,
+                           log_torch)
 from .surrogate import HISTORY, RateSurrogate
+
+
+def observe(template, hp_true: torch.Tensor, windows: int, base: dict, seed: int) -> torch.Tensor:
+    """BOLD at the end of every window of one network with the hidden g_ui factors hp_true
+    [R, 4], plus Gaussian noise of 0.1 x the per-region std over the windows: [windows, R]."""
+    dev = hp_true.device
+    truth = EnsembleDA(template, DAConfig(n_members=1, **base))
+    truth.hp_log = log_torch(hp_true.reshape(1, -1), truth.low, truth.high)
+    truth.apply_hp()
+    bold_true = torch.stack([truth.evolve()[0, :, -1].double() for _ in range(windows)])   # [W, R]
+    del truth
+    sd = bold_true.std(0, keepdim=True).clamp_min(1e-9)
+    noise = torch.randn(bold_true.shape, device=dev, dtype=torch.float64,
+                        generator=torch.Generator(device=dev).manual_seed(seed))
+    return (bold_true + 0.1 * sd * noise).float()
 
 
 def main(argv=None, quiet: bool = False) -> dict:
@@ -45,6 +61,9 @@ def main(argv=None, quiet: bool = False) -> dict:
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--train-sigma", type=float, default=2.0,
                     help="random-walk variance of the training ensemble (wider than the DA walk for coverage)")
+    ap.add_argument("--train-source", default="da", choices=["da", "walk"],
+                    help="da: training windows from an assimilation run against another hidden truth (its "
+                         "analysis steps move the parameters as the served run's do); walk: a random-walk ensemble")
     ap.add_argument("--threshold", type=float, default=None,
                     help="judge fallback threshold (default: --margin x the held-out judge error of the surrogate)")
     ap.add_argument("--margin", type=float, default=1.5)
@@ -74,19 +93,8 @@ def main(argv=None, quiet: bool = False) -> dict:
     rng = np.random.default_rng(a.seed + 99)
 
     # ---- truth and observations
-    truth = EnsembleDA(template, DAConfig(n_members=1, **base))
     hp_true = torch.from_numpy(rng.uniform(0.6, 1.4, (template.R, 4)).astype(np.float32)).to(dev)
-    truth.hp_log = log_torch(hp_true.reshape(1, -1), truth.low, truth.high)
-    truth.apply_hp()
-    bold_true = []
-    for _ in range(a.windows):
-        bold_true.append(truth.evolve()[0, :, -1].double())
-    bold_true = torch.stack(bold_true)                                  # [W, R]
-    sd = bold_true.std(0, keepdim=True).clamp_min(1e-9)
-    obs = (bold_true + 0.1 * sd * torch.randn(bold_true.shape, device=dev, dtype=torch.float64,
-                                               generator=torch.Generator(device=dev).manual_seed(a.seed + 5)))
-    obs = obs.float()
-    del truth
+    obs = observe(template, hp_true, a.windows, base, a.seed + 5)
 
     def summarize(res, label):
         bp = res["bold_pred"][a.skip:]
@@ -116,10 +124,18 @@ def main(argv=None, quiet: bool = False) -> dict:
         torch.cuda.empty_cache()
     out["plain_rmse_by_seed"] = plain_rmse
 
-    # ---- surrogate training windows (a separate random-walk ensemble)
+    # ---- surrogate training windows: an assimilation run against another hidden truth, or a
+    #      separate random-walk ensemble
     t0 = time.perf_counter()
-    g, h, tgt = collect_windows(template, DAConfig(n_members=a.members, hp_sigma=a.train_sigma, **{**base, "seed": a.seed + 7}),
-                                windows=a.train_windows)
+    if a.train_source == "da":
+        hp_train = torch.from_numpy(np.random.default_rng(a.seed + 31).uniform(0.6, 1.4, (template.R, 4))
+                                    .astype(np.float32)).to(dev)
+        obs_train = observe(template, hp_train, a.train_windows, {**base, "seed": a.seed + 11}, a.seed + 13)
+        g, h, tgt = collect_da_windows(template, DAConfig(n_members=a.members, **{**base, "seed": a.seed + 7}),
+                                       obs_train)
+    else:
+        g, h, tgt = collect_windows(template, DAConfig(n_members=a.members, hp_sigma=a.train_sigma,
+                                                       **{**base, "seed": a.seed + 7}), windows=a.train_windows)
     t_collect = time.perf_counter() - t0
     n = g.shape[0]
     perm = torch.from_numpy(np.random.default_rng(a.seed).permutation(n))
@@ -136,7 +152,8 @@ def main(argv=None, quiet: bool = False) -> dict:
     val_err = judge_error(pred, tgt[te])
     threshold = a.threshold if a.threshold is not None else a.margin * val_err
     out.update(heldout_judge_err=val_err, threshold=threshold)
-    out.update(train_samples=int(n), train_windows=a.train_windows, train_sigma=a.train_sigma, train_collect_s=t_collect, train_s=t_train,
+    out.update(train_samples=int(n), train_windows=a.train_windows, train_source=a.train_source, train_sigma=a.train_sigma,
+               train_collect_s=t_collect, train_s=t_train,
                train_loss_first=hist[0], train_loss_last=hist[-1], heldout_logrmse_net=lerr_net,
                heldout_logrmse_persistence=lerr_persist)
 
