@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--da-region-size", type=float, default=2000)
     ap.add_argument("--da-windows", type=int, default=24)
     ap.add_argument("--da-members", type=int, default=128)
-    ap.add_argument("--da-train-windows", type=int, default=16)
+    ap.add_argument("--da-train-windows", type=int, default=10)
     return ap.parse_args()
 
 

@@ -24,7 +24,7 @@ FIELD_V, FIELD_J, FIELD_I_UI, FIELD_I_SYN, FIELD_T_LAST, FIELD_ACTIVE, FIELD_NEW
 
 TUNE_SCATTER_WORDS, TUNE_CHUNK, TUNE_PULL_THRESHOLD_PPM, TUNE_USE_GRAPHS, TUNE_STEP_VARIANT, TUNE_PULL_METHOD, \
     TUNE_J_CACHE, TUNE_SCATTER_VARIANT, TUNE_PUSH_METHOD, TUNE_BIN_WORDS, TUNE_BIN_CAPACITY, TUNE_BIN_SHIFT, \
-    TUNE_STAGE_WAIT_LIMIT = range(13)
+    TUNE_STAGE_WAIT_LIMIT, TUNE_SCATTER_REVERSE = range(14)
 
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "out of memory", 4: "I/O error", 5: "format error",
           6: "invalid state", 7: "limit exceeded"}

@@ -135,6 +135,7 @@ class BlockWrapper:
             self._sub_of = torch.from_numpy(sub).to(self._dev)
             self._sub_valid = (self._sub_of >= 0) & (self._sub_of < self._net.n_sub)
         isyn = torch.empty(self._net.N, dtype=torch.float32, device=self._dev)
+        self._net._torch_ready()
         _lib.call("dtb_block_get", self._net._h, FIELD_I_SYN, _lib.c_vp(isyn.data_ptr()), DTB_DEVICE)
         self._net.synchronize()
         acc = torch.zeros(max(self._net.n_sub, 1), dtype=torch.float64, device=self._dev)

@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <thread>
 #include <array>
 #include <cmath>
 #include <cstdarg>
@@ -1490,65 +1493,107 @@ int dtb_block_create_from_npz(const char* dir, float dt, uint64_t seed, uint32_t
     if (rc == DTB_OK) rc = dalloc(b, &prow, (size_t)N + 1);
     if (rc == DTB_OK) rc = dalloc(b, &pcol, (size_t)S);
     if (rc == DTB_OK) rc = dalloc(b, &pw, (size_t)S);
+    // Second pass, the files in parallel (worker threads, each with its own file): a worker
+    // reads a file, sorts its entries into the file's own rows (stable: file order inside a
+    // row) and uploads them to their place; out-degrees are counted on the device afterwards.
     std::vector<int64_t> rp((size_t)N + 1, 0);
-    std::vector<uint32_t> outdeg(build_push ? (size_t)N + 1 : 0, 0u);
     const std::vector<std::string> syn_names = {"output_neuron_idx", "input_block_idx", "input_neuron_idx",
                                                 "input_channel_offset", "weight"};
-    for (size_t i = 0; i < F && rc == DTB_OK; ++i) {
-        std::map<std::string, NpyArray> m;
-        std::string err;
-        if (!npz_read(paths[i], m, err, &syn_names)) { rc = fail(DTB_ERR_FORMAT, "%s", err.c_str()); break; }
-        for (auto& nm : syn_names)
-            if (!m.count(nm)) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: missing %s", i, nm.c_str()); break; }
-        if (rc != DTB_OK) break;
-        const NpyArray &on = m["output_neuron_idx"], &ib = m["input_block_idx"], &in = m["input_neuron_idx"],
-                       &ic = m["input_channel_offset"], &wt = m["weight"];
-        const int64_t E = on.count();
-        if (E != syn[i + 1] - syn[i] || ib.count() != E || in.count() != E || ic.count() != E || wt.count() != 2 * E) {
-            rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: inconsistent synapse array lengths", i);
-            break;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int workers = (int)std::min<size_t>(F, std::min(8u, hw));
+    std::atomic<size_t> next_file{0};
+    std::atomic<int> wstatus{rc};
+    std::mutex err_mu;
+    std::string werr;
+    std::vector<int64_t> wmax_in((size_t)workers, 0);
+    auto report = [&](int code, const std::string& msg) {
+        std::lock_guard<std::mutex> lk(err_mu);
+        if (wstatus.load() == DTB_OK) { werr = msg; wstatus.store(code); }
+    };
+    auto work = [&](int w) {
+        if (cudaSetDevice(device) != cudaSuccess) { report(DTB_ERR_CUDA, "cudaSetDevice in a loader thread"); return; }
+        char msg[256];
+        for (;;) {
+            if (wstatus.load() != DTB_OK) return;
+            const size_t i = next_file.fetch_add(1);
+            if (i >= F) return;
+            std::map<std::string, NpyArray> m;
+            std::string err;
+            if (!npz_read(paths[i], m, err, &syn_names)) { report(DTB_ERR_FORMAT, err); return; }
+            for (auto& nm : syn_names)
+                if (!m.count(nm)) {
+                    std::snprintf(msg, sizeof(msg), "block_%zu.npz: missing %s", i, nm.c_str());
+                    report(DTB_ERR_FORMAT, msg);
+                    return;
+                }
+            const NpyArray &on = m["output_neuron_idx"], &ib = m["input_block_idx"], &in = m["input_neuron_idx"],
+                           &ic = m["input_channel_offset"], &wt = m["weight"];
+            const int64_t E = on.count();
+            if (E != syn[i + 1] - syn[i] || ib.count() != E || in.count() != E || ic.count() != E || wt.count() != 2 * E) {
+                std::snprintf(msg, sizeof(msg), "block_%zu.npz: inconsistent synapse array lengths", i);
+                report(DTB_ERR_FORMAT, msg);
+                return;
+            }
+            if (on.descr != "<u4" || in.descr != "<u4" || ib.descr != "<i2" || ic.descr != "|u1" || wt.descr != "<f4") {
+                std::snprintf(msg, sizeof(msg), "block_%zu.npz: unexpected synapse dtypes", i);
+                report(DTB_ERR_FORMAT, msg);
+                return;
+            }
+            const uint32_t* onp = reinterpret_cast<const uint32_t*>(on.data.data());
+            const int16_t* ibp = reinterpret_cast<const int16_t*>(ib.data.data());
+            const uint32_t* inp = reinterpret_cast<const uint32_t*>(in.data.data());
+            const uint8_t* icp = reinterpret_cast<const uint8_t*>(ic.data.data());
+            const float* wtp = reinterpret_cast<const float*>(wt.data.data());
+            // stable counting sort of this file's entries into its rows (file order inside a row)
+            const int64_t n_i = bases[i + 1] - bases[i];
+            std::vector<int64_t> cur((size_t)n_i + 1, 0);
+            for (int64_t e = 0; e < E; ++e) {
+                if ((int64_t)onp[e] >= n_i) {
+                    std::snprintf(msg, sizeof(msg), "block_%zu.npz: neuron index out of range", i);
+                    report(DTB_ERR_FORMAT, msg);
+                    return;
+                }
+                cur[(size_t)onp[e] + 1]++;
+            }
+            for (int64_t r = 0; r < n_i; ++r) {
+                wmax_in[(size_t)w] = std::max<int64_t>(wmax_in[(size_t)w], cur[(size_t)r + 1]);
+                cur[(size_t)r + 1] += cur[(size_t)r];
+                rp[(size_t)(bases[i] + r + 1)] = syn[i] + cur[(size_t)r + 1];
+            }
+            std::vector<uint32_t> col((size_t)E);
+            std::vector<float2> val((size_t)E);
+            for (int64_t e = 0; e < E; ++e) {
+                const int64_t sb = (int64_t)i + ibp[e];
+                const bool ok = sb >= 0 && sb < (int64_t)F && bases[(size_t)sb] + inp[e] < bases[(size_t)sb + 1] &&
+                                (icp[e] == 0 || icp[e] == 2);
+                if (!ok) {
+                    std::snprintf(msg, sizeof(msg), "block_%zu.npz: synapse %lld: %s", i, (long long)e,
+                                  (sb < 0 || sb >= (int64_t)F) ? "input_block_idx out of range"
+                                  : (icp[e] != 0 && icp[e] != 2) ? "input_channel_offset must be 0 or 2"
+                                                                 : "neuron index out of range");
+                    report(DTB_ERR_FORMAT, msg);
+                    return;
+                }
+                const int64_t pr = bases[(size_t)sb] + inp[e];
+                const int64_t d = cur[onp[e]]++;
+                col[(size_t)d] = (uint32_t)pr | (icp[e] ? kKindBit : 0u);
+                val[(size_t)d] = make_float2(wtp[2 * e], wtp[2 * e + 1]);
+            }
+            if (E > 0) {
+                cudaError_t e1 = cudaMemcpy(pcol + syn[i], col.data(), 4 * (size_t)E, cudaMemcpyHostToDevice);
+                if (e1 == cudaSuccess) e1 = cudaMemcpy(pw + syn[i], val.data(), 8 * (size_t)E, cudaMemcpyHostToDevice);
+                if (e1 != cudaSuccess) { report(DTB_ERR_CUDA, std::string("synapse upload: ") + cudaGetErrorString(e1)); return; }
+            }
         }
-        if (on.descr != "<u4" || in.descr != "<u4" || ib.descr != "<i2" || ic.descr != "|u1" || wt.descr != "<f4") {
-            rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: unexpected synapse dtypes", i);
-            break;
-        }
-        const uint32_t* onp = reinterpret_cast<const uint32_t*>(on.data.data());
-        const int16_t* ibp = reinterpret_cast<const int16_t*>(ib.data.data());
-        const uint32_t* inp = reinterpret_cast<const uint32_t*>(in.data.data());
-        const uint8_t* icp = reinterpret_cast<const uint8_t*>(ic.data.data());
-        const float* wtp = reinterpret_cast<const float*>(wt.data.data());
-        // stable counting sort of this file's entries into its rows (file order inside a row)
-        const int64_t n_i = bases[i + 1] - bases[i];
-        std::vector<int64_t> cur((size_t)n_i + 1, 0);
-        for (int64_t e = 0; e < E; ++e) {
-            if ((int64_t)onp[e] >= n_i) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: neuron index out of range", i); break; }
-            cur[(size_t)onp[e] + 1]++;
-        }
-        if (rc != DTB_OK) break;
-        for (int64_t r = 0; r < n_i; ++r) {
-            b->max_in = std::max<int64_t>(b->max_in, cur[(size_t)r + 1]);
-            cur[(size_t)r + 1] += cur[(size_t)r];
-            rp[(size_t)(bases[i] + r + 1)] = syn[i] + cur[(size_t)r + 1];
-        }
-        std::vector<uint32_t> col((size_t)E);
-        std::vector<float2> val((size_t)E);
-        for (int64_t e = 0; e < E; ++e) {
-            const int64_t sb = (int64_t)i + ibp[e];
-            if (sb < 0 || sb >= (int64_t)F) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: input_block_idx out of range", i); break; }
-            const int64_t pr = bases[(size_t)sb] + inp[e];
-            if (pr >= bases[(size_t)sb + 1]) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: neuron index out of range", i); break; }
-            if (icp[e] != 0 && icp[e] != 2) { rc = fail(DTB_ERR_FORMAT, "block_%zu.npz: input_channel_offset must be 0 or 2", i); break; }
-            const int64_t d = cur[onp[e]]++;
-            col[(size_t)d] = (uint32_t)pr | (icp[e] ? kKindBit : 0u);
-            val[(size_t)d] = make_float2(wtp[2 * e], wtp[2 * e + 1]);
-            if (build_push) outdeg[(size_t)pr]++;
-        }
-        if (rc != DTB_OK) break;
-        if (E > 0) {
-            cudaError_t e1 = cudaMemcpy(pcol + syn[i], col.data(), 4 * (size_t)E, cudaMemcpyHostToDevice);
-            if (e1 == cudaSuccess) e1 = cudaMemcpy(pw + syn[i], val.data(), 8 * (size_t)E, cudaMemcpyHostToDevice);
-            if (e1 != cudaSuccess) rc = fail(DTB_ERR_CUDA, "synapse upload: %s", cudaGetErrorString(e1));
-        }
+    };
+    if (rc == DTB_OK) {
+        std::vector<std::thread> pool;
+        for (int w = 1; w < workers; ++w) pool.emplace_back(work, w);
+        work(0);
+        for (auto& t : pool) t.join();
+        cudaSetDevice(device);
+        if (wstatus.load() != DTB_OK) rc = fail(wstatus.load(), "%s", werr.c_str());
+        for (int64_t v : wmax_in) b->max_in = std::max(b->max_in, v);
     }
     if (rc == DTB_OK) {
         cudaError_t e1 = cudaMemcpy(prow, rp.data(), sizeof(int64_t) * rp.size(), cudaMemcpyHostToDevice);
@@ -1559,8 +1604,12 @@ int dtb_block_create_from_npz(const char* dir, float dt, uint64_t seed, uint32_t
     if (rc == DTB_OK && build_push) {
         rc = dalloc(b, &counts, (size_t)N + 1);
         if (rc == DTB_OK) {
-            cudaError_t e1 = cudaMemcpy(counts, outdeg.data(), sizeof(uint32_t) * outdeg.size(), cudaMemcpyHostToDevice);
-            if (e1 != cudaSuccess) rc = fail(DTB_ERR_CUDA, "out-degree upload: %s", cudaGetErrorString(e1));
+            cudaError_t e1 = cudaMemsetAsync(counts, 0, sizeof(uint32_t) * ((size_t)N + 1), b->stream);
+            if (e1 == cudaSuccess && S > 0) {
+                k_count_outdeg<<<grid_for(S, 256), 256, 0, b->stream>>>(S, pcol, counts);
+                e1 = cudaGetLastError();
+            }
+            if (e1 != cudaSuccess) rc = fail(DTB_ERR_CUDA, "out-degree count: %s", cudaGetErrorString(e1));
         }
         if (rc == DTB_OK) rc = build_push_device(b, counts, b->max_in <= 65535);
     }
@@ -1775,6 +1824,10 @@ int dtb_block_set_tuning(dtb_block* b, int key, int64_t value)
         if (value < 0 || value > 4) return fail(DTB_ERR_ARG, "step variant must be 0..4");
         b->step_variant = (int)value;
         break;
+    case DTB_TUNE_SCATTER_REVERSE:
+        if (value < 0 || value > 1) return fail(DTB_ERR_ARG, "scatter order must be 0 (forward) or 1 (reverse)");
+        b->ds.rev_scatter = (int)value;
+        break;
     case DTB_TUNE_STAGE_WAIT_LIMIT:
         if (value < 0 || value > 0x7fffffffLL) return fail(DTB_ERR_ARG, "stage wait limit must be 0..2^31-1");
         b->ds.stage_wait_limit = (uint32_t)value;
@@ -1823,6 +1876,7 @@ int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value)
     case DTB_TUNE_SCATTER_VARIANT: *value = b->scatter_variant; break;
     case DTB_TUNE_PUSH_METHOD: *value = b->push_method; break;
     case DTB_TUNE_STAGE_WAIT_LIMIT: *value = b->ds.stage_wait_limit; break;
+    case DTB_TUNE_SCATTER_REVERSE: *value = b->ds.rev_scatter; break;
     case DTB_TUNE_BIN_WORDS: *value = b->bin_words; break;
     case DTB_TUNE_BIN_CAPACITY: *value = b->bin_cap_per_neuron; break;
     case DTB_TUNE_BIN_SHIFT: *value = b->ds.bin_cnt ? b->ds.bin_shift : bin_shift_for(b); break;
@@ -1864,13 +1918,20 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
             }
         b->scatter_wpw = best_w;
         b->scatter_variant = best_sv;
-        {   // J lines kept in L2 for the scatter vs streamed
-            const int keep = b->ds.j_keep;
-            b->ds.j_keep = 1 - keep;
-            float o[4];
-            RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PUSH, o));
-            if (o[2] < best_ms) { best_ms = o[2]; ev = o[3]; }
-            else b->ds.j_keep = keep;
+        {   // J lines kept in L2 for the scatter vs streamed, scatter order forward vs reverse
+            const int keep0 = b->ds.j_keep, rev0 = b->ds.rev_scatter;
+            int bk = keep0, br = rev0;
+            for (int keep = 0; keep < 2; ++keep)
+                for (int rev = 0; rev < 2; ++rev) {
+                    if (keep == keep0 && rev == rev0) continue;
+                    b->ds.j_keep = keep;
+                    b->ds.rev_scatter = rev;
+                    float o[4];
+                    RET(dtb_block_time_kernels(b, n_steps, noise_rate, 0, DTB_MODE_PUSH, o));
+                    if (o[2] < best_ms) { best_ms = o[2]; ev = o[3]; bk = keep; br = rev; }
+                }
+            b->ds.j_keep = bk;
+            b->ds.rev_scatter = br;
         }
         // binned push: update register budget x scatter round size, kept when faster
         b->push_method = pm0;

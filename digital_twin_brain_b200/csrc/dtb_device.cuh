@@ -97,6 +97,7 @@ struct DevState {
     int64_t j_ps;               // plane stride (float2 units): N for the split layout, 1 for [N][4]
     int64_t j_es;               // neuron stride (float2 units): 1 for the split layout, 2 for [N][4]
     int j_keep;                 // J stores at normal L2 priority (else evict-first)
+    int rev_scatter;            // the atomic scatter walks the bitmask from its end
     float* tlast;
     float* isyn_override;       // [N] used once after update_property
     const uint32_t* cls;

@@ -106,44 +106,62 @@ static bool inflate_raw(const unsigned char* src, size_t n, std::vector<char>& d
     return true;
 }
 
+// Reads [off, off + n) of f into dst; false on a short read.
+static bool read_at(FILE* f, uint64_t off, size_t n, void* dst)
+{
+    if (fseeko(f, (off_t)off, SEEK_SET) != 0) return false;
+    return n == 0 || std::fread(dst, 1, n, f) == n;
+}
+
 bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std::string& err,
               const std::vector<std::string>* only, std::vector<std::string>* names)
 {
+    // Only the archive's tail, its central directory and the wanted members are read.
     FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) { err = "cannot open " + path; return false; }
-    std::fseek(f, 0, SEEK_END);
-    const long long fsize = std::ftell(f);
-    std::fseek(f, 0, SEEK_SET);
-    if (fsize < 22) { std::fclose(f); err = "file too small for a zip archive: " + path; return false; }
-    std::vector<unsigned char> file((size_t)fsize);
-    if (std::fread(file.data(), 1, file.size(), f) != file.size()) { std::fclose(f); err = "read failed: " + path; return false; }
-    std::fclose(f);
-    const unsigned char* b = file.data();
-    // end of central directory
+    struct Closer { FILE* f; ~Closer() { std::fclose(f); } } closer{f};
+    fseeko(f, 0, SEEK_END);
+    const uint64_t fsize = (uint64_t)ftello(f);
+    if (fsize < 22) { err = "file too small for a zip archive: " + path; return false; }
+    // end of central directory (within the last 64 KB + its 22 bytes)
+    const uint64_t tail_n = std::min<uint64_t>(fsize, 22 + 65535 + 20);
+    std::vector<unsigned char> tail((size_t)tail_n);
+    if (!read_at(f, fsize - tail_n, (size_t)tail_n, tail.data())) { err = "read failed: " + path; return false; }
     long long eocd = -1;
-    for (long long i = fsize - 22; i >= 0 && i >= fsize - 22 - 65535; --i) {
-        if (rd32(b + i) == 0x06054b50u) { eocd = i; break; }
-    }
+    for (long long k = (long long)tail_n - 22; k >= 0; --k)
+        if (rd32(tail.data() + k) == 0x06054b50u) { eocd = k; break; }
     if (eocd < 0) { err = "no end-of-central-directory record: " + path; return false; }
-    uint64_t n_entries = rd16(b + eocd + 10);
-    uint64_t cd_off = rd32(b + eocd + 16);
-    if (eocd >= 20 && rd32(b + eocd - 20) == 0x07064b50u) {  // zip64 locator
-        const uint64_t z64 = rd64(b + eocd - 20 + 8);
-        if (z64 + 56 > (uint64_t)fsize || rd32(b + z64) != 0x06064b50u) { err = "bad zip64 record: " + path; return false; }
-        n_entries = rd64(b + z64 + 32);
-        cd_off = rd64(b + z64 + 48);
+    const unsigned char* e = tail.data() + eocd;
+    uint64_t n_entries = rd16(e + 10);
+    uint64_t cd_size = rd32(e + 12);
+    uint64_t cd_off = rd32(e + 16);
+    if (eocd >= 20 && rd32(e - 20) == 0x07064b50u) {  // zip64 locator
+        const uint64_t z64 = rd64(e - 20 + 8);
+        unsigned char z[56];
+        if (z64 + 56 > fsize || !read_at(f, z64, 56, z) || rd32(z) != 0x06064b50u) {
+            err = "bad zip64 record: " + path;
+            return false;
+        }
+        n_entries = rd64(z + 32);
+        cd_size = rd64(z + 40);
+        cd_off = rd64(z + 48);
     }
-    uint64_t p = cd_off;
-    for (uint64_t e = 0; e < n_entries; ++e) {
-        if (p + 46 > (uint64_t)fsize || rd32(b + p) != 0x02014b50u) { err = "bad central directory: " + path; return false; }
-        const int method = rd16(b + p + 10);
-        const uint32_t crc_expect = rd32(b + p + 16);
-        uint64_t csize = rd32(b + p + 20), usize = rd32(b + p + 24);
-        const int nlen = rd16(b + p + 28), xlen = rd16(b + p + 30), clen = rd16(b + p + 32);
-        uint64_t loff = rd32(b + p + 42);
-        std::string name(reinterpret_cast<const char*>(b + p + 46), nlen);
+    if (cd_off + cd_size > fsize) { err = "bad central directory: " + path; return false; }
+    std::vector<unsigned char> cd((size_t)cd_size);
+    if (!read_at(f, cd_off, (size_t)cd_size, cd.data())) { err = "read failed: " + path; return false; }
+    uint64_t p = 0;
+    for (uint64_t k = 0; k < n_entries; ++k) {
+        if (p + 46 > cd_size || rd32(cd.data() + p) != 0x02014b50u) { err = "bad central directory: " + path; return false; }
+        const unsigned char* c = cd.data() + p;
+        const int method = rd16(c + 10);
+        const uint32_t crc_expect = rd32(c + 16);
+        uint64_t csize = rd32(c + 20), usize = rd32(c + 24);
+        const int nlen = rd16(c + 28), xlen = rd16(c + 30), clen = rd16(c + 32);
+        uint64_t loff = rd32(c + 42);
+        if (p + 46 + (uint64_t)nlen + xlen > cd_size) { err = "bad central directory: " + path; return false; }
+        std::string name(reinterpret_cast<const char*>(c + 46), nlen);
         // zip64 extra field: present values replace the 0xffffffff markers in order
-        const unsigned char* x = b + p + 46 + nlen;
+        const unsigned char* x = c + 46 + nlen;
         for (int q = 0; q + 4 <= xlen;) {
             const int id = rd16(x + q), sz = rd16(x + q + 2);
             if (id == 0x0001) {
@@ -155,25 +173,33 @@ bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std
             q += 4 + sz;
         }
         p += 46 + (uint64_t)nlen + xlen + clen;
-        {
-            std::string key = name;
-            if (key.size() > 4 && key.compare(key.size() - 4, 4, ".npy") == 0) key = key.substr(0, key.size() - 4);
-            if (names) names->push_back(key);
-            if (only && std::find(only->begin(), only->end(), key) == only->end()) continue;
+        std::string key = name;
+        if (key.size() > 4 && key.compare(key.size() - 4, 4, ".npy") == 0) key = key.substr(0, key.size() - 4);
+        if (names) names->push_back(key);
+        if (only && std::find(only->begin(), only->end(), key) == only->end()) continue;
+        unsigned char lh[30];
+        if (loff + 30 > fsize || !read_at(f, loff, 30, lh) || rd32(lh) != 0x04034b50u) {
+            err = "bad local header: " + name;
+            return false;
         }
-        if (loff + 30 > (uint64_t)fsize || rd32(b + loff) != 0x04034b50u) { err = "bad local header: " + name; return false; }
-        const uint64_t data = loff + 30 + rd16(b + loff + 26) + rd16(b + loff + 28);
-        if (data + csize > (uint64_t)fsize) { err = "truncated member: " + name; return false; }
-        std::vector<char> raw;
+        const uint64_t data = loff + 30 + rd16(lh + 26) + rd16(lh + 28);
+        if (data + csize > fsize) { err = "truncated member: " + name; return false; }
+        std::vector<char> raw((size_t)csize);
+        if (!read_at(f, data, (size_t)csize, raw.data())) { err = "read failed: " + name; return false; }
+        std::vector<char> inflated;
         const char* buf;
         size_t blen;
         if (method == 0) {
-            buf = reinterpret_cast<const char*>(b + data);
-            blen = (size_t)csize;
-        } else if (method == 8) {
-            if (!inflate_raw(b + data, (size_t)csize, raw, (size_t)usize, err)) { err += ": " + name; return false; }
             buf = raw.data();
             blen = raw.size();
+        } else if (method == 8) {
+            if (!inflate_raw(reinterpret_cast<const unsigned char*>(raw.data()), raw.size(), inflated, (size_t)usize,
+                             err)) {
+                err += ": " + name;
+                return false;
+            }
+            buf = inflated.data();
+            blen = inflated.size();
         } else {
             err = "unsupported zip compression method in " + name;
             return false;
@@ -188,8 +214,6 @@ bool npz_read(const std::string& path, std::map<std::string, NpyArray>& out, std
             }
             if ((uint32_t)crc != crc_expect) { err = "CRC-32 mismatch (corrupt member): " + name; return false; }
         }
-        std::string key = name;
-        if (key.size() > 4 && key.compare(key.size() - 4, 4, ".npy") == 0) key = key.substr(0, key.size() - 4);
         NpyArray a;
         if (!npy_parse(buf, blen, a, err)) { err += " (" + name + ")"; return false; }
         out[key] = std::move(a);

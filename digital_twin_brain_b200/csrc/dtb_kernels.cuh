@@ -1079,7 +1079,10 @@ __global__ void __launch_bounds__(kScatterThreads, MINB) k_scatter(DevState s, i
     const uint32_t* __restrict__ bits = s.bits[(steps_done - 1ull) & 1ull];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
-    const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    // rev_scatter: CTAs take the bitmask from its end, so that the first rows scattered
+    // target the neurons the update wrote last, whose J lines may still be in L2
+    const int64_t bid = s.rev_scatter ? (int64_t)(gridDim.x - 1u - blockIdx.x) : (int64_t)blockIdx.x;
+    const int64_t warp_global = (bid * blockDim.x + threadIdx.x) >> 5;
     const int64_t w0 = warp_global * wpw;
     uint32_t* rows = sh_rows_dyn + (size_t)wid * wpw * 32;
     uint32_t word = (lane < wpw && w0 + lane < s.n_words) ? __ldcs(bits + w0 + lane) : 0u;

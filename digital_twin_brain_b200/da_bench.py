@@ -61,19 +61,20 @@ def main(argv=None, quiet: bool = False) -> dict:
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--train-sigma", type=float, default=2.0,
                     help="random-walk variance of the training ensemble (wider than the DA walk for coverage)")
-    ap.add_argument("--train-source", default="da", choices=["da", "walk"],
+    ap.add_argument("--train-source", default="both", choices=["da", "walk", "both"],
                     help="da: training windows from an assimilation run against another hidden truth (its "
-                         "analysis steps move the parameters as the served run's do); walk: a random-walk ensemble")
+                         "analysis steps move the parameters as the served run's do); walk: a random-walk "
+                         "ensemble; both: the two sets together")
     ap.add_argument("--threshold", type=float, default=None,
                     help="judge fallback threshold (default: --margin x the held-out judge error of the surrogate)")
-    ap.add_argument("--margin", type=float, default=1.5)
+    ap.add_argument("--margin", type=float, default=2.0)
     ap.add_argument("--burn-in-windows", type=int, default=1,
                     help="judge windows before the assimilation (histories, surrogate adaptation); timed")
     ap.add_argument("--spread", type=int, default=0,
                     help="give the surrogate members' rates the judges' residual spread")
     ap.add_argument("--bias-correct", type=int, default=0,
                     help="correct the surrogate members' BOLD by the judges' simulated-minus-surrogate mean")
-    ap.add_argument("--adapt-steps", type=int, default=20,
+    ap.add_argument("--adapt-steps", type=int, default=60,
                     help="Adam steps per window on the judges' windows (0: the surrogate stays as trained)")
     ap.add_argument("--gain", type=float, default=2.0,
                     help="excitatory g_ui of the template as a multiple of the single-block values (2.0: ~6 Hz)")
@@ -127,15 +128,17 @@ def main(argv=None, quiet: bool = False) -> dict:
     # ---- surrogate training windows: an assimilation run against another hidden truth, or a
     #      separate random-walk ensemble
     t0 = time.perf_counter()
-    if a.train_source == "da":
+    sets = []
+    if a.train_source in ("da", "both"):
         hp_train = torch.from_numpy(np.random.default_rng(a.seed + 31).uniform(0.6, 1.4, (template.R, 4))
                                     .astype(np.float32)).to(dev)
         obs_train = observe(template, hp_train, a.train_windows, {**base, "seed": a.seed + 11}, a.seed + 13)
-        g, h, tgt = collect_da_windows(template, DAConfig(n_members=a.members, **{**base, "seed": a.seed + 7}),
-                                       obs_train)
-    else:
-        g, h, tgt = collect_windows(template, DAConfig(n_members=a.members, hp_sigma=a.train_sigma,
-                                                       **{**base, "seed": a.seed + 7}), windows=a.train_windows)
+        sets.append(collect_da_windows(template, DAConfig(n_members=a.members, **{**base, "seed": a.seed + 7}),
+                                       obs_train))
+    if a.train_source in ("walk", "both"):
+        sets.append(collect_windows(template, DAConfig(n_members=a.members, hp_sigma=a.train_sigma,
+                                                       **{**base, "seed": a.seed + 17}), windows=a.train_windows))
+    g, h, tgt = (torch.cat([x[i] for x in sets]) for i in range(3))
     t_collect = time.perf_counter() - t0
     n = g.shape[0]
     perm = torch.from_numpy(np.random.default_rng(a.seed).permutation(n))

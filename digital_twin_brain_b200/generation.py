@@ -42,3 +42,21 @@ def write_blocks(directory: str, property: np.ndarray, bounds, post, pre, kind, 
                  input_neuron_idx=np.ascontiguousarray(pre[sel] - bounds[pop_pre[sel]], np.uint32),
                  input_channel_offset=np.ascontiguousarray(kind[sel], np.uint8),
                  weight=np.ascontiguousarray(weight[sel], np.float32))
+
+
+def write_population(directory: str, i: int, bounds, property_rows: np.ndarray, post_local, pre, kind, weight):
+    """Write population i alone as block_i.npz (the layout of write_blocks), from its synapses:
+    post_local (postsynaptic index inside the population, in the order to keep), pre (global
+    presynaptic index), kind, weight [E,2].  Writing a large network population by population
+    keeps host memory at one population's synapses."""
+    os.makedirs(directory, exist_ok=True)
+    bounds = np.asarray(bounds, np.int64)
+    pre = np.asarray(pre, np.int64)
+    pop_pre = np.searchsorted(bounds, pre, side="right") - 1
+    np.savez(os.path.join(directory, f"block_{i}"),
+             property=np.ascontiguousarray(property_rows, np.float32),
+             output_neuron_idx=np.ascontiguousarray(post_local, np.uint32),
+             input_block_idx=np.ascontiguousarray(pop_pre - i, np.int16),
+             input_neuron_idx=np.ascontiguousarray(pre - bounds[pop_pre], np.uint32),
+             input_channel_offset=np.ascontiguousarray(kind, np.uint8),
+             weight=np.ascontiguousarray(np.asarray(weight, np.float32).reshape(-1, 2)))

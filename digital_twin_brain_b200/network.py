@@ -126,6 +126,12 @@ class Network:
     def synchronize(self):
         _lib.call("dtb_block_synchronize", self._h)
 
+    def _torch_ready(self):
+        """Before the library writes into (or reads) torch device memory on its own stream: torch's
+        caching allocator may have handed out memory that work still queued on torch's current
+        stream uses, so that work must finish first."""
+        torch.cuda.current_stream(self.device).synchronize()
+
     # ------------------------------------------------------------ stepping
     def run(self, n_steps: int, noise_rate: float | None = 0.01, isolated: bool = False, mode: str = "auto",
             out: str = "host"):
@@ -143,6 +149,7 @@ class Network:
             s = torch.empty((n_steps, self.n_sub), dtype=torch.float32, device=dev)
             mn = torch.empty((n_steps, self.n_sub), dtype=torch.float32, device=dev)
             na = torch.empty((n_steps,), dtype=torch.int32, device=dev)
+            self._torch_ready()
             _lib.call("dtb_block_run", self._h, int(n_steps), rate, int(bool(isolated)), m, _ptr(s), _ptr(mn),
                       _ptr(na), DTB_DEVICE)
             self.synchronize()
@@ -183,7 +190,9 @@ class Network:
         return dict(scatter_words=int(r[0]), push_ms=float(r[1]), pull_ms=float(r[2]), activity=float(r[3]),
                     pull_threshold=float(r[4]), step_variant=int(r[5]),
                     j_cache=self.get_tuning(_lib.TUNE_J_CACHE),
-                    scatter_variant=self.get_tuning(_lib.TUNE_SCATTER_VARIANT))
+                    scatter_variant=self.get_tuning(_lib.TUNE_SCATTER_VARIANT),
+                    scatter_reverse=self.get_tuning(_lib.TUNE_SCATTER_REVERSE),
+                    push_method=self.get_tuning(_lib.TUNE_PUSH_METHOD))
 
     def step_forced(self, forced_active=None, forced_new_active=None, noise_rate: float | None = 0.01,
                     isolated: bool = False, mode: str = "pull"):
@@ -216,6 +225,7 @@ class Network:
         shape = (rows, self.N) if rows > 1 else (self.N,)
         if device:
             out = torch.empty(shape, dtype=_TORCH[dt], device=torch.device("cuda", self.device))
+            self._torch_ready()
             _lib.call("dtb_block_get", self._h, field, _ptr(out), DTB_DEVICE)
             self.synchronize()
             return out
@@ -244,6 +254,7 @@ class Network:
             dev = torch.device("cuda", self.device)
             ix = torch.empty(count, dtype=torch.int32, device=dev)
             w = torch.empty((count, 2), dtype=torch.float32, device=dev) if weights else None
+            self._torch_ready()
             _lib.call("dtb_block_get_csr_entries", self._h, which_i, int(first), int(count), _ptr(ix), _ptr(w),
                       DTB_DEVICE)
             self.synchronize()
@@ -326,6 +337,7 @@ class Network:
         idx = {"s": 0, "q": 1, "v": 2, "f_in": 3, "bold": 4, "act": 5}[field]
         if device:
             out = torch.empty(self.n_regions, dtype=torch.float64, device=torch.device("cuda", self.device))
+            self._torch_ready()
             _lib.call("dtb_block_get_bold", self._h, idx, _ptr(out), DTB_DEVICE)
             self.synchronize()
             return out
@@ -361,7 +373,9 @@ class Network:
             sp = torch.empty((rows.value, n), dtype=torch.uint8, device=dev)
             v = torch.empty((rows.value, n), dtype=torch.float32, device=dev)
             if rows.value and n:
+                self._torch_ready()
                 _lib.call("dtb_block_get_samples", self._h, _ptr(sp), _ptr(v), ctypes.byref(rows), DTB_DEVICE)
+                self.synchronize()
             return sp, v
         sp = np.empty((rows.value, n), np.uint8)
         v = np.empty((rows.value, n), np.float32)

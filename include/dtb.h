@@ -250,6 +250,9 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  * DTB_TUNE_BIN_CAPACITY    binned push: bin entries per neuron of the bin
  *                          (1..1024, default 8; 10 bytes each); reallocates
  * DTB_TUNE_BIN_SHIFT       binned push: B (10..13), 0 = chosen from N (11 from 8M neurons, else 10); reallocates
+ * DTB_TUNE_SCATTER_REVERSE atomic push scatter: 0 = CTAs take the bitmask from its start,
+ *                          1 = from its end (the rows scattered first then target the
+ *                          neurons whose J the update wrote last)
  * DTB_TUNE_STAGE_WAIT_LIMIT polls of a staged copy's completion barrier before the
  *                          update gives up on it (default 2^20; 0 gives up at once, for
  *                          tests): the update then loads that state from global memory,
@@ -259,7 +262,7 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
 enum { DTB_TUNE_SCATTER_WORDS = 0, DTB_TUNE_CHUNK = 1, DTB_TUNE_PULL_THRESHOLD_PPM = 2, DTB_TUNE_USE_GRAPHS = 3,
        DTB_TUNE_STEP_VARIANT = 4, DTB_TUNE_PULL_METHOD = 5, DTB_TUNE_J_CACHE = 6, DTB_TUNE_SCATTER_VARIANT = 7,
        DTB_TUNE_PUSH_METHOD = 8, DTB_TUNE_BIN_WORDS = 9, DTB_TUNE_BIN_CAPACITY = 10, DTB_TUNE_BIN_SHIFT = 11,
-       DTB_TUNE_STAGE_WAIT_LIMIT = 12 };
+       DTB_TUNE_STAGE_WAIT_LIMIT = 12, DTB_TUNE_SCATTER_REVERSE = 13 };
 int dtb_block_set_tuning(dtb_block* b, int key, int64_t value);
 int dtb_block_get_tuning(dtb_block* b, int key, int64_t* value);
 

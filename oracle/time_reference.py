@@ -13,7 +13,9 @@ import torch
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 sys.path = [p for p in sys.path if os.path.abspath(p or ".") != HERE]   # the package, not this folder
-REF = os.environ.get("DTB_REFERENCE", "/root/reference")
+REF = os.environ.get("DTB_REFERENCE")   # the reference checkout (yeyeleijun/Digital_twin_brain)
+if not REF or not os.path.isdir(REF):
+    sys.exit("set DTB_REFERENCE to a checkout of the reference, e.g. DTB_REFERENCE=/path/to/Digital_twin_brain python oracle/time_reference.py")
 sys.path.insert(0, ROOT)
 sys.path.insert(0, REF)
 

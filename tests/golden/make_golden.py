@@ -1,14 +1,14 @@
 """Generate the golden fixtures from the reference's own Python code.
 
-Runs only where the reference checkout is available (default
-/root/reference, or $DTB_REFERENCE).  For each case it writes the network in
+Runs only where a checkout of the reference is available, named by
+$DTB_REFERENCE.  For each case it writes the network in
 the reference's block_{i}.npz layout, loads it with the reference's
 generation/read_block.py:connect_for_block, and steps the reference's
 models/block.py:block with torch.rand replaced by the Philox4x32-10 noise
 stream (oracle/philox layout), recording the per-step results.  The BOLD
 fixture runs models/bold_model_pytorch.py:BOLD directly.
 
-    python tests/golden/make_golden.py
+    DTB_REFERENCE=/path/to/Digital_twin_brain python tests/golden/make_golden.py
 
 Outputs (committed): tests/golden/*.npz and tests/golden/small_blocks/.
 """
@@ -24,7 +24,9 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("DTB_REFERENCE", "/root/reference")
+REF = os.environ.get("DTB_REFERENCE")   # the reference checkout (yeyeleijun/Digital_twin_brain)
+if not REF or not os.path.isdir(REF):
+    sys.exit("set DTB_REFERENCE to a checkout of the reference, e.g. DTB_REFERENCE=/path/to/Digital_twin_brain python tests/golden/make_golden.py")
 sys.path.insert(0, ROOT)
 sys.path.insert(0, REF)
 

@@ -178,16 +178,19 @@ def test_autotune_and_tuning_knobs():
         net.set_tuning(TUNE_SCATTER_WORDS, 0)
 
 
+@pytest.mark.parametrize("reverse", [0, 1])
 @pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("wpw", [1, 4, 32])
-def test_scatter_shapes_agree_with_pull_under_forcing(wpw, variant):
-    """One push step from identical state at several launch shapes and register budgets vs the
-    exact pull step."""
-    from digital_twin_brain_b200._lib import TUNE_PUSH_METHOD, TUNE_SCATTER_VARIANT, TUNE_SCATTER_WORDS
+def test_scatter_shapes_agree_with_pull_under_forcing(wpw, variant, reverse):
+    """One push step from identical state at several launch shapes, register budgets and scatter
+    orders vs the exact pull step."""
+    from digital_twin_brain_b200._lib import (TUNE_PUSH_METHOD, TUNE_SCATTER_REVERSE, TUNE_SCATTER_VARIANT,
+                                              TUNE_SCATTER_WORDS)
     spec = synthetic.single_block(8000, 100, name="n8k")
     a = Network.from_spec(spec, device=0)
     b = Network.from_spec(spec, device=0)
     a.set_tuning(TUNE_PUSH_METHOD, 1)     # the atomic scatter these shapes belong to
+    a.set_tuning(TUNE_SCATTER_REVERSE, reverse)
     a.set_tuning(TUNE_SCATTER_WORDS, wpw)
     a.set_tuning(TUNE_SCATTER_VARIANT, variant)
     for _ in range(80):
