@@ -260,7 +260,9 @@ def roofline_of(spec, kt, mode, push_method, pull_method, peaks):
     # V, J, t_last read, one class id per 128-neuron tile; V, J written; two bitmasks
     upd_bytes = N * (4 + 16 + 4 + 4 / 128) + N * (4 + 16) + 2 * N / 8
     prop_bytes = N / 8 + 16 * nact + 12 * evs                              # bitmask, row pointers, (post, w) of rows
-    ordered = mode == "pull" and pull_method != 1 and kt["propagate_ms"] > 0 and nact / N <= 0.1
+    # pull mode runs as ordered push with method 2 (slots) or 3 (masks), or when auto (0) picks
+    # slots at low activity (active fraction <= 0.1); rows (1) and streamed (4) are one fused kernel
+    ordered = mode == "pull" and (pull_method in (2, 3) or (pull_method in (0, -1) and nact / N <= 0.1))
     if mode == "push" and push_method == 2:
         # binned: the scatter also writes every event into its bin (u16 index + weight pair), the
         # update reads them back
@@ -322,7 +324,9 @@ def mlp_measure(dev, peaks) -> dict:
     """The surrogate network's tensor-core kernels (tcgen05, BF16 operands, FP32 accumulation) timed
     on the DA forecast batch (128 members x 90 regions) and a training minibatch, against the
     measured dense BF16 peak.  Algorithmic FLOPs count each multiply-add of the network once (the
-    kernels run three BF16 products per FP32 operand to keep FP32 accuracy)."""
+    kernels run three BF16 products per FP32 operand to keep FP32 accuracy).  `ms` is the device
+    time of one call's kernels (the call captured once in a CUDA graph and replayed: no host time
+    between launches); `ms_per_call` times the same calls issued one by one from Python."""
     import torch
     from digital_twin_brain_b200.surrogate import MLP
     torch.cuda.set_device(dev)
@@ -330,6 +334,7 @@ def mlp_measure(dev, peaks) -> dict:
     m = MLP(in_dim, H, seed=0, device=dev)
     g = torch.Generator(device=f"cuda:{dev}").manual_seed(0)
     out = {}
+    side = torch.cuda.Stream(device=dev)
     for name, B, fn in (("forward", 128 * 90, "fwd"), ("train_step", 4096, "train")):
         x = torch.randn(B, in_dim, device=f"cuda:{dev}", generator=g)
         t = torch.randn(B, device=f"cuda:{dev}", generator=g)
@@ -343,12 +348,30 @@ def mlp_measure(dev, peaks) -> dict:
             run()
         e1.record()
         torch.cuda.synchronize(dev)
-        ms = e0.elapsed_time(e1) / 20
+        ms_call = e0.elapsed_time(e1) / 20
+        graph = torch.cuda.CUDAGraph()
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            run()                                   # warm-up on the capture stream
+            side.synchronize()
+            with torch.cuda.graph(graph, stream=side):
+                run()
+        torch.cuda.synchronize(dev)
+        for _ in range(3):
+            graph.replay()
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(50):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / 50
+        del graph
         flops = 2.0 * B * (in_dim * H + H * H + H) * (1 if fn == "fwd" else 3)
         tf = flops / (ms * 1e-3) / 1e12
         peak = float(peaks.get("bf16_tflops", 1590.0))
-        out[name] = {"rows": B, "ms": ms, "tflops": tf, "peak_tflops": peak, "frac": tf / peak,
-                     "unit": "TFLOP/s", "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)"
+        out[name] = {"rows": B, "ms": ms, "ms_per_call": ms_call, "tflops": tf, "peak_tflops": peak,
+                     "frac": tf / peak, "unit": "TFLOP/s", "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)"
                      if "bf16_tflops" in peaks else "fallback 1590 TFLOP/s"}
     m.close()
     return out

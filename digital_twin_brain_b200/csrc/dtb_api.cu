@@ -679,10 +679,40 @@ static void launch_step_bins(dtb_block* b, const DevState& s)
     k_step<kGatherBins, U, F, M><<<grid, kStepThreads, smem, b->stream>>>(s, (int)cpc);
 }
 
+// The update with the bin fold and staged state loads: bins of 1024 neurons (one tile per
+// warp of a CTA per chunk), the events added into the tiles' staged J planes.
+template <bool F, int M>
+static void launch_step_bins_staged(dtb_block* b, const DevState& s)
+{
+    static int per_sm = 0;
+    if (!per_sm) {
+        cudaFuncSetAttribute(k_step<kGatherBins, true, F, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kBinStagedSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<kGatherBins, true, F, M, true>, kStepThreads,
+                                                      kBinStagedSmem);
+        if (per_sm < 1) per_sm = 1;
+    }
+    const int64_t nchunks = (b->N + ((int64_t)1 << kBinMinShift) - 1) >> kBinMinShift;
+    const int64_t maxb = (int64_t)std::max(1, b->n_sm) * per_sm;
+    const int64_t cpc = std::max<int64_t>(1, (nchunks + maxb - 1) / maxb);
+    const unsigned grid = (unsigned)std::max<int64_t>(1, (nchunks + cpc - 1) / cpc);
+    k_step<kGatherBins, true, F, M, true><<<grid, kStepThreads, kBinStagedSmem, b->stream>>>(s, (int)cpc);
+}
+
+static bool staged_layout(const DevState& s);
+
 template <int G, bool U, bool F>
 static void launch_step(dtb_block* b, const DevState& s)
 {
     if constexpr (G == kGatherBins) {
+        if constexpr (U) {
+            // step variants 2..4 stage the state (bins of 1024 neurons, split J planes)
+            if (b->step_variant >= 2 && s.bin_shift == kBinMinShift && staged_layout(s)) {
+                if (b->step_variant == 2) launch_step_bins_staged<F, 2>(b, s);
+                else launch_step_bins_staged<F, 3>(b, s);
+                return;
+            }
+        }
         if (b->step_variant == 1 || b->step_variant >= 3) launch_step_bins<U, F, 3>(b, s);
         else launch_step_bins<U, F, 2>(b, s);
         return;
@@ -782,13 +812,14 @@ static void drop_graphs(dtb_block* b)
 
 // ------------------------------------------------------------ binned push
 // Bin geometry: 2^B neurons per bin (the update's chunk), B >= 10 (one tile per warp of
-// the update CTA), 11 from 8M neurons (the scatter's window of kBinWin bins then spans
-// 2M neurons, more than a region), at most kBinMaxShift (the update's 16 << B bytes of
-// sums in shared memory).
+// the update CTA), at most kBinMaxShift (the unstaged update's 16 << B bytes of sums in
+// shared memory).  The default, 10, is the geometry of the staged update (its chunk's
+// eight tiles are the warps' stage buffers); the scatter's window of kBinWin bins then
+// spans 1M neurons.
 static int bin_shift_for(const dtb_block* b)
 {
     if (b->bin_shift_req) return b->bin_shift_req;
-    return b->N >= (int64_t)8 << 20 ? 11 : kBinMinShift;
+    return kBinMinShift;
 }
 
 // Bitmask words per scatter round: the round's synapses must stay below 2^31.
@@ -827,7 +858,7 @@ static int ensure_bins(dtb_block* b)
     const int B = bin_shift_for(b);
     const int64_t n_bins = (b->N + ((int64_t)1 << B) - 1) >> B;
     int64_t cap = (int64_t)b->bin_cap_per_neuron << B;
-    cap = std::min<int64_t>(cap, (int64_t)0xffffffffLL / n_bins);
+    cap = std::min<int64_t>(cap, (int64_t)0xffffffffLL / n_bins) & ~(int64_t)7;   // whole 16-byte units per bin
     const size_t entries = (size_t)n_bins * (size_t)cap;
     uint16_t* bi = nullptr; float2* bw = nullptr; uint32_t* bc = nullptr;
     int rc = dalloc(b, &bi, entries);
@@ -1933,15 +1964,17 @@ int dtb_block_autotune(dtb_block* b, int n_steps, float noise_rate, float* repor
             b->ds.j_keep = bk;
             b->ds.rev_scatter = br;
         }
-        // binned push: update register budget x scatter round size, kept when faster
+        // binned push: update variant (registers, staging) x scatter round size, kept when faster
         b->push_method = pm0;
         if (pm0 != 1 && bins_possible(b) && ensure_bins(b) == DTB_OK) {
             const int atomic_v = b->step_variant, atomic_words = b->bin_words;
             float best_b = 1e30f, ev_b = 0.0f;
             int bv = 0, bw = atomic_words;
             b->push_method = 2;
-            for (int v = 0; v < 2; ++v)
+            const bool stageable = staged_layout(b->ds) && b->ds.bin_shift == kBinMinShift;
+            for (int v = 0; v < 4; ++v)
                 for (int w : {64, 128, 256}) {
+                    if (v >= 2 && !stageable) continue;
                     b->step_variant = v;
                     b->bin_words = w;
                     float o[4];

@@ -410,6 +410,35 @@ __device__ __forceinline__ bool stage_wait(uint32_t mbar, uint32_t parity, uint3
 // of the CTA calls it (three barriers).
 constexpr int kFoldBatch = 8;   // entries per thread in flight
 
+// Staged bin fold (kGatherBins with staged state): the first kBinStageMax entries of the
+// next chunk's bin are bulk-copied into one of two shared buffers one chunk ahead (index
+// array, then weight pairs); entries past it are read from global memory by the fold.
+constexpr uint32_t kBinStageMax = 1216;                         // a multiple of 8 (16-byte copies)
+constexpr int kBinStageBytes = (int)kBinStageMax * 10;
+constexpr int kBinStagedSmem = kStagedSmem + 2 * kBinStageBytes;
+
+// entries of a bin with n_raw appended events that the staged copy covers
+__device__ __forceinline__ uint32_t bin_stage_n(const DevState& s, uint32_t n_raw)
+{
+    const uint32_t lst = kBinStageMax < (s.bin_cap & ~7u) ? kBinStageMax : (s.bin_cap & ~7u);
+    const uint32_t n = n_raw < s.bin_cap ? n_raw : s.bin_cap;
+    return n < lst ? n : lst;
+}
+
+// One thread: the copies of the first n entries of bin c (rounded up to whole 16-byte
+// units: the bin capacity is a multiple of 8) into buf, completion counted on mbar.
+__device__ __forceinline__ void stage_bin(const DevState& s, int64_t c, uint32_t n, unsigned char* buf, uint32_t mbar)
+{
+    const uint32_t nr = (n + 7u) & ~7u;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier generic reads of buf first
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mbar), "r"(nr * 10u) : "memory");
+    if (nr) {
+        const uint32_t d = smem_u32(buf);
+        stage_issue(d, s.bin_idx + c * (int64_t)s.bin_cap, nr * 2u, mbar);
+        stage_issue(d + kBinStageMax * 2u, s.bin_w + c * (int64_t)s.bin_cap, nr * 8u, mbar);
+    }
+}
+
 __device__ __forceinline__ void fold_bin(const DevState& s, int64_t c, float4* acc, uint32_t n_raw)
 {
     const int chunk_n = 1 << s.bin_shift;
@@ -459,10 +488,18 @@ __device__ __forceinline__ void fold_bin(const DevState& s, int64_t c, float4* a
 // subblock, so the CTA-wide barrier and the done-count happen once per CTA.
 // MINB = resident CTAs per SM the register budget is sized for (2: no spills,
 // 3: more warps, a few spills); the autotuner picks per network.
+//
+// STAGED with kGatherBins (bins of 1024 neurons: one tile per warp per chunk): the
+// chunk's eight tiles are in the warps' stage buffers before the fold, and the
+// bin's events are added by shared-memory atomics straight into their J planes
+// there (no separate sums, two CTA barriers per chunk); the bin's entries are
+// loaded while the warps wait for their copies.
 template <int GATHER, bool UPDATE, bool FORCED, int MINB = 2, bool STAGED = false>
 __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int tiles_per_warp)
 {
-    static_assert(!STAGED || GATHER == 0, "staged loads are for the update without gather");
+    static_assert(!STAGED || GATHER == 0 || (GATHER == kGatherBins && UPDATE),
+                  "staged loads are for the update without gather, or with the bin fold");
+    constexpr bool kBinStaged = STAGED && GATHER == kGatherBins;
     constexpr int kWarps = kStepThreads / 32;
     extern __shared__ __align__(128) unsigned char stage_smem[];   // STAGED: [warp][2][kStageBytes]
     __shared__ __align__(8) unsigned long long stage_bar[kWarps][2];
@@ -472,6 +509,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     __shared__ double sh_vsum[kWarps];
     __shared__ unsigned long long sh_ev[kWarps];
     __shared__ int sh_last;
+    __shared__ uint32_t sh_buf[kWarps];   // kBinStaged: each warp's stage buffer of the chunk (byte offset)
+    __shared__ __align__(8) unsigned long long bin_bar[2];   // kBinStaged: the bin buffers' copies
 
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
@@ -524,16 +563,144 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&stage_bar[wid][0])) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&stage_bar[wid][1])) : "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (tile0 < tile1 && (tile0 + 1) * kWarpNeurons <= s.N)
-                stage_tile(s, tile0 * kWarpNeurons, my_stage, smem_u32(&stage_bar[wid][0]));
+            const int64_t first = kBinStaged ? bc0 * kWarps + wid : tile0;
+            if (n_iter > 0 && (first + 1) * kWarpNeurons <= s.N)
+                stage_tile(s, first * kWarpNeurons, my_stage, smem_u32(&stage_bar[wid][0]));
         }
         __syncwarp();
+    }
+    // kBinStaged: counts of the current and next chunk's bins, copies issued per bin buffer,
+    // copies given up on (drained at exit); CTA-uniform
+    unsigned char* bin_sm = stage_smem + kStagedSmem;
+    uint32_t cnt_cur = 0u, cnt_nxt = 0u;
+    uint32_t bin_npar = 0u;   // bit b: phase parity of the next copy into bin buffer b
+    uint32_t bin_pend = 0u;   // bit b: the latest copy into bin buffer b was given up on
+    bool bins_off = false, cur_staged = false;
+    if (kBinStaged) {
+        if (bc0 < bc1) cnt_cur = __ldcg(s.bin_cnt + bc0);
+        if (bc0 + 1 < bc1) cnt_nxt = __ldcg(s.bin_cnt + bc0 + 1);
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bin_bar[0])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bin_bar[1])) : "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (bc0 < bc1) stage_bin(s, bc0, bin_stage_n(s, cnt_cur), bin_sm, smem_u32(&bin_bar[0]));
+        }
+        if (bc0 < bc1) { bin_npar = 1u; cur_staged = true; }
+        __syncthreads();   // the barriers' initialisation before any wait
     }
 
     for (int64_t iter = 0; iter < n_iter; ++iter) {
         int64_t tile = tile0 + iter;
         int64_t bchunk = 0;
-        if (GATHER == kGatherBins) {   // CTA-uniform: every warp runs the same iterations
+        const int it = (int)iter;   // the warp's tile sequence number: stage buffer and phase
+        const int sb = it & 1;
+        bool staged = false;        // this tile's state is in stage_buf
+        unsigned char* stage_buf = my_stage + sb * kStageBytes;
+        if (kBinStaged) {   // CTA-uniform: every warp runs the same iterations, one tile each
+            bchunk = bc0 + iter;
+            tile = bchunk * kWarps + wid;
+            const bool have = tile < ntiles;
+            const int bb = it & 1;   // bin buffer of this chunk
+            // the next chunk's bin entries, into the other bin buffer (its last reader, the
+            // previous chunk's fold, finished before the previous barrier)
+            const bool nxt_staged = !bins_off && bchunk + 1 < bc1;
+            if (nxt_staged) {
+                if (threadIdx.x == 0)
+                    stage_bin(s, bchunk + 1, bin_stage_n(s, cnt_nxt), bin_sm + (bb ^ 1) * kBinStageBytes,
+                              smem_u32(&bin_bar[bb ^ 1]));
+                bin_npar ^= 1u << (bb ^ 1);
+            }
+            const uint32_t n_raw = cnt_cur;
+            cnt_cur = cnt_nxt;
+            cnt_nxt = bchunk + 2 < bc1 ? __ldcg(s.bin_cnt + bchunk + 2) : 0u;
+            const uint32_t nb = n_raw < s.bin_cap ? n_raw : s.bin_cap;
+            if (have) {
+                const int64_t base = tile * kWarpNeurons;
+                if (!stage_off && base + kWarpNeurons <= s.N) {
+                    const bool ok = stage_wait(smem_u32(&stage_bar[wid][sb]), (uint32_t)((it >> 1) & 1),
+                                               s.stage_wait_limit);
+                    staged = __all_sync(0xffffffffu, ok);
+                    if (!staged) {   // as below: flag, stop copying, keep off the buffer
+                        if (lane == 0) atomicOr(&s.ctl->err, kErrStageTimeout);
+                        stage_off = true;
+                        bad_sb = sb;
+                        bad_parity = (uint32_t)((it >> 1) & 1);
+                    }
+                }
+                if (stage_off && sb == bad_sb) stage_buf = my_stage + (sb ^ 1) * kStageBytes;
+                if (!staged) {   // a partial tile, or a copy given up on: the lanes load it
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int k = j * 32 + lane;
+                        const int64_t n = base + k;
+                        if (n >= s.N) continue;
+                        reinterpret_cast<float*>(stage_buf)[k] = __ldcs(s.V + n);
+                        reinterpret_cast<float*>(stage_buf + kWarpNeurons * 4)[k] = __ldcs(s.tlast + n);
+                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 8)[k] = __ldcs(s.J2 + n);
+                        reinterpret_cast<float2*>(stage_buf + kWarpNeurons * 16)[k] = __ldcs(s.J2 + s.j_ps + n);
+                    }
+                }
+                // the next chunk's tile of this warp, into the buffer this warp has finished with
+                const int64_t nt = tile + kWarps;
+                if (!stage_off && lane == 0 && iter + 1 < n_iter && (nt + 1) * kWarpNeurons <= s.N)
+                    stage_tile(s, nt * kWarpNeurons, my_stage + (sb ^ 1) * kStageBytes,
+                               smem_u32(&stage_bar[wid][sb ^ 1]));
+            }
+            if (lane == 0) sh_buf[wid] = (uint32_t)(stage_buf - stage_smem);
+            // this chunk's staged bin entries (every thread waits: the copies' data is then
+            // visible to it), and every tile of the chunk staged
+            bool ok = true;
+            if (cur_staged)
+                ok = stage_wait(smem_u32(&bin_bar[bb]), ((bin_npar >> bb) & 1u) ^ 1u, s.stage_wait_limit);
+            const bool bad = __syncthreads_or(!ok);
+            uint32_t n_st = 0u;
+            if (cur_staged) {
+                if (bad) {   // given up on: the entries come from global memory, no more bin copies
+                    if (threadIdx.x == 0) atomicOr(&s.ctl->err, kErrStageTimeout);
+                    bins_off = true;
+                    bin_pend |= 1u << bb;
+                } else {
+                    n_st = bin_stage_n(s, n_raw);
+                }
+            }
+            cur_staged = nxt_staged;
+            if (threadIdx.x == 0 && n_raw) s.bin_cnt[bchunk] = 0u;
+            // fold: entry = local neuron (10 bits: warp, lane-neuron) | kind << 15, added into the
+            // staged J planes
+            auto fold_add = [&](uint32_t x, float2 w) {
+                const uint32_t l = x & 0x3ffu;
+                float* a = reinterpret_cast<float*>(stage_smem + sh_buf[l >> 7] + kWarpNeurons * 8 +
+                                                    (x >> 15) * (kWarpNeurons * 8)) + 2 * (l & 127u);
+                atomicAdd(a, w.x);
+                atomicAdd(a + 1, w.y);
+            };
+            {
+                const uint16_t* sbi = reinterpret_cast<const uint16_t*>(bin_sm + bb * kBinStageBytes);
+                const float2* sbw = reinterpret_cast<const float2*>(bin_sm + bb * kBinStageBytes + kBinStageMax * 2);
+                for (uint32_t i = threadIdx.x; i < n_st; i += kStepThreads) fold_add(sbi[i], sbw[i]);
+            }
+            if (nb > n_st) {   // the rest of the bin from global memory, kFoldBatch entries per thread in flight
+                const uint16_t* __restrict__ bi = s.bin_idx + bchunk * (int64_t)s.bin_cap;
+                const float2* __restrict__ bw = s.bin_w + bchunk * (int64_t)s.bin_cap;
+                for (uint32_t i0 = n_st; i0 < nb; i0 += kStepThreads * kFoldBatch) {
+                    uint32_t x[kFoldBatch];
+                    float2 w[kFoldBatch];
+#pragma unroll
+                    for (int u = 0; u < kFoldBatch; ++u) {
+                        const uint32_t i = i0 + threadIdx.x + u * kStepThreads;
+                        x[u] = 0u;
+                        w[u] = make_float2(0.f, 0.f);
+                        if (i < nb) { x[u] = __ldcs(bi + i); w[u] = __ldcs(bw + i); }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kFoldBatch; ++u)
+                        if (i0 + threadIdx.x + u * kStepThreads < nb) fold_add(x[u], w[u]);
+                }
+            }
+            __syncthreads();   // the chunk's events are in the staged J planes
+            staged = true;
+            if (!have) continue;
+        } else if (GATHER == kGatherBins) {   // CTA-uniform: every warp runs the same iterations
             const int64_t ci = iter / tpw_b;
             const int jj = (int)(iter - ci * tpw_b);
             bchunk = bc0 + ci;
@@ -547,11 +714,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         }
         const int64_t base = tile * kWarpNeurons;
         float4 Jn[4];
-        const int it = (int)(tile - tile0);
-        const int sb = it & 1;
-        bool staged = false;   // this tile's state is in stage_buf
-        unsigned char* stage_buf = my_stage + sb * kStageBytes;
-        if (STAGED) {
+        if (STAGED && !kBinStaged) {
             if (!stage_off && base + kWarpNeurons <= s.N) {
                 const bool ok = stage_wait(smem_u32(&stage_bar[wid][sb]), (uint32_t)((it >> 1) & 1),
                                            s.stage_wait_limit);
@@ -790,7 +953,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 }
                 continue;
             }
-        } else if (GATHER == kGatherBins) {
+        } else if (GATHER == kGatherBins && !kBinStaged) {
             const float4* acc = bacc + (base - bchunk * chunk_tiles * kWarpNeurons);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -1010,6 +1173,13 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         if (STAGED) __syncwarp();   // every lane is done with the buffer before lane 0 refills it
     }
     if (flushed) __threadfence();
+    if (kBinStaged && threadIdx.x == 0) {
+        // bin copies given up on must land before this CTA's shared memory is released
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+            if (((bin_pend >> b) & 1u) && !stage_wait(smem_u32(&bin_bar[b]), ((bin_npar >> b) & 1u) ^ 1u, 1u << 22))
+                atomicOr(&s.ctl->err, kErrStageDrain);
+    }
     if (STAGED && stage_off) {
         // a copy given up on must land before this CTA's shared memory is released
         if (lane == 0 && !stage_wait(smem_u32(&stage_bar[wid][bad_sb]), bad_parity, 1u << 22))

@@ -249,7 +249,8 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          firing rows one scatter CTA takes per round (1..256)
  * DTB_TUNE_BIN_CAPACITY    binned push: bin entries per neuron of the bin
  *                          (1..1024, default 8; 10 bytes each); reallocates
- * DTB_TUNE_BIN_SHIFT       binned push: B (10..13), 0 = chosen from N (11 from 8M neurons, else 10); reallocates
+ * DTB_TUNE_BIN_SHIFT       binned push: B (10..13), 0 = 10; reallocates; the update stages
+ *                          its state (step variants 2..4) only with B = 10
  * DTB_TUNE_SCATTER_REVERSE atomic push scatter: 0 = CTAs take the bitmask from its start,
  *                          1 = from its end (the rows scattered first then target the
  *                          neurons whose J the update wrote last)

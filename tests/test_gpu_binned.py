@@ -12,7 +12,8 @@ import pytest
 
 from digital_twin_brain_b200 import Network, synthetic
 from digital_twin_brain_b200._lib import (FIELD_I_SYN, FIELD_J, FIELD_STEP, FIELD_T, FIELD_T_LAST, FIELD_V, TUNE_BIN_CAPACITY,
-                                          TUNE_BIN_SHIFT, TUNE_BIN_WORDS, TUNE_PUSH_METHOD)
+                                          TUNE_BIN_SHIFT, TUNE_BIN_WORDS, TUNE_PUSH_METHOD, TUNE_STAGE_WAIT_LIMIT,
+                                          TUNE_STEP_VARIANT, DtbError)
 from tests._helpers import GOLDEN, unpack
 from tests.test_gpu_parity import class_decay_like_reference
 
@@ -35,13 +36,17 @@ def _binned(spec, tune=None):
     return net
 
 
+@pytest.mark.parametrize("variant", [0, 3])
 @pytest.mark.parametrize("words", [1, 64, 256])
 @pytest.mark.parametrize("shift", [10, 11, 13])
-def test_binned_step_equals_pull_step_from_same_state(shift, words):
+def test_binned_step_equals_pull_step_from_same_state(shift, words, variant):
     """One binned push step from identical state vs the exact pull step, 60 times (past the
-    50-step refractory window, so spikes, thresholds and t_last are exercised)."""
+    50-step refractory window, so spikes, thresholds and t_last are exercised).  Step
+    variant 3 with 1024-neuron bins is the staged update that adds the bins into the staged
+    J planes (a partial last tile, and a last chunk with a warp that has no tile: N = 9000);
+    with larger bins it runs the unstaged fold."""
     spec = synthetic.single_block(9000, 100, noise_rate=0.02, name="n9k")
-    a = _binned(spec, {TUNE_BIN_SHIFT: shift, TUNE_BIN_WORDS: words})
+    a = _binned(spec, {TUNE_BIN_SHIFT: shift, TUNE_BIN_WORDS: words, TUNE_STEP_VARIANT: variant})
     b = Network.from_spec(spec, device=0)
     for _ in range(60):
         a.run(1, mode="push")
@@ -52,12 +57,13 @@ def test_binned_step_equals_pull_step_from_same_state(shift, words):
         _resync(b, a)
 
 
+@pytest.mark.parametrize("variant", [0, 2, 3])
 @pytest.mark.parametrize("cap", [1, 2])
-def test_bins_overflowing_into_atomics(cap):
+def test_bins_overflowing_into_atomics(cap, variant):
     """Capacities far below the events per bin: most events take the atomic fallback; dense
-    activity (p = 0.3) keeps every bin full."""
+    activity (p = 0.3) keeps every bin full (unstaged and staged update)."""
     spec = synthetic.whole_brain(R=5, mean_size=900, sigma=0.5, K=80, gen_seed=4, name="wb5_k80")
-    a = _binned(spec, {TUNE_BIN_CAPACITY: cap})
+    a = _binned(spec, {TUNE_BIN_CAPACITY: cap, TUNE_STEP_VARIANT: variant})
     b = Network.from_spec(spec, device=0)
     for k in range(40):
         rate = 0.3 if k % 2 else 0.05
@@ -67,12 +73,14 @@ def test_bins_overflowing_into_atomics(cap):
         _resync(b, a)
 
 
-def test_binned_teacher_forced_vs_reference_golden():
+@pytest.mark.parametrize("variant", [0, 3])
+def test_binned_teacher_forced_vs_reference_golden(variant):
     """The reference's own block.py run (golden fixture), its spikes fed to the binned push."""
     g = np.load(os.path.join(GOLDEN, "single_block_2k.npz"))
     spec = synthetic.config_single_block()
     net = Network.from_spec(spec, device=0, build_push=True, class_decay=class_decay_like_reference(spec))
     net.set_tuning(TUNE_PUSH_METHOD, BINNED)
+    net.set_tuning(TUNE_STEP_VARIANT, variant)
     act_ref = unpack(g["active"], spec.N)
     nact_ref = unpack(g["new_active"], spec.N)
     every = int(g["v_every"])
@@ -153,3 +161,25 @@ def test_synaptic_event_count_every_method(how):
             net.run(1, noise_rate=0.03, mode=mode)
             na = net.get(FIELD_NEW_ACTIVE).astype(bool)
             assert net.get(FIELD_EVENTS) - e0 == int(outdeg[na].sum())
+
+
+def test_binned_staged_copy_given_up():
+    """The staged binned update with the completion-wait limit at 0: every warp gives up on
+    its first copy, loads its tiles from global memory into the other buffer, the fold adds
+    the bins there, the run reports DTB_ERR_CUDA each step, and the results match the exact
+    pull step from the same state."""
+    spec = synthetic.single_block(9000, 100, noise_rate=0.02, name="n9k")
+    a = _binned(spec, {TUNE_STEP_VARIANT: 3, TUNE_STAGE_WAIT_LIMIT: 0})
+    b = Network.from_spec(spec, device=0)
+    for _ in range(60):
+        with pytest.raises(DtbError) as e:
+            a.run(1, mode="push")
+        assert e.value.code == 2 and "staged state copy did not complete" in str(e.value)
+        b.run(1, mode="pull")
+        np.testing.assert_allclose(a.get(FIELD_J), b.get(FIELD_J), rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(a.get(FIELD_V), b.get(FIELD_V), rtol=1e-5, atol=1e-5)
+        assert np.array_equal(a.get(FIELD_T_LAST), b.get(FIELD_T_LAST))
+        _resync(b, a)
+    a.set_tuning(TUNE_STAGE_WAIT_LIMIT, 1 << 20)
+    a.run(5, mode="push")
+    a.synchronize()

@@ -67,3 +67,31 @@ def test_whole_brain_npz_load(tmp_path):
     assert np.array_equal(np.diff(qrp), counts.cpu().numpy())
     s, _, _ = net.run(80, noise_rate=0.01, mode="push")
     assert s[60:].sum() > 0
+
+
+def test_npz_error_in_a_loader_thread(tmp_path):
+    """A corrupt member that only the second pass reads (the weights of one of 12 files): the
+    worker thread that meets it stops the load, and the caller gets DTB_ERR_FORMAT naming the
+    member; the library stays usable and the rewritten files then load."""
+    import zipfile
+    from digital_twin_brain_b200._lib import DtbError
+    spec = synthetic.whole_brain(R=12, mean_size=800, sigma=0.3, K=30, gen_seed=3, name="wb12")
+    d = str(tmp_path / "blocks")
+    write_whole_brain_blocks(d, spec)
+    path = os.path.join(d, "block_7.npz")
+    with zipfile.ZipFile(path) as z:
+        info = z.getinfo("weight.npy")
+    with open(path, "r+b") as f:
+        f.seek(info.header_offset + 26)
+        skip = int.from_bytes(f.read(2), "little") + int.from_bytes(f.read(2), "little")
+        at = info.header_offset + 30 + skip + info.compress_size // 2
+        f.seek(at)
+        b = f.read(1)
+        f.seek(at)
+        f.write(bytes([b[0] ^ 0xFF]))
+    with pytest.raises(DtbError) as e:
+        Network.from_npz(d, dt=0.1, device=0)
+    assert e.value.code == 5 and "weight" in str(e.value)
+    write_whole_brain_blocks(d, spec)
+    net = Network.from_npz(d, dt=0.1, device=0)
+    assert net.N == spec.N and net.S == spec.S
