@@ -380,7 +380,7 @@ def mlp_measure(dev, peaks) -> dict:
 def run_da(args, dev):
     """The data-assimilation comparison (metric part 3) at a reduced region size."""
     from digital_twin_brain_b200 import da_bench
-    argv = ["--members", str(args.da_members), "--judges", str(max(1, args.da_members // 8)),
+    argv = ["--members", str(args.da_members), "--judges", str(max(2, args.da_members // 16)),
             "--region-size", str(args.da_region_size), "--windows", str(args.da_windows),
             "--train-windows", str(args.da_train_windows), "--plain-seeds", "1", "--skip", "4"]
     r = da_bench.main(argv, quiet=True)

@@ -172,6 +172,14 @@ class EnsembleDA:
         cols = [torch.from_numpy(self.net.get_bold(f)[idx]) for f in ("s", "q", "v", "f_in")]
         return torch.stack(cols, dim=-1).reshape(self.M, self.R, 4).to(self.dev)
 
+    def reset_bold_state(self):
+        """The (member, region) BOLD states back to their initial values s = q = 0, v = f_in = 1."""
+        idx = self.region_idx.reshape(-1)
+        for f, v0 in (("s", 0.0), ("q", 0.0), ("v", 1.0), ("f_in", 1.0)):
+            full = self.net.get_bold(f)
+            full[idx] = v0
+            self.net.set_bold(f, full)
+
     def set_bold_state(self, sqvf: torch.Tensor):
         """bold.state_update (bold_model_pytorch.py:34-41) for the (member, region) BOLD states."""
         idx = self.region_idx.reshape(-1)
@@ -231,11 +239,23 @@ class SurrogateDA:
     (calibrate it on held-out windows: a margin over the surrogate's validated error),
     the window is recomputed for the surrogate members on the simulator
     (fallback).  The analysis step is the same diffusion EnKF over all members.
+
+    adapt_split: the judges' window also serves the forecast of the same window:
+    the surrogate first adapts on the first half of the judges, then forecasts every
+    member, is scored on the other half (windows it has not seen) and finally adapts
+    on that half too.  Without it the forecast comes from the surrogate as adapted up
+    to the previous window and every judge scores it.
+
+    self_history: after the burn-in, the members off the simulator start from rate
+    histories the surrogate forecasts from their own g_ui (iterated on its own output)
+    instead of the judges' regional mean, and the judges' BOLD state restarts from the
+    initial state, so that every member's hemodynamics start together at the first window.
     """
 
     def __init__(self, template: synthetic.NetworkSpec, cfg: DAConfig, surrogate, n_judge: int = 16,
                  threshold: float = 0.3, device: int = 0, adapt_steps: int = 0, adapt_lr: float = 5e-4,
-                 bias_correct: bool = False, spread: bool = False):
+                 bias_correct: bool = False, spread: bool = False, adapt_split: bool = False,
+                 self_history: bool = False):
         from .network import BoldModel
         from .surrogate import HISTORY
         self.cfg = cfg
@@ -250,6 +270,8 @@ class SurrogateDA:
         self.threshold = threshold
         self.adapt_steps = adapt_steps
         self.adapt_lr = adapt_lr
+        self.adapt_split = adapt_split and adapt_steps > 0 and n_judge >= 2
+        self.self_history = self_history
         jcfg = DAConfig(**{**cfg.__dict__, "n_members": n_judge})
         self.judge = EnsembleDA(template, jcfg, device)
         self.full = None   # fallback simulator for the surrogate members (built on first use)
@@ -308,6 +330,17 @@ class SurrogateDA:
             jh = torch.cat([jh[:, :, :1].repeat(1, 1, self.H - jh.shape[2]), jh], 2)
         self.hist = jh.mean(0, keepdim=True).repeat(self.M, 1, 1)
         self.hist[:self.J] = jh
+        if self.self_history and self.M > self.J:
+            # the other members' histories from their own g_ui: the surrogate iterated on its own
+            # forecasts, HISTORY times, starting from the judges' regional mean
+            g_s = self.hp.reshape(self.M, self.R, self.n_hp)[self.J:].reshape(-1, self.n_hp)
+            for _ in range(self.H):
+                p = self.sur.predict(g_s, with_context(self.hist[self.J:], self.sur.context)).reshape(self.M - self.J,
+                                                                                                    self.R)
+                self.hist[self.J:] = torch.cat([self.hist[self.J:, :, 1:], p[:, :, None]], dim=2)
+            # every member's hemodynamics from the initial state at the first window, as in an
+            # all-simulator run (the judges' burn-in windows only warm their neurons)
+            self.judge.reset_bold_state()
 
     def _fallback(self, hp_s: torch.Tensor, bold_sqvf: torch.Tensor):
         if self.full is None:
@@ -333,12 +366,18 @@ class SurrogateDA:
         rates_j = torch.from_numpy(self.judge.window_rates()).to(self.dev).float()
         # surrogate forecast of every member's window rate
         gui = hp.reshape(-1, self.n_hp)
-        pred = self.sur.predict(gui, with_context(self.hist, self.sur.context)).reshape(self.M, self.R)
-        # judge score: symmetric relative error of the window rates (floor 1e-5 spikes/step ~ 0.1 Hz)
-        err = judge_error(pred[:self.J], rates_j)
+        ctx = with_context(self.hist, self.sur.context)
+        Ja = self.J // 2 if self.adapt_split else 0      # judges the surrogate adapts on before forecasting
+        if Ja:
+            self.sur.adapt(gui[:Ja * self.R], ctx[:Ja * self.R], rates_j[:Ja].reshape(-1), steps=self.adapt_steps,
+                           lr=self.adapt_lr)
+        pred = self.sur.predict(gui, ctx).reshape(self.M, self.R)
+        # judge score on the judges the surrogate has not seen this window: symmetric relative
+        # error of the window rates (floor 1e-5 spikes/step ~ 0.1 Hz)
+        err = judge_error(pred[Ja:self.J], rates_j[Ja:])
         self.errors.append(err)
         if self.adapt_steps:   # the judges' fresh windows refine the surrogate (scored before it learns them)
-            self.sur.adapt(gui[:self.J * self.R], with_context(self.hist[:self.J], self.sur.context), rates_j.reshape(-1),
+            self.sur.adapt(gui[Ja * self.R:self.J * self.R], ctx[Ja * self.R:self.J * self.R], rates_j[Ja:].reshape(-1),
                            steps=self.adapt_steps, lr=self.adapt_lr)
         sqvf = torch.stack([self.bold.get(k) for k in range(4)], dim=-1).reshape(self.M - self.J, self.R, 4)
         if err > self.threshold:
@@ -350,7 +389,7 @@ class SurrogateDA:
             rates_s = pred[self.J:]
             if self.spread:
                 eps = 1e-6
-                res = torch.log(rates_j + eps) - torch.log(pred[:self.J] + eps)
+                res = torch.log(rates_j[Ja:] + eps) - torch.log(pred[Ja:self.J] + eps)
                 sd = float(res.std())
                 z = torch.randn(rates_s.shape, generator=self.gen, device=self.dev)
                 rates_s = rates_s * torch.exp(sd * z - 0.5 * sd * sd)

@@ -166,7 +166,7 @@ struct dtb_block {
     int chunk = 32;
     int scatter_wpw = 32;         // bitmask words per warp in the push scatter
     int scatter_variant = 0;      // 0: registers unbounded, 1: budgeted for 6 resident CTAs per SM
-    int step_variant = 0;         // 0: 2 resident CTAs/SM register budget, 1: 3; 2..4: staged, 2..4 CTAs/SM
+    int step_variant = 3;         // 0: 2 resident CTAs/SM register budget, 1: 3; 2..4: staged, 2..4 CTAs/SM
     // ordered push (bit-exact pull through per-neuron slots)
     bool has_qpos = false;
     int pull_method = 0;          // 0: auto, 1: row gather, 2: ordered push (slots), 3: (masks), 4: streamed gather

@@ -1,6 +1,6 @@
 """Data-assimilation window benchmark: surrogate-served vs all-simulator ensemble.
 
-    python -m digital_twin_brain_b200.da_bench [--members 128] [--judges 16] [--regions 90]
+    python -m digital_twin_brain_b200.da_bench [--members 128] [--judges 8] [--regions 90]
         [--region-size 2000] [--windows 50] [--steps-per-window 8000] [--train-windows 18] [--out FILE]
 
 1. Truth: one network with hidden true g_ui factors (per region, 4 receptors)
@@ -8,9 +8,12 @@
    noise (sigma = 0.1 x the per-region std over windows) is the observation.
 2. Plain: EnsembleDA with every member on the simulator
    (data_assimilation/DataAssimilation.py:402-453 restated).
-3. Surrogate: training windows from a random-walk ensemble, RateSurrogate
-   trained on them, then SurrogateDA (judges on the simulator, the rest
-   forecast by the network, fallback on judge error).
+3. Surrogate: training windows from an assimilation run against another
+   hidden truth and from a random-walk ensemble, RateSurrogate trained on
+   them, then SurrogateDA: judges on the simulator, the rest forecast by the
+   network, which adapts on half of each window's judges before forecasting
+   that window and is scored on the other half (fallback on judge error); the
+   members off the simulator start from histories forecast from their own g_ui.
 Reports mean window time of both, their ratio, the BOLD-fit RMSE of the
 ensemble-mean forecast against the observation, and the g_ui recovery error.
 The reference's 2e5 neurons per region do not fit 128 members on one GPU
@@ -51,7 +54,7 @@ def main(argv=None, quiet: bool = False) -> dict:
     (and prints it as one JSON line unless quiet)."""
     ap = argparse.ArgumentParser()
     ap.add_argument("--members", type=int, default=128)
-    ap.add_argument("--judges", type=int, default=16)
+    ap.add_argument("--judges", type=int, default=8)
     ap.add_argument("--regions", type=int, default=90)
     ap.add_argument("--region-size", type=float, default=2000)
     ap.add_argument("--K", type=int, default=100)
@@ -74,6 +77,11 @@ def main(argv=None, quiet: bool = False) -> dict:
                     help="give the surrogate members' rates the judges' residual spread")
     ap.add_argument("--bias-correct", type=int, default=0,
                     help="correct the surrogate members' BOLD by the judges' simulated-minus-surrogate mean")
+    ap.add_argument("--self-history", type=int, default=1,
+                    help="1: members off the simulator start from surrogate-forecast histories of their own g_ui, "
+                         "and every member's BOLD starts at the first window")
+    ap.add_argument("--adapt-split", type=int, default=1,
+                    help="1: adapt on half of each window's judges before forecasting that window, score on the other half")
     ap.add_argument("--adapt-steps", type=int, default=60,
                     help="Adam steps per window on the judges' windows (0: the surrogate stays as trained)")
     ap.add_argument("--gain", type=float, default=2.0,
@@ -163,7 +171,7 @@ def main(argv=None, quiet: bool = False) -> dict:
     # ---- surrogate-served DA
     sda = SurrogateDA(template, DAConfig(n_members=a.members, **base), sur, n_judge=a.judges,
                       threshold=threshold, adapt_steps=a.adapt_steps, bias_correct=bool(a.bias_correct),
-                      spread=bool(a.spread))
+                      spread=bool(a.spread), adapt_split=bool(a.adapt_split), self_history=bool(a.self_history))
     sda.hp_random_initialize()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -173,7 +181,7 @@ def main(argv=None, quiet: bool = False) -> dict:
     res_s = sda.run(obs)
     out.update(summarize(res_s, "surrogate"))
     out.update(fallbacks=int(res_s["fallbacks"]), judge_err_mean=float(np.mean(res_s["errors"])),
-               judge_err=[round(float(e), 4) for e in res_s["errors"]], adapt_steps=a.adapt_steps,
+               judge_err=[round(float(e), 4) for e in res_s["errors"]], adapt_steps=a.adapt_steps, adapt_split=a.adapt_split, self_history=a.self_history,
                bias_correct=a.bias_correct, spread=a.spread)
     out["surrogate_burn_in_s"] = t_burn
     out["burn_in_windows"] = a.burn_in_windows

@@ -160,3 +160,37 @@ class RateSurrogate:
     def predict(self, gui, hist) -> torch.Tensor:
         y = self.mlp.forward(self.features(gui, hist))
         return torch.clamp(torch.exp(y * self.sd_y + self.mu_y) - self.eps, min=0.0)
+
+
+def _main(argv=None):
+    """python -m digital_twin_brain_b200.surrogate [--rows B] [--calls n]: n forward passes and n
+    Adam training steps of the surrogate network (14 -> 256 -> 256 -> 1) on B random rows, for
+    timing and profiling its tensor-core kernels; prints the mean milliseconds of each."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rows", type=int, default=128 * 90)
+    ap.add_argument("--calls", type=int, default=5)
+    a = ap.parse_args(argv)
+    dev = torch.device("cuda", 0)
+    m = MLP(N_GUI + HISTORY + CONTEXT, 256, seed=0, device=0)
+    g = torch.Generator(device=dev).manual_seed(0)
+    x = torch.randn(a.rows, m.in_dim, device=dev, generator=g)
+    t = torch.randn(a.rows, device=dev, generator=g)
+    out = {}
+    for name, fn in (("forward", lambda: m.forward(x)), ("train_step", lambda: m.train_step(x, t, 1e-4))):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.calls):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        out[name + "_ms"] = e0.elapsed_time(e1) / a.calls
+    m.close()
+    print(json.dumps({"rows": a.rows, **out}))
+
+
+if __name__ == "__main__":
+    _main()

@@ -217,7 +217,9 @@ int dtb_block_time_kernels(dtb_block* b, int n_steps, float noise_rate, int isol
  *                          CTAs per SM (no spills), 1 = three, 2, 3 and 4 =
  *                          two, three and four with the state of the next
  *                          tile bulk-copied to shared memory while the
- *                          current one computes
+ *                          current one computes (default 3; the results are
+ *                          bit-identical every way; a network whose J planes
+ *                          do not allow the copies runs variant 0 or 1)
  * DTB_TUNE_PULL_METHOD     how DTB_MODE_PULL propagates (bit-identical every
  *                          way): 1 = every postsynaptic row gathers its firing
  *                          inputs; 2 = ordered push: firing rows scatter into

@@ -60,6 +60,17 @@ def test_surrogate_da_runs_with_judges_and_fallback():
     sda3.burn_in(2)
     res3 = sda3.run(obs)
     assert res3["fallbacks"] == 0 and np.isfinite(res3["bold_pred"]).all()
+    # the forecast of a window from the surrogate adapted on half of that window's judges; the
+    # other members' start histories forecast from their own g_ui, every BOLD state restarted
+    sda4 = SurrogateDA(TEMPLATE, cfg, sur, n_judge=4, threshold=1e9, adapt_steps=3, adapt_split=True,
+                       self_history=True)
+    sda4.hp_random_initialize()
+    sda4.burn_in(1)
+    assert not torch.equal(sda4.hist[4], sda4.hist[5])          # members' own histories
+    jb = sda4.judge.get_bold_state()
+    assert torch.all(jb[..., 0] == 0) and torch.all(jb[..., 2] == 1) and torch.all(jb[..., 3] == 1)
+    res4 = sda4.run(obs)
+    assert res4["fallbacks"] == 0 and np.isfinite(res4["bold_pred"]).all() and len(res4["errors"]) == 3
 
 
 def test_surrogate_adapt_lowers_loss_on_new_windows():
