@@ -442,6 +442,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     clk.__enter__()
     try:
         kt = net.time_kernels(64, noise_rate=args.noise, mode=mode)
+        # the chunk graphs of the chosen method are captured here, outside the timed region
+        net.run(64, noise_rate=args.noise, mode=mode, out=None)
         torch.cuda.synchronize(dev)
 
         # ---- timed region: exactly K steps on the device

@@ -214,6 +214,55 @@ __device__ __forceinline__ void stage_rows(unsigned char* tiles, int nt, Get get
     }
 }
 
+// Eight consecutive elements of a row as FP32 (16-byte aligned source).
+__device__ __forceinline__ void load8(const float* p, float* x)
+{
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p)), b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+}
+__device__ __forceinline__ void load8(const __nv_bfloat16* p, float* x)
+{
+    const uint4 a = __ldg(reinterpret_cast<const uint4*>(p));
+    const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&a);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) x[e] = __bfloat162float(h[e]);
+}
+
+// stage_rows for a K-contiguous operand whose chunk lies inside the matrix: thread t loads
+// row t's 32 elements with 16-byte loads (row = nullptr: a row past the matrix, zeros).
+template <typename T>
+__device__ __forceinline__ void stage_rows_contig(unsigned char* tiles, int nt, const T* row)
+{
+    const int r = threadIdx.x;
+    float x[kMmaKc];
+#pragma unroll
+    for (int c = 0; c < kMmaKc / 8; ++c) {
+        if (row) load8(row + c * 8, x + c * 8);
+        else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) x[c * 8 + e] = 0.0f;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kMmaKc / 8; ++c) {
+        __align__(16) __nv_bfloat16 t[3][8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            __nv_bfloat16 s3[3];
+            split_bf16(x[c * 8 + e], nt, s3);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) t[i][e] = s3[i];
+        }
+        const int off = ((r >> 3) * (kMmaKc / 8) + c) * 128 + (r & 7) * 16;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if (i < nt) *reinterpret_cast<uint4*>(tiles + i * kMmaTile + off) = *reinterpret_cast<const uint4*>(t[i]);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ bool aligned16(const T* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 template <typename TA, typename TB>
 __global__ void __launch_bounds__(kMmaThreads) k_mma_gemm(MmaArgs g)
 {
@@ -250,14 +299,27 @@ __global__ void __launch_bounds__(kMmaThreads) k_mma_gemm(MmaArgs g)
     bool ok = true;
     for (int64_t k0 = k_begin; k0 < k_end; k0 += kMmaKc, ++chunks) {
         if (chunks > 0 && ok) ok = mma_wait(mb, (uint32_t)((chunks - 1) & 1), 1u << 22);   // tiles free again
-        stage_rows(sA, nA, [&](int r, int k) -> float {
-            const int64_t m = m0 + r, kk = k0 + k;
-            return (m < g.M && kk < k_end) ? ld_elem(A, m * g.a_m + kk * g.a_k) : 0.0f;
-        });
-        stage_rows(sB, nB, [&](int r, int k) -> float {
-            const int64_t n = n0 + r, kk = k0 + k;
-            return (r < g.n_tile && n < g.N && kk < k_end) ? ld_elem(B, kk * g.b_k + n * g.b_n) : 0.0f;
-        });
+        // K-contiguous rows with a whole chunk in range: 16-byte loads; otherwise element by element
+        const bool full = k0 + kMmaKc <= k_end;
+        if (full && g.a_k == 1 && aligned16(A) && (g.a_m * (int64_t)sizeof(TA)) % 16 == 0) {
+            const int64_t m = m0 + threadIdx.x;
+            stage_rows_contig(sA, nA, m < g.M ? A + m * g.a_m + k0 : static_cast<const TA*>(nullptr));
+        } else {
+            stage_rows(sA, nA, [&](int r, int k) -> float {
+                const int64_t m = m0 + r, kk = k0 + k;
+                return (m < g.M && kk < k_end) ? ld_elem(A, m * g.a_m + kk * g.a_k) : 0.0f;
+            });
+        }
+        if (full && g.b_k == 1 && aligned16(B) && (g.b_n * (int64_t)sizeof(TB)) % 16 == 0) {
+            const int64_t n = n0 + threadIdx.x;
+            stage_rows_contig(sB, nB, (threadIdx.x < g.n_tile && n < g.N) ? B + n * g.b_n + k0
+                                                                          : static_cast<const TB*>(nullptr));
+        } else {
+            stage_rows(sB, nB, [&](int r, int k) -> float {
+                const int64_t n = n0 + r, kk = k0 + k;
+                return (r < g.n_tile && n < g.N && kk < k_end) ? ld_elem(B, kk * g.b_k + n * g.b_n) : 0.0f;
+            });
+        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic stores -> tensor-core reads
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -298,15 +360,38 @@ __global__ void __launch_bounds__(kMmaThreads) k_mma_gemm(MmaArgs g)
                          : "r"(taddr) : "memory");
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (ok && m < g.M) {
+                // four columns per access where the row allows it (16-byte aligned, in range)
+                const bool vec = (g.c_m & 3) == 0 && (reinterpret_cast<uintptr_t>(g.C) & 15) == 0 &&
+                                 (reinterpret_cast<uintptr_t>(g.bias) & 15) == 0 &&
+                                 (reinterpret_cast<uintptr_t>(g.H) & 15) == 0;
 #pragma unroll
-                for (int e = 0; e < 16; ++e) {
+                for (int e = 0; e < 16; e += 4) {
                     const int64_t n = n0 + c + e;
-                    if (c + e >= g.n_tile || n >= g.N) continue;
-                    float z = __uint_as_float(v[e]);
-                    if (gridDim.z > 1) { atomicAdd(g.C + m * g.c_m + n, z); continue; }
-                    if (g.bias) z += g.bias[n];
-                    g.C[m * g.c_m + n] = z;
-                    if (g.H) g.H[m * g.c_m + n] = gelu(z);
+                    if (vec && c + e + 4 <= g.n_tile && n + 4 <= g.N) {
+                        float4 z = make_float4(__uint_as_float(v[e]), __uint_as_float(v[e + 1]),
+                                               __uint_as_float(v[e + 2]), __uint_as_float(v[e + 3]));
+                        float4* cp = reinterpret_cast<float4*>(g.C + m * g.c_m + n);
+                        if (gridDim.z > 1) { atomicAdd(cp, z); continue; }
+                        if (g.bias) {
+                            const float4 b = *reinterpret_cast<const float4*>(g.bias + n);
+                            z.x += b.x; z.y += b.y; z.z += b.z; z.w += b.w;
+                        }
+                        *cp = z;
+                        if (g.H)
+                            *reinterpret_cast<float4*>(g.H + m * g.c_m + n) =
+                                make_float4(gelu(z.x), gelu(z.y), gelu(z.z), gelu(z.w));
+                        continue;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int64_t nq = n + q;
+                        if (c + e + q >= g.n_tile || nq >= g.N) continue;
+                        float z = __uint_as_float(v[e + q]);
+                        if (gridDim.z > 1) { atomicAdd(g.C + m * g.c_m + nq, z); continue; }
+                        if (g.bias) z += g.bias[nq];
+                        g.C[m * g.c_m + nq] = z;
+                        if (g.H) g.H[m * g.c_m + nq] = gelu(z);
+                    }
                 }
             }
         }
@@ -448,7 +533,9 @@ int mma_gemm(dtb_mlp* p, int M, int N, int64_t K, const TA* A, int64_t a_m, int6
     g.C = C; g.c_m = c_m;
     g.bias = bias; g.H = H;
     g.err = p->err;
+    // 128-column tiles, or 64 when that leaves fewer than two CTAs per SM (more CTAs in flight)
     g.n_tile = N >= 128 ? 128 : ((N + 15) / 16) * 16;
+    if (g.n_tile == 128 && (int64_t)cdiv(N, 128) * cdiv(M, kMmaM) < 2 * 148) g.n_tile = 64;
     const int64_t tiles = (int64_t)cdiv(N, g.n_tile) * cdiv(M, kMmaM);
     int64_t splits = 1;
     if (split) {
