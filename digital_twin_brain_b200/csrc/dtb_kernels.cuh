@@ -1090,7 +1090,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
             const bool notsat = t >= __fadd_rn(tl, p.Tref);
             const float vs = notsat ? vn : p.Vreset;
             bool a = vs >= p.Vth;
-            const float vmin = isnan(vs) ? vs : (isnan(p.Vth) ? p.Vth : (vs < p.Vth ? vs : p.Vth));
+            // torch.minimum(vs, V_th): NaN when either is NaN (one compare-or-NaN test and a select)
+            const float vmin = (vs < p.Vth || isnan(vs)) ? vs : p.Vth;
             if (FORCED && s.forced_active && (!s.forced_mask || ((__ldg(s.forced_mask + (n >> 5)) >> (n & 31)) & 1u)))
                 a = (__ldg(s.forced_active + (n >> 5)) >> (n & 31)) & 1u;
             const float rate = noise_rate >= 0.0f ? noise_rate : p.noise;
