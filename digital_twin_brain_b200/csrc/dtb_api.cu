@@ -152,6 +152,7 @@ struct dtb_block {
     float* d_export = nullptr;    // [4N]
     float* d_iui_override = nullptr;
     bool override_pending = false;
+    bool override_live = false;   // the device's I_syn override flag may be set: the next update runs the general form
     unsigned* d_err = nullptr;
     // pinned host staging
     void* pinned = nullptr;
@@ -755,6 +756,9 @@ static int launch_update(dtb_block* b, const DevState& s, int gather, bool force
         RET(launch_src(b, s));
         forced = true;
     }
+    // the general form also serves the I_syn override and gamma-distributed g_ui
+    if (s.gnrn != nullptr || b->override_live) forced = true;
+    b->override_live = false;   // this update consumes the override
     if (forced) {
         if (gather == kGatherBins) launch_step<kGatherBins, true, true>(b, s);
         else if (gather == kGatherRows) launch_step<kGatherRows, true, true>(b, s);
@@ -1011,7 +1015,9 @@ static int enqueue_chunk(dtb_block* b, int n, int mode)
 
 static int enqueue_chunk_inner(dtb_block* b, int n, int mode)
 {
-    if (!b->use_graphs || n != b->chunk || b->stream == nullptr) return enqueue_steps(b, n, mode);
+    // a chunk whose first update takes the I_syn override runs ungraphed (the captured graphs
+    // hold the plain form of every step)
+    if (!b->use_graphs || n != b->chunk || b->stream == nullptr || b->override_live) return enqueue_steps(b, n, mode);
     cudaGraphExec_t& ge = b->graph[mode];
     if (!ge) {
         cudaGraph_t g = nullptr;
@@ -1099,6 +1105,8 @@ static int emit_stats(dtb_block* b, int rows, int64_t row0, float* sum_out, floa
         if (*herr) {   // reported once: the flags are cleared
             CK(cudaMemsetAsync(&b->ds.ctl->err, 0, sizeof(uint32_t), b->stream));
             CK(cudaStreamSynchronize(b->stream));
+            if (*herr & kErrGeneralSkipped)
+                return fail(DTB_ERR_STATE, "internal: an update ran without the I_syn override or gamma g_ui it needed");
             if (*herr & (kErrStageTimeout | kErrStageDrain))
                 return fail(DTB_ERR_CUDA, "a staged state copy did not complete in time%s (the update loaded that "
                             "state from global memory instead)", (*herr & kErrStageDrain) ? " and had not landed at exit" : "");
@@ -1676,6 +1684,8 @@ int dtb_block_synchronize(dtb_block* b)
     CK(cudaMemcpy(&err, &b->ds.ctl->err, sizeof(err), cudaMemcpyDeviceToHost));
     if (err) {
         CK(cudaMemset(&b->ds.ctl->err, 0, sizeof(uint32_t)));
+        if (err & kErrGeneralSkipped)
+            return fail(DTB_ERR_STATE, "internal: an update ran without the I_syn override or gamma g_ui it needed");
         if (err & (kErrStageTimeout | kErrStageDrain))
             return fail(DTB_ERR_CUDA, "a staged state copy did not complete in time (the update loaded that state "
                         "from global memory instead)");
@@ -2203,6 +2213,7 @@ static int keep_current_isyn(dtb_block* b)
     CK(cudaMemcpyAsync(&s.ctl->use_isyn_override, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
     CK(cudaStreamSynchronize(b->stream));
     b->override_pending = true;
+    b->override_live = true;
     return DTB_OK;
 }
 
@@ -2222,6 +2233,7 @@ int dtb_block_update_property(dtb_block* b, const float* property, const float* 
     if (b->bold_R == 0) RET(rebuild_groups(b, nullptr));
     b->class_prop_base.clear();
     s.gnrn = nullptr;   // the new matrix holds every neuron's g_ui: gamma factors no longer apply
+    drop_graphs(b);     // captured graphs hold the update's form for the old gnrn
     for (auto& ge : b->graph) if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
     b->override_pending = true;
     return DTB_OK;
@@ -2342,6 +2354,7 @@ int dtb_block_gamma_property_by_subblock(dtb_block* b, int n, const int32_t* sub
         if (e == cudaSuccess) e = cudaMemcpyAsync(db, hb.data(), sizeof(double) * hb.size(), cudaMemcpyHostToDevice, b->stream);
         if (e == cudaSuccess) {
             b->ds.gnrn = b->d_gnrn;
+            drop_graphs(b);   // captured graphs hold the plain form of the update
             k_gamma<<<grid_for(b->N, 256), 256, 0, b->stream>>>(b->ds, dreq, da, db, b->gamma_calls, b->d_gnrn);
             e = cudaGetLastError();
         }
@@ -2496,6 +2509,7 @@ int dtb_block_load(dtb_block* b, const char* path)
     if (ov) CK(cudaMemcpy(b->ds.isyn_override, I.data(), 4 * N, cudaMemcpyHostToDevice));
     b->steps = steps;
     b->override_pending = false;
+    b->override_live = ov != 0;
     return DTB_OK;
 }
 

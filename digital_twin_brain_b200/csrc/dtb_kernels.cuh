@@ -361,6 +361,7 @@ constexpr int kStageBytes = kWarpNeurons * (4 + 4 + 8 + 8);       // 3072 per ti
 constexpr int kStagedSmem = (kStepThreads / 32) * 2 * kStageBytes;
 constexpr uint32_t kErrStageTimeout = 1u;                        // Ctl::err bit: a staged copy was given up on
 constexpr uint32_t kErrStageDrain = 2u;                          // Ctl::err bit: ... and had not landed at exit
+constexpr uint32_t kErrGeneralSkipped = 4u;                      // Ctl::err bit: an update needing the general form ran plain
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -487,7 +488,10 @@ __device__ __forceinline__ void fold_bin(const DevState& s, int64_t c, float4* a
 // statistics are kept in registers while consecutive tiles stay in one
 // subblock, so the CTA-wide barrier and the done-count happen once per CTA.
 // MINB = resident CTAs per SM the register budget is sized for (2: no spills,
-// 3: more warps, a few spills); the autotuner picks per network.
+// 3: more warps, a few spills); the autotuner picks per network.  FORCED = the
+// general form: teacher-forced or input spikes, the I_syn override of the step
+// after a property change, gamma-distributed g_ui; the plain form leaves their
+// branches out of the neuron update (fewer registers and instructions).
 //
 // STAGED with kGatherBins (bins of 1024 neurons: one tile per warp per chunk): the
 // chunk's eight tiles are in the warps' stage buffers before the fold, and the
@@ -541,7 +545,7 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     const float t = UPDATE ? __fadd_rn(ctl->t, s.dt) : 0.0f;
     const float noise_rate = ctl->noise_rate;
     const int isolated = ctl->isolated;
-    const bool use_override = UPDATE && ctl->use_isyn_override != 0u;
+    const bool use_override = UPDATE && FORCED && ctl->use_isyn_override != 0u;
     uint32_t* obits = s.bits[steps_done & 1ull];
     const uint32_t* gbits = s.bits[(steps_done - 1ull) & 1ull];
 
@@ -1081,9 +1085,13 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 J = GATHER ? Jn[j] : J_in[j];
             }
             float isyn;
-            if (use_override) isyn = s.isyn_override[n];
-            else if (s.gnrn) isyn = isyn_g(mul4(p.g, __ldcs(s.gnrn + n)), p.Vu, v, J);   // gamma-distributed g_ui
-            else isyn = isyn_of(p, v, J);
+            if (FORCED) {   // the general form: the I_syn override, gamma-distributed g_ui
+                if (use_override) isyn = s.isyn_override[n];
+                else if (s.gnrn) isyn = isyn_g(mul4(p.g, __ldcs(s.gnrn + n)), p.Vu, v, J);
+                else isyn = isyn_of(p, v, J);
+            } else {
+                isyn = isyn_of(p, v, J);
+            }
             const float mainp = __fmul_rn(-p.gL, __fsub_rn(v, p.VL));
             const float cd = __fadd_rn(__fadd_rn(mainp, isyn), p.Iext);
             const float vn = __fadd_rn(v, __fmul_rn(p.rCdt, cd));
@@ -1208,6 +1216,11 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         }
         if (cur >= 0) { atomicAdd(s.sub_spk + cur, cs); atomicAdd(s.sub_nact + cur, cn); atomicAdd(s.sub_vsum + cur, cv); }
         add_events(s, ev, blockIdx.x);
+        // the plain form (FORCED false) has neither the I_syn override nor gamma g_ui: the host
+        // routes such steps to the general form; a step that reached the plain one is flagged
+        // (read before the done-count: the last CTA's epilogue clears the override flag)
+        if (UPDATE && !FORCED && (s.ctl->use_isyn_override != 0u || s.gnrn != nullptr))
+            atomicOr(&s.ctl->err, kErrGeneralSkipped);
         if (UPDATE) {
             __threadfence();   // the CTA's statistics before its done-count
             const unsigned prev = atomicAdd(&s.ctl->done, 1u);
