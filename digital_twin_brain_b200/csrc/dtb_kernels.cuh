@@ -549,7 +549,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     uint32_t* obits = s.bits[steps_done & 1ull];
     const uint32_t* gbits = s.bits[(steps_done - 1ull) & 1ull];
 
-    // warp-level statistics carried across tiles (identical in every lane)
+    // warp-level statistics carried across tiles (identical in every lane, except acc_v: each
+    // lane's own V sum, reduced over the warp when it is flushed)
     int cur_sub = -1;
     uint32_t acc_spk = 0, acc_nact = 0;
     double acc_v = 0.0;
@@ -1119,11 +1120,13 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
                 if (na) atomicAdd(s.unmapped_nact, 1u);
             }
         };
-        bool same = true;
+        bool same = true;   // a tile of one class (known from the tile table, or checked)
+        if (mixed) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (valid[j]) same = same && (c_in[j] == c0);
-        if (__all_sync(0xffffffffu, same)) {
+            for (int j = 0; j < 4; ++j)
+                if (valid[j]) same = same && (c_in[j] == c0);
+        }
+        if (!mixed || __all_sync(0xffffffffu, same)) {
             // one class for the warp's tile, loaded once into registers (a per-warp shared
             // copy read field by field measured slower: 0.230 against 0.224 ms)
             const ParamClass p = load_class(s.pc, c0);
@@ -1152,19 +1155,21 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
         const bool uni = __all_sync(0xffffffffu, lane_uni && (mysub0 == sub0 || !valid[0])) && sub0 >= 0 &&
                          sub0 < s.n_sub;
         if (uni) {
-            double vs = vsum_lane;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) vs += __shfl_xor_sync(0xffffffffu, vs, o);
+            // the V sum stays per lane across the subblock's tiles; the warp reduces it when
+            // the subblock changes and at the end
             if (sub0 != cur_sub) {
+                double vw = acc_v;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) vw += __shfl_xor_sync(0xffffffffu, vw, o);
                 if (cur_sub >= 0 && lane == 0) {
                     atomicAdd(s.sub_spk + cur_sub, acc_spk);
                     atomicAdd(s.sub_nact + cur_sub, acc_nact);
-                    atomicAdd(s.sub_vsum + cur_sub, acc_v);
+                    atomicAdd(s.sub_vsum + cur_sub, vw);
                     flushed = true;
                 }
                 cur_sub = sub0; acc_spk = 0; acc_nact = 0; acc_v = 0.0;
             }
-            acc_spk += cnt_spk; acc_nact += cnt_nact; acc_v += vs;
+            acc_spk += cnt_spk; acc_nact += cnt_nact; acc_v += vsum_lane;
         } else {
             // mixed subblocks in this tile: per-neuron atomics (classes re-read from L1)
 #pragma unroll
@@ -1197,6 +1202,8 @@ __global__ void __launch_bounds__(kStepThreads, MINB) k_step(DevState s, int til
     }
 
     // ---- CTA merge: one barrier, one set of atomics, one done-count per CTA
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc_v += __shfl_xor_sync(0xffffffffu, acc_v, o);   // the lanes' V sums
     if (lane == 0) { sh_sub[wid] = cur_sub; sh_spk[wid] = acc_spk; sh_nact[wid] = acc_nact; sh_vsum[wid] = acc_v; sh_ev[wid] = acc_ev; }
     __syncthreads();
     if (threadIdx.x == 0) {
