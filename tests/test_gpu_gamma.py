@@ -88,3 +88,25 @@ def test_gamma_delta_limit_and_errors():
     net.update_property(spec.property())
     with pytest.raises(DtbError):
         net.g_factors()
+
+
+def test_graphs_follow_the_update_form():
+    """The step's plain form (no gamma g_ui, no I_syn override) and its general form: chunks
+    captured in CUDA graphs before gamma factors are drawn, after they are drawn, and after a
+    property change (whose next step takes the saved I_syn) give the results of the same run
+    without graphs, bit for bit (pull mode)."""
+    from digital_twin_brain_b200._lib import FIELD_J, FIELD_T_LAST, TUNE_USE_GRAPHS
+    spec = _spec()
+    nets = [Network.from_spec(spec, device=0) for _ in range(2)]
+    nets[1].set_tuning(TUNE_USE_GRAPHS, 0)
+    prop = spec.property().copy()
+    prop[:, 10] *= np.float32(1.3)
+    for net in nets:
+        net.run(64, noise_rate=0.02, mode="pull")                   # plain form, graphs captured
+        net.gamma_property_by_subblock([0, 1], [10, 12], [5.0, 0.5], [5.0, 2.0])
+        net.run(64, noise_rate=0.02, mode="pull")                   # general form (gamma g_ui)
+        net.update_property(prop)                                   # drops the gamma factors
+        net.run(64, noise_rate=0.02, mode="pull")                   # override step, then plain
+        net.synchronize()
+    for f in (FIELD_V, FIELD_J, FIELD_T_LAST, FIELD_I_SYN):
+        assert np.array_equal(nets[0].get(f), nets[1].get(f))
